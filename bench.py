@@ -1,0 +1,378 @@
+"""Benchmark: the plain one-plan execute() of the 4M x 64M equi-join.
+
+Workload (one "step" = one execute of this plan):
+  build  4,000,000 unique shuffled INT32 keys + INT64 payload
+  probe  64,000,000 rows: INT32 foreign key Zipf(0.8) over the build keys,
+         30% outside the build domain, 2% NULL; + FP64 payload
+  output build key, build payload, probe key, probe payload
+         (2 INT32 + INT64 + FP64), ~43.5M rows, paged
+Seeded synthetic tables with these shapes stand in for the reference's JOB /
+IMDB data (not available offline).
+
+metric  probe rows/s of the whole job (all ranks).
+value   inputs' pages resident in HBM when the timed region starts; each
+        step decodes, builds, probes and writes the result pages in HBM.
+        Device time of K steps from CUDA events on the library's stream,
+        max over ranks. The inputs (~1.1 GB of pages) are larger than L2,
+        so L2 is not flushed between steps.
+e2e     the same plan through cj_execute with HOST page-locked input pages
+        and a host result: page upload and result download inside the timed
+        region; wall clock per step.
+roofline dominant kernel's algorithmic bytes per launch / its mean
+        event-timed duration, against the measured HBM copy bandwidth.
+cpu_baseline the reference's own execute() (oracle/_ref, all host threads)
+        on the same shape with INT32 payload stand-ins (the reference cannot
+        emit INT64 / FP64 columns), rank 0 at N=1 only.
+
+--impl reference runs only that CPU reference (rank 0; other ranks exit).
+Multi-GPU (torchrun): independent replicas, one per GPU, no collective on
+the data path ("scaling": "weak").
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "probe rows/s, 4M x 64M INT32 equi-join (plain execute)"
+UNIT = "rows/s"
+WORKLOAD = ("C2: build 4,000,000 unique shuffled INT32 keys + INT64 payload; probe 64,000,000 rows, "
+            "INT32 FK Zipf(0.8) over build keys, 30% outside the build domain, 2% NULL, + FP64 payload; "
+            "output build key, build INT64, probe key, probe FP64 (2 INT32 + INT64 + FP64)")
+
+
+def rank_info():
+    return (int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")),
+            int(os.environ.get("LOCAL_RANK", "0")))
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.thread.join(timeout=2)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if len(r) > 2 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 2 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            for k, n in enumerate(names):
+                if len(r) > 5 + k and r[5 + k].lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def traffic_table():
+    """Per-launch DRAM traffic of kernels from committed ncu summaries."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
+def algorithmic_bytes(kernel: str, st: dict, plan_info: dict):
+    """Algorithmic HBM bytes of ONE launch of `kernel` in this workload."""
+    nb, npr = plan_info["build_rows"], plan_info["probe_rows"]
+    m = st["matches"]
+    slots = plan_info["slots"]
+    if kernel == "probe_hash":
+        # probe keys (4 B + 1 validity bit per row), one pass over the hash
+        # table (8 B tuples + 8 B directory slots), 2 x 4 B row ids per match
+        return npr * (4 + 1 / 8) + nb * 8 + slots * 8 + m * 8
+    if kernel == "write_pages_int32":
+        # per output row: 4 B match row id + 4 B value + validity bit read; page bytes written
+        pages = (m + 1983) // 1984
+        return m * (4 + 4 + 1 / 8) + pages * 8192
+    if kernel == "write_pages_8byte":
+        pages = (m + 1006) // 1007
+        return m * (4 + 8 + 1 / 8) + pages * 8192
+    if kernel == "decode_int32":
+        return plan_info["int32_pages"] * 8192 / plan_info["int32_cols"] + 0  # per launch: one column
+    if kernel == "build":
+        return nb * (4 + 4 + 8 + 8 + 8 + 8) + slots * 8
+    return None
+
+
+def gen_workload(pinned: bool, scale: float, int32_standin: bool = False):
+    from calamarijoins_b200.datagen import config_c2, join2
+    from calamarijoins_b200 import DataType
+    if int32_standin:
+        return join2(max(int(4_000_000 * scale), 16), max(int(64_000_000 * scale), 16), seed=202, zipf=0.8,
+                     outside=0.30, probe_null=0.02, build_payload=(DataType.INT32,),
+                     probe_payload=(DataType.INT32,), output=[0, 1, 2, 3], pinned=pinned)
+    return config_c2(seed=202, scale=scale, pinned=pinned)
+
+
+def plan_info(plan):
+    import math
+    nb = plan.inputs[0].num_rows
+    npr = plan.inputs[1].num_rows
+    i32 = [c for t in plan.inputs for c in t.columns if int(c.type) == 0]
+    return {"build_rows": nb, "probe_rows": npr, "slots": 1 << max(11, math.ceil(math.log2(max(nb, 1)))),
+            "int32_pages": sum(c.num_pages for c in i32), "int32_cols": max(len(i32), 1)}
+
+
+def ref_threads():
+    from oracle import oracle_api as oa
+    avail = oa.ref_available()
+    if not avail:
+        return None, []
+    n = os.cpu_count() or 1
+    best = max([t for t in avail if t <= max(n, 8)] or [avail[0]])
+    cands = sorted(set([best] + ([32] if 32 in avail else [])))
+    return best, cands
+
+
+def time_reference(plan, warmup: int, steps: int):
+    """Times oracle/_ref (the reference's execute()) on the host cores."""
+    from calamarijoins_b200 import PlanDescriptor
+    from oracle import oracle_api as oa
+    best, cands = ref_threads()
+    if best is None:
+        return None
+    d = PlanDescriptor(plan)
+    results = {}
+    for t in cands:
+        for _ in range(max(warmup, 1)):
+            oa.ref_execute(d, t)
+        ms = []
+        for _ in range(steps):
+            _, w, _ = oa.ref_execute(d, t)
+            ms.append(w)
+        results[t] = statistics.median(ms)
+    t_best = min(results, key=results.get)
+    return {"threads": t_best, "ms": results[t_best], "all_ms": results}
+
+
+def run_reference(args):
+    rank, world, _ = rank_info()
+    if rank != 0:
+        return 0
+    scale = args.scale
+    plan = gen_workload(False, scale, int32_standin=True)
+    r = time_reference(plan, args.warmup, args.steps)
+    if r is None:
+        print(json.dumps({"impl": "reference", "unavailable": "reference not compiled into oracle/_ref"}))
+        return 0
+    npr = plan.inputs[1].num_rows
+    val = npr / (r["ms"] / 1000.0)
+    sample = (f"C2 shape at scale {scale}: {plan.inputs[0].num_rows} x {npr} rows, INT32 stand-ins for the "
+              f"INT64/FP64 payloads (the reference cannot emit them); median of {args.steps} runs after "
+              f"{max(args.warmup, 1)} warm-up; best of thread counts {sorted(r['all_ms'])}")
+    line = {"impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": 0, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": r["ms"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+            "config": {"workload": WORKLOAD + " [reference: INT32 stand-in payloads]", "parallelism": "cpu threads"},
+            "cpu_baseline": {"value": val, "unit": UNIT, "cores": r["threads"], "kind": "reference",
+                             "sample": sample},
+            "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def run_ours(args):
+    import ctypes as C
+    import numpy as np
+    import torch
+    import calamarijoins_b200 as cj
+    from calamarijoins_b200 import _lib
+
+    rank, world, local = rank_info()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    ctx = cj.Context(local)
+    plan = gen_workload(True, args.scale)
+    info = plan_info(plan)
+    resident = cj.Plan()
+    resident.nodes, resident.root = plan.nodes, plan.root
+    resident.inputs = [cj.ResidentTable(ctx, t) for t in plan.inputs]
+    d_res = cj.PlanDescriptor(resident)
+    d_host = cj.PlanDescriptor(plan)
+    sp = C.c_void_p()
+    _lib.check(_lib.lib().cj_context_stream(ctx.handle, C.byref(sp)))
+    stream = torch.cuda.ExternalStream(sp.value, device=torch.device("cuda", local))
+
+    def step_device():
+        res, st = cj.execute_raw(resident, ctx, _lib.CJ_EXEC_RESULT_ON_DEVICE, d_res)
+        res.free()
+        return st
+
+    for _ in range(args.warmup):
+        st = step_device()
+    ctx.set_option(_lib.CJ_OPT_PROFILE_KERNELS, 1)
+    ctx.profile_reset()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches = 0
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            st = step_device()
+            launches += st.exec["kernel_launches"]
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms_total = e0.elapsed_time(e1)
+    if dist:
+        t = torch.tensor([ms_total], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_total = float(t.item())
+        dist.barrier()
+    prof = ctx.profile()
+    ctx.set_option(_lib.CJ_OPT_PROFILE_KERNELS, 0)
+    ms_step = ms_total / args.steps
+    probe_rows = info["probe_rows"] * world
+    value = probe_rows / (ms_step / 1000.0)
+
+    # e2e through the public API with host buffers
+    for _ in range(max(1, args.warmup)):
+        res, st_h = cj.execute_raw(plan, ctx, 0, d_host)
+        res.free()
+    if dist:
+        dist.barrier()
+    walls = []
+    h2d = d2h = 0
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        res, st_h = cj.execute_raw(plan, ctx, 0, d_host)
+        walls.append(time.perf_counter() - t0)
+        res.free()
+        h2d, d2h = st_h.exec["h2d_bytes"], st_h.exec["d2h_bytes"]
+    e2e_s = statistics.mean(walls)
+    if dist:
+        t = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_value = probe_rows / e2e_s
+
+    # roofline of the dominant kernel
+    peak, peak_kind = measured_peaks()
+    dom = max(prof.items(), key=lambda kv: kv[1][1]) if prof else None
+    roof = None
+    if dom:
+        name, (nl, tot_us) = dom
+        avg_us = tot_us / max(nl, 1)
+        ab = algorithmic_bytes(name, st.exec, info)
+        tr = traffic_table().get(name)
+        achieved = (ab / (avg_us * 1e-6) / 1e9) if ab else None
+        roof = {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": (achieved / peak) if achieved else None,
+                "traffic": (tr.get("bytes_per_launch") if tr else None), "peak_source": peak_kind,
+                "launches_timed": nl, "avg_launch_us": avg_us, "algorithmic_bytes_per_launch": ab}
+
+    kernels = {k: {"launches": v[0], "total_us": v[1], "share": v[1] / max(sum(x[1] for x in prof.values()), 1e-9)}
+               for k, v in sorted(prof.items(), key=lambda kv: -kv[1][1])}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        sample_scale = args.cpu_scale
+        splan = gen_workload(False, sample_scale, int32_standin=True)
+        r = time_reference(splan, 1, 3)
+        if r is not None:
+            snp = splan.inputs[1].num_rows
+            cpu = {"value": snp / (r["ms"] / 1000.0), "unit": UNIT, "cores": r["threads"], "kind": "reference",
+                   "sample": (f"reference execute() (oracle/_ref) on the C2 shape at scale {sample_scale} "
+                              f"({splan.inputs[0].num_rows} x {snp} rows) with INT32 stand-ins for the "
+                              f"INT64/FP64 payloads; median of 3 runs after 1 warm-up; "
+                              f"{r['threads']} threads of {os.cpu_count()} host CPUs")}
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+                "config": {"workload": WORKLOAD, "scale": args.scale,
+                           "inputs": "paged columns resident in HBM (device-resident cj_table)",
+                           "l2": "inputs larger than L2 (1.1 GB of pages); no flush",
+                           "parallelism": f"replicas x{world}",
+                           "output_rows": st.exec["output_rows"], "output_pages": st.exec["output_pages"]},
+                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                        "ms_per_step": e2e_s * 1000.0},
+                "roofline": roof, "cpu_baseline": cpu, "gpu_launches": launches,
+                "clocks": clk.summary(), "kernels": kernels,
+                "phases_us": {k: st.exec[k] for k in ("decode_us", "build_us", "probe_us", "materialize_us")}}
+        print(json.dumps(line))
+    for t in resident.inputs:
+        t.free()
+    ctx.close()
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--scale", type=float, default=1.0, help="row-count scale of the workload")
+    ap.add_argument("--cpu-scale", type=float, default=0.25, help="scale of the CPU-baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args(argv)
+    if args.warmup < 3 and args.impl == "ours":
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

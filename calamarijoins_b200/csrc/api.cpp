@@ -1,0 +1,365 @@
+/*
+ * api.cpp — the C ABI (include/cj_b200.h). Every entry point catches
+ * internal errors and returns a status code; nothing throws across it.
+ */
+#include <cstdlib>
+#include <cstring>
+#include <string>
+
+#include "engine.h"
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int set_error(int code, const std::string &msg) {
+    g_last_error = msg;
+    return code;
+}
+
+#define API_BEGIN try {
+#define API_END                                                                 \
+    }                                                                           \
+    catch (const cj::Error &e) {                                                \
+        return set_error(e.code, e.msg);                                        \
+    }                                                                           \
+    catch (const std::bad_alloc &) {                                            \
+        return set_error(CJ_ERR_OUT_OF_MEMORY, "host allocation failed");       \
+    }                                                                           \
+    catch (...) {                                                               \
+        return set_error(CJ_ERR_INTERNAL, "unexpected exception");              \
+    }                                                                           \
+    g_last_error.clear();                                                       \
+    return CJ_OK;
+
+/* The 2048 smallest 16-bit values with exactly five bits set, ascending:
+ * the Bloom tag table of the reference (include/join_execution/
+ * bloom_tags.h:35-263), regenerated. */
+void make_bloom(uint16_t *out) {
+    int n = 0;
+    for (uint32_t v = 0; v < 65536 && n < 2048; ++v)
+        if (__builtin_popcount(v) == 5) out[n++] = (uint16_t)v;
+}
+
+int64_t env_opt(const char *name, int64_t dflt) {
+    const char *v = std::getenv(name);
+    if (!v || !*v) return dflt;
+    return std::strtoll(v, nullptr, 10);
+}
+
+void set_device(const cj::Context *ctx) { cudaSetDevice(ctx->device); }
+
+} // namespace
+
+extern "C" {
+
+const char *cj_last_error(void) { return g_last_error.c_str(); }
+
+const char *cj_version(void) { return "cj_b200 1 sm_100a"; }
+
+int cj_context_create(int device, cj_context **out) {
+    if (!out) return set_error(CJ_ERR_INVALID_ARGUMENT, "out is null");
+    *out = nullptr;
+    cj_context *c = nullptr;
+    API_BEGIN
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n == 0) {
+        cudaGetLastError();
+        cj::fail(CJ_ERR_NO_DEVICE, "no CUDA device visible");
+    }
+    if (device < 0) cj::check_cuda(cudaGetDevice(&device), "cudaGetDevice");
+    if (device >= n) cj::fail(CJ_ERR_INVALID_ARGUMENT, "device ordinal out of range");
+    cj::check_cuda(cudaSetDevice(device), "cudaSetDevice");
+    c = new cj_context();
+    c->device = device;
+    cj::check_cuda(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device), "attr");
+    cj::check_cuda(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "stream");
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    cj::check_cuda(cudaMemPoolCreate(&c->pool, &props), "cudaMemPoolCreate");
+    uint64_t keep = UINT64_MAX;
+    cj::check_cuda(cudaMemPoolSetAttribute(c->pool, cudaMemPoolAttrReleaseThreshold, &keep), "pool attr");
+    uint16_t bloom[2048];
+    make_bloom(bloom);
+    cj::check_cuda(cudaMalloc(&c->d_bloom, sizeof(bloom)), "cudaMalloc");
+    cj::check_cuda(cudaMemcpy(c->d_bloom, bloom, sizeof(bloom), cudaMemcpyHostToDevice), "bloom upload");
+    cj::check_cuda(cudaMalloc(&c->d_status, sizeof(cj::StatusBlock)), "cudaMalloc");
+    cj::check_cuda(cudaMemset(c->d_status, 0, sizeof(cj::StatusBlock)), "memset");
+    cj::check_cuda(cudaHostAlloc(reinterpret_cast<void **>(&c->h_status), sizeof(cj::StatusBlock), 0), "host");
+    std::memset(c->h_status, 0, sizeof(cj::StatusBlock));
+    for (int i = 0; i < 2; ++i) {
+        cj::check_cuda(cudaHostAlloc(&c->staging[i], c->staging_bytes, 0), "staging");
+        cj::check_cuda(cudaEventCreateWithFlags(&c->staging_ev[i], cudaEventDisableTiming), "event");
+    }
+    c->opt.nested_loop_max_build = env_opt("CJ_NESTED_LOOP_MAX_BUILD", c->opt.nested_loop_max_build);
+    c->opt.slots_per_partition = env_opt("CJ_SLOTS_PER_PARTITION", c->opt.slots_per_partition);
+    c->opt.profile_kernels = env_opt("CJ_PROFILE_KERNELS", c->opt.profile_kernels);
+    c->opt.block_threads = env_opt("CJ_BLOCK_THREADS", c->opt.block_threads);
+    c->opt.varchar_tile_rows = env_opt("CJ_VARCHAR_TILE_ROWS", c->opt.varchar_tile_rows);
+    c->opt.ctas_per_sm = env_opt("CJ_CTAS_PER_SM", c->opt.ctas_per_sm);
+    *out = c;
+    c = nullptr;
+    }
+    catch (const cj::Error &e) {
+        delete c;
+        return set_error(e.code, e.msg);
+    }
+    catch (...) {
+        delete c;
+        return set_error(CJ_ERR_INTERNAL, "unexpected exception");
+    }
+    g_last_error.clear();
+    return CJ_OK;
+}
+
+void cj_context_destroy(cj_context *ctx) {
+    if (!ctx) return;
+    set_device(ctx);
+    delete ctx;
+}
+
+int cj_context_set_option(cj_context *ctx, int32_t option, int64_t value) {
+    if (!ctx) return set_error(CJ_ERR_INVALID_ARGUMENT, "ctx is null");
+    switch (option) {
+    case CJ_OPT_NESTED_LOOP_MAX_BUILD: ctx->opt.nested_loop_max_build = value; break;
+    case CJ_OPT_SLOTS_PER_PARTITION:
+        if (value < 0 || (value & (value - 1))) return set_error(CJ_ERR_INVALID_ARGUMENT, "not a power of two");
+        ctx->opt.slots_per_partition = value;
+        break;
+    case CJ_OPT_PROFILE_KERNELS: ctx->opt.profile_kernels = value; break;
+    case CJ_OPT_BLOCK_THREADS: ctx->opt.block_threads = value; break;
+    case CJ_OPT_VARCHAR_TILE_ROWS:
+        if (value < 64 || value > 8192) return set_error(CJ_ERR_INVALID_ARGUMENT, "tile rows in [64, 8192]");
+        ctx->opt.varchar_tile_rows = value;
+        break;
+    case CJ_OPT_CTAS_PER_SM: ctx->opt.ctas_per_sm = value; break;
+    default: return set_error(CJ_ERR_INVALID_ARGUMENT, "unknown option");
+    }
+    return CJ_OK;
+}
+
+int cj_context_get_option(const cj_context *ctx, int32_t option, int64_t *value) {
+    if (!ctx || !value) return set_error(CJ_ERR_INVALID_ARGUMENT, "null argument");
+    switch (option) {
+    case CJ_OPT_NESTED_LOOP_MAX_BUILD: *value = ctx->opt.nested_loop_max_build; break;
+    case CJ_OPT_SLOTS_PER_PARTITION: *value = ctx->opt.slots_per_partition; break;
+    case CJ_OPT_PROFILE_KERNELS: *value = ctx->opt.profile_kernels; break;
+    case CJ_OPT_BLOCK_THREADS: *value = ctx->opt.block_threads; break;
+    case CJ_OPT_VARCHAR_TILE_ROWS: *value = ctx->opt.varchar_tile_rows; break;
+    case CJ_OPT_CTAS_PER_SM: *value = ctx->opt.ctas_per_sm; break;
+    default: return set_error(CJ_ERR_INVALID_ARGUMENT, "unknown option");
+    }
+    return CJ_OK;
+}
+
+int cj_profile_reset(cj_context *ctx) {
+    if (!ctx) return set_error(CJ_ERR_INVALID_ARGUMENT, "ctx is null");
+    set_device(ctx);
+    cudaStreamSynchronize(ctx->stream);
+    ctx->resolve_profile();
+    ctx->profile.clear();
+    ctx->profile_index.clear();
+    return CJ_OK;
+}
+
+int cj_profile_count(const cj_context *ctx, uint64_t *n) {
+    if (!ctx || !n) return set_error(CJ_ERR_INVALID_ARGUMENT, "null argument");
+    *n = ctx->profile.size();
+    return CJ_OK;
+}
+
+int cj_profile_entry(const cj_context *ctx, uint64_t index, const char **name, uint64_t *launches,
+                     double *total_us) {
+    if (!ctx || index >= ctx->profile.size()) return set_error(CJ_ERR_INVALID_ARGUMENT, "bad index");
+    const auto &p = ctx->profile[index];
+    if (name) *name = p.name.c_str();
+    if (launches) *launches = p.launches;
+    if (total_us) *total_us = p.total_us;
+    return CJ_OK;
+}
+
+int cj_context_stream(const cj_context *ctx, void **stream) {
+    if (!ctx || !stream) return set_error(CJ_ERR_INVALID_ARGUMENT, "null argument");
+    *stream = ctx->stream;
+    return CJ_OK;
+}
+
+int cj_context_memory(const cj_context *ctx, uint64_t *used, uint64_t *reserved) {
+    if (!ctx) return set_error(CJ_ERR_INVALID_ARGUMENT, "ctx is null");
+    API_BEGIN
+    set_device(ctx);
+    cj::check_cuda(cudaStreamSynchronize(ctx->stream), "sync");
+    uint64_t u = 0, r = 0;
+    cj::check_cuda(cudaMemPoolGetAttribute(ctx->pool, cudaMemPoolAttrUsedMemCurrent, &u), "pool attr");
+    cj::check_cuda(cudaMemPoolGetAttribute(ctx->pool, cudaMemPoolAttrReservedMemCurrent, &r), "pool attr");
+    if (used) *used = u;
+    if (reserved) *reserved = r;
+    API_END
+}
+
+/* ------------------------------------------------------------------ */
+int cj_table_upload(cj_context *ctx, const cj_table_desc *table, cj_table **out) {
+    if (!ctx || !table || !out) return set_error(CJ_ERR_INVALID_ARGUMENT, "null argument");
+    *out = nullptr;
+    API_BEGIN
+    set_device(ctx);
+    auto t = std::make_unique<cj_table>();
+    t->ctx = ctx;
+    t->num_rows = table->num_rows;
+    if (table->num_columns && !table->columns) cj::fail(CJ_ERR_INVALID_ARGUMENT, "no column array");
+    for (uint64_t c = 0; c < table->num_columns; ++c) {
+        const cj_column_desc &cd = table->columns[c];
+        if (cd.type < CJ_INT32 || cd.type > CJ_VARCHAR) cj::fail(CJ_ERR_INVALID_ARGUMENT, "unknown column type");
+        cj::ColumnPages cp;
+        cj::upload_pages(*ctx, cd, cp, nullptr);
+        t->cols.push_back(cp);
+    }
+    cj::check_cuda(cudaStreamSynchronize(ctx->stream), "upload");
+    *out = t.release();
+    API_END
+}
+
+int cj_table_from_device(cj_context *ctx, uint64_t num_rows, uint64_t num_columns, const int32_t *types,
+                         const uint64_t *num_pages, const void *const *device_pages, cj_table **out) {
+    if (!ctx || !out || (num_columns && (!types || !num_pages || !device_pages)))
+        return set_error(CJ_ERR_INVALID_ARGUMENT, "null argument");
+    *out = nullptr;
+    API_BEGIN
+    auto t = std::make_unique<cj_table>();
+    t->ctx = ctx;
+    t->num_rows = num_rows;
+    for (uint64_t c = 0; c < num_columns; ++c) {
+        if (types[c] < CJ_INT32 || types[c] > CJ_VARCHAR) cj::fail(CJ_ERR_INVALID_ARGUMENT, "unknown column type");
+        cj::ColumnPages cp;
+        cp.type = types[c];
+        cp.num_pages = num_pages[c];
+        cp.dev = static_cast<const uint8_t *>(device_pages[c]);
+        if (cp.num_pages && !cp.dev) cj::fail(CJ_ERR_INVALID_ARGUMENT, "null device pages");
+        t->cols.push_back(cp);
+    }
+    *out = t.release();
+    API_END
+}
+
+int cj_table_column_pages(const cj_table *table, uint64_t column, const void **device_pages,
+                          uint64_t *num_pages) {
+    if (!table || column >= table->cols.size()) return set_error(CJ_ERR_INVALID_ARGUMENT, "bad column");
+    if (device_pages) *device_pages = table->cols[column].dev;
+    if (num_pages) *num_pages = table->cols[column].num_pages;
+    return CJ_OK;
+}
+
+void cj_table_free(cj_table *table) {
+    if (!table) return;
+    set_device(table->ctx);
+    delete table;
+}
+
+/* ------------------------------------------------------------------ */
+int cj_execute(cj_context *ctx, const cj_plan_desc *plan, uint32_t flags, cj_result **out,
+               cj_timing_stats *timing, cj_exec_stats *stats) {
+    if (!ctx || !plan || !out) return set_error(CJ_ERR_INVALID_ARGUMENT, "null argument");
+    *out = nullptr;
+    set_device(ctx);
+    try {
+        cj_exec_stats st{};
+        cj_result *r = cj::execute_plan(*ctx, *plan, flags, &st);
+        *out = r;
+        if (stats) *stats = st;
+        if (timing) {
+            /* TimingStats fields are whole milliseconds (plan.h:370-378) */
+            timing->hashtable_build_ms = (int64_t)(st.build_us / 1000.0);
+            timing->hash_join_probe_ms = (int64_t)(st.probe_us / 1000.0);
+            timing->nested_loop_join_ms = (int64_t)(st.nested_loop_us / 1000.0);
+            timing->materialize_ms = (int64_t)((st.materialize_us + st.download_us) / 1000.0);
+            timing->setup_ms = (int64_t)((st.upload_us + st.decode_us) / 1000.0);
+            timing->total_execution_ms = (int64_t)(st.total_us / 1000.0);
+            timing->intermediate_ms = (int64_t)(st.intermediate_us / 1000.0);
+        }
+    } catch (const cj::Error &e) {
+        cudaStreamSynchronize(ctx->stream);
+        cudaGetLastError();
+        return set_error(e.code, e.msg);
+    } catch (const std::bad_alloc &) {
+        cudaStreamSynchronize(ctx->stream);
+        return set_error(CJ_ERR_OUT_OF_MEMORY, "host allocation failed");
+    } catch (...) {
+        cudaStreamSynchronize(ctx->stream);
+        return set_error(CJ_ERR_INTERNAL, "unexpected exception");
+    }
+    g_last_error.clear();
+    return CJ_OK;
+}
+
+int cj_result_num_rows(const cj_result *r, uint64_t *n) {
+    if (!r || !n) return set_error(CJ_ERR_INVALID_ARGUMENT, "null argument");
+    *n = r->num_rows;
+    return CJ_OK;
+}
+
+int cj_result_num_columns(const cj_result *r, uint64_t *n) {
+    if (!r || !n) return set_error(CJ_ERR_INVALID_ARGUMENT, "null argument");
+    *n = r->types.size();
+    return CJ_OK;
+}
+
+int cj_result_column(const cj_result *r, uint64_t c, int32_t *type, uint64_t *num_pages, const void **host_pages) {
+    if (!r || c >= r->types.size()) return set_error(CJ_ERR_INVALID_ARGUMENT, "bad column");
+    if (type) *type = r->types[c];
+    if (num_pages) *num_pages = r->num_pages[c];
+    if (host_pages) *host_pages = r->host_cols.empty() ? nullptr : r->host_cols[c];
+    return CJ_OK;
+}
+
+int cj_result_column_device(const cj_result *r, uint64_t c, const void **device_pages) {
+    if (!r || c >= r->types.size() || !device_pages) return set_error(CJ_ERR_INVALID_ARGUMENT, "bad column");
+    *device_pages = r->dev_pages[c] ? r->dev_pages[c]->ptr : nullptr;
+    return CJ_OK;
+}
+
+int cj_result_copy_column(const cj_result *r, uint64_t c, void *dst, uint64_t dst_bytes) {
+    if (!r || c >= r->types.size() || (!dst && r->num_pages[c]))
+        return set_error(CJ_ERR_INVALID_ARGUMENT, "bad argument");
+    const uint64_t bytes = r->num_pages[c] * CJ_PAGE_SIZE;
+    if (dst_bytes < bytes) return set_error(CJ_ERR_INVALID_ARGUMENT, "destination too small");
+    if (!bytes) return CJ_OK;
+    API_BEGIN
+    set_device(r->ctx);
+    if (!r->host_cols.empty() && r->host_cols[c]) {
+        std::memcpy(dst, r->host_cols[c], bytes);
+    } else {
+        cj::check_cuda(cudaMemcpyAsync(dst, r->dev_pages[c]->ptr, bytes, cudaMemcpyDeviceToHost, r->ctx->stream),
+                       "download");
+        cj::check_cuda(cudaStreamSynchronize(r->ctx->stream), "download");
+    }
+    API_END
+}
+
+void cj_result_free(cj_result *r) {
+    if (!r) return;
+    set_device(r->ctx);
+    delete r;
+}
+
+int cj_host_alloc(uint64_t bytes, void **out) {
+    if (!out) return set_error(CJ_ERR_INVALID_ARGUMENT, "out is null");
+    *out = nullptr;
+    cudaError_t e = cudaHostAlloc(out, bytes ? bytes : 1, cudaHostAllocPortable);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        *out = nullptr;
+        return set_error(e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver ? CJ_ERR_NO_DEVICE
+                                                                                      : CJ_ERR_OUT_OF_MEMORY,
+                         cudaGetErrorString(e));
+    }
+    return CJ_OK;
+}
+
+void cj_host_free(void *p) {
+    if (p) cudaFreeHost(p);
+}
+
+} /* extern "C" */

@@ -1,0 +1,126 @@
+/*
+ * cj_device.cuh — device helpers shared by the sm_100a kernels: hashing,
+ * Bloom tags, warp/block scans and column accessors.
+ */
+#pragma once
+
+#include <cstdint>
+
+#include "cj_internal.h"
+
+namespace cj {
+
+#define CJ_DEV __device__ __forceinline__
+
+/* 64-bit key hash: the MurmurHash3 64-bit finaliser (Austin Appleby,
+ * public domain). The reference hashes with the x86/ARM CRC32C instruction
+ * times a multiplier (include/join_execution/hashtable.h:146-154); the GPU
+ * has no CRC instruction and the hash does not change any result, only the
+ * slot a key lands in, so a multiply-xorshift finaliser is used instead.
+ * Slot = top bits (as slot_for, hashtable.h:167-169); Bloom tag index = the
+ * low 11 bits, which stay independent of the slot bits for every directory
+ * size (the reference takes bits 32..42, which overlap the slot bits once
+ * the directory exceeds 2^21 slots). */
+__host__ __device__ __forceinline__ uint64_t hash_key(int64_t key) {
+    uint64_t x = (uint64_t)key;
+    x ^= x >> 33;
+    x *= 0xff51afd7ed558ccdull;
+    x ^= x >> 33;
+    x *= 0xc4ceb9fe1a85ec53ull;
+    x ^= x >> 33;
+    return x;
+}
+
+CJ_DEV uint32_t slot_of(uint64_t h, int log2_slots) {
+    return (uint32_t)(h >> (64 - log2_slots));
+}
+
+CJ_DEV uint32_t bloom_index(uint64_t h) { return (uint32_t)(h & 0x7FFu); }
+
+/* Loads the 2048-entry Bloom tag table into shared memory. */
+CJ_DEV void load_bloom(uint16_t *s_bloom, const uint16_t *g_bloom) {
+    const uint32_t *src = reinterpret_cast<const uint32_t *>(g_bloom);
+    uint32_t *dst = reinterpret_cast<uint32_t *>(s_bloom);
+    for (int i = threadIdx.x; i < 1024; i += blockDim.x) dst[i] = src[i];
+}
+
+CJ_DEV uint32_t lane_id() { return threadIdx.x & 31u; }
+CJ_DEV uint32_t lanemask_lt() { return (1u << lane_id()) - 1u; }
+
+template <typename T> CJ_DEV T warp_inclusive_scan(T v) {
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        T o = __shfl_up_sync(0xffffffffu, v, d);
+        if ((int)lane_id() >= d) v += o;
+    }
+    return v;
+}
+
+template <typename T> CJ_DEV T warp_sum(T v) {
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) v += __shfl_xor_sync(0xffffffffu, v, d);
+    return v;
+}
+
+/* Exclusive scan over the block; `warp_buf` needs blockDim.x/32 + 1
+ * entries. Returns the exclusive prefix and the block total in *total.
+ * Contains __syncthreads(): every thread of the block must call it. */
+template <typename T> CJ_DEV T block_exclusive_scan(T v, T *warp_buf, T *total) {
+    const int warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    T incl = warp_inclusive_scan(v);
+    if (lane_id() == 31) warp_buf[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        T w = (int)lane_id() < nwarps ? warp_buf[lane_id()] : T(0);
+        T wi = warp_inclusive_scan(w);
+        if ((int)lane_id() < nwarps) warp_buf[lane_id()] = wi - w;
+        if (lane_id() == 31) warp_buf[nwarps] = wi;
+    }
+    __syncthreads();
+    T res = warp_buf[warp] + incl - v;
+    *total = warp_buf[nwarps];
+    __syncthreads();
+    return res;
+}
+
+/* Relation row -> base row through the view's indirections. */
+CJ_DEV uint32_t base_row(const ColView &c, uint32_t i) {
+    if (c.rid_a) i = __ldg(c.rid_a + i);
+    if (c.rid_b) i = __ldg(c.rid_b + i);
+    return i;
+}
+
+CJ_DEV bool valid_bit(const uint32_t *valid, uint32_t r) {
+    return (__ldg(valid + (r >> 5)) >> (r & 31)) & 1u;
+}
+
+/* Join key of relation row i as a 64-bit integer; false if NULL. */
+CJ_DEV bool load_key(const ColView &c, uint32_t i, int64_t *key) {
+    uint32_t r = base_row(c, i);
+    if (!valid_bit(c.valid, r)) return false;
+    if (c.type == CJ_INT32) {
+        int32_t v = __ldg(reinterpret_cast<const int32_t *>(c.values) + r);
+        if (c.null_sentinel && v == INT32_MIN) return false;
+        *key = v;
+    } else {
+        *key = __ldg(reinterpret_cast<const long long *>(c.values) + r);
+    }
+    return true;
+}
+
+/* Streaming variant for a dense key column read once in row order: the
+ * loads are marked evict-first so the hash table stays in L2. */
+CJ_DEV bool load_key_stream(const ColView &c, uint32_t i, int64_t *key) {
+    if (c.rid_a || c.rid_b) return load_key(c, i, key);
+    if (!((__ldcs(c.valid + (i >> 5)) >> (i & 31)) & 1u)) return false;
+    if (c.type == CJ_INT32) {
+        int32_t v = __ldcs(reinterpret_cast<const int32_t *>(c.values) + i);
+        if (c.null_sentinel && v == INT32_MIN) return false;
+        *key = v;
+    } else {
+        *key = __ldcs(reinterpret_cast<const long long *>(c.values) + i);
+    }
+    return true;
+}
+
+} // namespace cj

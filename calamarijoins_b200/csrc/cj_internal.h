@@ -1,0 +1,193 @@
+/*
+ * cj_internal.h — types shared by the host engine and the sm_100a kernels.
+ *
+ * Device data layout (all in HBM, one allocation per array):
+ *   pages        a column's 8 KiB pages, consecutive, exactly as on the host
+ *   row_start    u64[num_pages + 1], first row of each page (prefix sum of
+ *                the rows each page holds: n_rows, 1 for a long-string start
+ *                page 0xffff, 0 for a continuation page 0xfffe)
+ *   values       dense fixed-width values, one per row (0 where NULL)
+ *   valid        validity bitmap, u32 words, bit r = row r present
+ *   str_desc     VARCHAR: one u64 per row, see CJ_DESC_* below
+ *   rid vectors  u32 row ids (late materialisation of intermediates)
+ *   hash table   u64 directory ((end << 16) | 16-bit Bloom tag) and a
+ *                slot-ordered tuple array {key, row id}
+ */
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+
+#include <cuda_runtime.h>
+
+#include "../../include/cj_b200.h"
+
+namespace cj {
+
+constexpr uint32_t kPageSize = CJ_PAGE_SIZE;
+constexpr uint32_t kMaxShortString = kPageSize - 7; /* plan.h:331 */
+constexpr uint32_t kLongChunk = kPageSize - 4;      /* plan.h:301 */
+constexpr uint32_t kRowsPerPageInt32 = 1984;        /* ColumnInserter<int32_t> fill */
+constexpr uint32_t kRowsPerPage8B = 1007;           /* ColumnInserter<int64_t/double> */
+
+/* VARCHAR row descriptor.
+ *   short string: bit 63 = 0, bits 62..24 = byte offset of the first
+ *                 character inside the column's page blob, bits 23..0 =
+ *                 length (<= 8185)
+ *   long string:  bit 63 = 1, bits 62..24 = index of its 0xffff page,
+ *                 bits 23..0 = number of pages in the chain (the 0xffff
+ *                 page and the 0xfffe pages that follow it)
+ *   NULL rows hold 0 (the validity bitmap says NULL). */
+constexpr uint64_t CJ_DESC_LONG = 1ull << 63;
+__host__ __device__ inline uint64_t desc_short(uint64_t off, uint32_t len) {
+    return (off << 24) | len;
+}
+__host__ __device__ inline uint64_t desc_long(uint64_t page, uint32_t chain) {
+    return CJ_DESC_LONG | (page << 24) | chain;
+}
+__host__ __device__ inline bool desc_is_long(uint64_t d) { return (d >> 63) != 0; }
+__host__ __device__ inline uint64_t desc_pos(uint64_t d) { return (d >> 24) & ((1ull << 39) - 1); }
+__host__ __device__ inline uint32_t desc_len(uint64_t d) { return (uint32_t)(d & 0xFFFFFFu); }
+
+/* Error bits the kernels raise in the device status word. */
+enum DevError : uint32_t {
+    DEV_ERR_PAGE_HEADER = 1u << 0,   /* n_values > n_rows or page overflow */
+    DEV_ERR_VARCHAR_OFFSETS = 1u << 1,
+    DEV_ERR_LONG_CHAIN = 1u << 2,    /* 0xfffe page without a 0xffff start */
+    DEV_ERR_BAD_PAGE_KIND = 1u << 3, /* 0xffff/0xfffe page in a fixed column */
+    DEV_ERR_LOOKBACK = 1u << 4,      /* a tile's look-back wait gave up      */
+    DEV_ERR_ROW_COUNT = 1u << 5,     /* pages hold more/fewer rows than the
+                                        table declares                       */
+    DEV_ERR_INTERNAL = 1u << 31
+};
+
+/* Small pinned block the host reads at each synchronisation point. */
+struct StatusBlock {
+    unsigned int errors;          /* DevError bits                          */
+    unsigned int pad;
+    unsigned long long counter;   /* match counter of the last probe        */
+    unsigned long long aux[6];    /* scratch totals (pages, rows)           */
+};
+
+/* How a kernel reads one column of a relation: row i of the relation is
+ * row rid_b[rid_a[i]] of the decoded base column (each indirection is
+ * skipped when its pointer is null). */
+struct ColView {
+    const void *values;
+    const uint32_t *valid;
+    const uint64_t *str_desc;
+    const uint8_t *pages;
+    const uint32_t *rid_a;
+    const uint32_t *rid_b;
+    int32_t type;
+    int32_t null_sentinel; /* INT32: INT32_MIN reads as NULL (value_t) */
+};
+
+template <typename K> struct Tuple;
+template <> struct alignas(8) Tuple<int32_t> {
+    int32_t key;
+    uint32_t rid;
+};
+template <> struct alignas(16) Tuple<int64_t> {
+    int64_t key;
+    uint32_t rid;
+    uint32_t pad;
+};
+
+template <typename K> struct HashTableView {
+    const uint64_t *dir;
+    const Tuple<K> *tuples;
+    int log2_slots;
+};
+
+/* Output of a probe / nested-loop launch. */
+struct MatchOut {
+    uint32_t *build_rids; /* null: not collected (RIGHT_ONLY)           */
+    uint32_t *probe_rids; /* null: not collected (LEFT_ONLY)            */
+    unsigned long long capacity;
+    unsigned long long *counter;
+};
+
+/* Kernels launched by this process (every launcher adds its launches). */
+void count_launches(uint64_t n);
+uint64_t launches_so_far();
+
+/* ----------------------------------------------------------------------- */
+/* Kernel launchers (defined in the .cu files; all enqueue on `s`).         */
+/* ----------------------------------------------------------------------- */
+struct Launch {
+    cudaStream_t stream;
+    int num_sms;
+    int block_threads; /* 0 = kernel default */
+    unsigned int *dev_errors;
+};
+
+/* Scan */
+size_t scan_temp_bytes(size_t n);
+/* out[i] = sum(in[0..i)), out[n] = total; in and out may not alias. */
+cudaError_t scan_u32_to_u64(const Launch &L, const uint32_t *in, uint64_t *out,
+                            size_t n, void *temp);
+
+/* Decode */
+cudaError_t launch_page_rows(const Launch &L, const uint8_t *pages,
+                             uint64_t num_pages, int32_t type,
+                             uint32_t *rows_per_page);
+/* Rows past max_rows are never written; a page that would write them
+ * raises DEV_ERR_ROW_COUNT instead. */
+cudaError_t launch_decode_fixed(const Launch &L, const uint8_t *pages,
+                                uint64_t num_pages, int32_t type,
+                                const uint64_t *row_start, uint64_t max_rows,
+                                void *values, uint32_t *valid);
+cudaError_t launch_decode_varchar(const Launch &L, const uint8_t *pages,
+                                  uint64_t num_pages,
+                                  const uint64_t *row_start, uint64_t max_rows,
+                                  uint64_t *desc, uint32_t *valid);
+/* Raises DEV_ERR_ROW_COUNT unless *total == expected. */
+cudaError_t launch_check_rows(const Launch &L, const uint64_t *total, uint64_t expected);
+
+/* Build */
+struct BuildPlan {
+    int log2_slots;      /* directory = 2^log2_slots u64 entries          */
+    int log2_parts;      /* radix partitions                              */
+    uint32_t num_rows;   /* rows of the build relation                    */
+};
+size_t build_temp_bytes(const Launch &L, const BuildPlan &bp, int key_bytes);
+size_t build_tuple_bytes(int key_bytes);
+cudaError_t launch_build(const Launch &L, const BuildPlan &bp, const ColView &key,
+                         const uint16_t *bloom, uint64_t *dir, void *tuples,
+                         void *temp);
+
+/* Probe and nested loop share one tiled kernel; `sched` is scratch of
+ * probe_sched_bytes(n_probe) bytes (tile tickets and look-back status). */
+size_t probe_sched_bytes(uint32_t n_probe);
+cudaError_t launch_probe_tiles_hash(const Launch &L, const ColView &pkey, uint32_t n_probe,
+                                    int32_t build_key_type, const uint64_t *dir,
+                                    const void *tuples, int log2_slots, const uint16_t *bloom,
+                                    const MatchOut &out, void *sched);
+
+/* Nested loop (build side <= 64 rows) */
+constexpr uint32_t kNestedLoopMax = 64;
+cudaError_t launch_nl_collect(const Launch &L, const ColView &bkey, uint32_t n_build,
+                              int64_t *keys, uint32_t *rids, uint32_t *count);
+cudaError_t launch_nl_probe_tiles(const Launch &L, const ColView &pkey, uint32_t n_probe,
+                                  const int64_t *keys, const uint32_t *rids,
+                                  const uint32_t *count, const MatchOut &out, void *sched);
+
+/* Intermediates: out[i] = src[idx[i]] */
+cudaError_t launch_gather_u32(const Launch &L, const uint32_t *src,
+                              const uint32_t *idx, uint64_t n, uint32_t *out);
+
+/* Output pages */
+uint32_t rows_per_page_fixed(int32_t type);
+cudaError_t launch_write_fixed_pages(const Launch &L, const ColView &col,
+                                     uint64_t rows, uint8_t *out_pages);
+size_t varchar_temp_bytes(uint64_t rows, uint32_t tile_rows);
+/* Pass 1: page count per tile; total pages into *total_pages_dev. */
+cudaError_t launch_varchar_plan(const Launch &L, const ColView &col, uint64_t rows,
+                                uint32_t tile_rows, void *temp,
+                                unsigned long long *total_pages_dev);
+/* Pass 2: write pages (out_pages sized by pass 1's total). */
+cudaError_t launch_varchar_write(const Launch &L, const ColView &col, uint64_t rows,
+                                 uint32_t tile_rows, void *temp, uint8_t *out_pages);
+
+} // namespace cj

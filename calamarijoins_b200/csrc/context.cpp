@@ -1,0 +1,204 @@
+/*
+ * context.cpp — context resources: stream-ordered device pool, pinned
+ * pool, events, status block, page upload.
+ */
+#include <cstring>
+#include <string>
+
+#include "engine.h"
+
+#include <atomic>
+
+namespace cj {
+
+static std::atomic<uint64_t> g_launches{0};
+void count_launches(uint64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+uint64_t launches_so_far() { return g_launches.load(std::memory_order_relaxed); }
+
+void fail(int code, const std::string &msg) { throw Error{code, msg}; }
+
+void check_cuda(cudaError_t e, const char *what) {
+    if (e == cudaSuccess) return;
+    int code = (e == cudaErrorMemoryAllocation) ? CJ_ERR_OUT_OF_MEMORY : CJ_ERR_CUDA;
+    fail(code, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+DevBuf::~DevBuf() {
+    if (ptr && ctx) cudaFreeAsync(ptr, ctx->stream);
+}
+
+PinnedBlock::~PinnedBlock() {
+    if (!ptr || !ctx) return;
+    std::lock_guard<std::mutex> g(ctx->pinned_mu);
+    ctx->pinned_free.emplace(bytes, ptr);
+}
+
+DevPtr Context::alloc(size_t bytes) {
+    auto b = std::make_shared<DevBuf>();
+    b->ctx = this;
+    b->bytes = bytes;
+    if (bytes == 0) return b;
+    size_t req = (bytes + 255) & ~size_t(255);
+    cudaError_t e = cudaMallocFromPoolAsync(&b->ptr, req, pool, stream);
+    if (e != cudaSuccess) {
+        b->ptr = nullptr;
+        cudaGetLastError();
+        fail(CJ_ERR_OUT_OF_MEMORY, "device allocation of " + std::to_string(bytes) + " bytes failed");
+    }
+    return b;
+}
+
+static size_t pinned_class(size_t bytes) {
+    size_t c = 1u << 20;
+    while (c < bytes) c <<= 1;
+    return c;
+}
+
+PinnedPtr Context::alloc_pinned(size_t bytes) {
+    auto b = std::make_shared<PinnedBlock>();
+    b->ctx = this;
+    if (bytes == 0) return b;
+    size_t cls = pinned_class(bytes);
+    {
+        std::lock_guard<std::mutex> g(pinned_mu);
+        auto it = pinned_free.find(cls);
+        if (it != pinned_free.end()) {
+            b->ptr = it->second;
+            b->bytes = cls;
+            pinned_free.erase(it);
+            return b;
+        }
+    }
+    void *p = nullptr;
+    cudaError_t e = cudaHostAlloc(&p, cls, cudaHostAllocDefault);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        fail(CJ_ERR_OUT_OF_MEMORY, "pinned allocation of " + std::to_string(cls) + " bytes failed");
+    }
+    b->ptr = p;
+    b->bytes = cls;
+    return b;
+}
+
+cudaEvent_t Context::get_event() {
+    if (!event_pool.empty()) {
+        cudaEvent_t e = event_pool.back();
+        event_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e;
+    check_cuda(cudaEventCreate(&e), "cudaEventCreate");
+    return e;
+}
+
+void Context::put_event(cudaEvent_t e) { event_pool.push_back(e); }
+
+void Context::sync_status() {
+    check_cuda(cudaMemcpyAsync(h_status, d_status, sizeof(StatusBlock), cudaMemcpyDeviceToHost, stream),
+               "status copy");
+    check_cuda(cudaStreamSynchronize(stream), "stream synchronize");
+    unsigned int err = h_status->errors;
+    if (err) {
+        /* clear for the next call */
+        cudaMemsetAsync(&d_status->errors, 0, sizeof(unsigned int), stream);
+        cudaStreamSynchronize(stream);
+        std::string what;
+        if (err & DEV_ERR_PAGE_HEADER) what += " page header inconsistent;";
+        if (err & DEV_ERR_VARCHAR_OFFSETS) what += " VARCHAR offsets out of range;";
+        if (err & DEV_ERR_LONG_CHAIN) what += " long-string continuation without start;";
+        if (err & DEV_ERR_BAD_PAGE_KIND) what += " special page in fixed-width column;";
+        if (err & DEV_ERR_ROW_COUNT) what += " pages hold a row count other than the table's;";
+        if (err & DEV_ERR_LOOKBACK) what += " tile look-back wait gave up;";
+        if (err & DEV_ERR_INTERNAL) what += " internal;";
+        int code = (err & (DEV_ERR_LOOKBACK | DEV_ERR_INTERNAL)) ? CJ_ERR_INTERNAL : CJ_ERR_MALFORMED_PAGE;
+        fail(code, "device reported:" + what);
+    }
+}
+
+void Context::resolve_profile() {
+    for (auto &p : pending) {
+        float ms = 0;
+        if (cudaEventElapsedTime(&ms, p.a, p.b) == cudaSuccess) {
+            profile[p.slot].launches += 1;
+            profile[p.slot].total_us += ms * 1000.0;
+        }
+        put_event(p.a);
+        put_event(p.b);
+    }
+    pending.clear();
+    cudaGetLastError();
+}
+
+Context::~Context() {
+    if (stream) cudaStreamSynchronize(stream);
+    for (auto &p : pending) {
+        cudaEventDestroy(p.a);
+        cudaEventDestroy(p.b);
+    }
+    for (auto e : event_pool) cudaEventDestroy(e);
+    for (int i = 0; i < 2; ++i) {
+        if (staging_ev[i]) cudaEventDestroy(staging_ev[i]);
+        if (staging[i]) cudaFreeHost(staging[i]);
+    }
+    for (auto &kv : pinned_free) cudaFreeHost(kv.second);
+    if (h_status) cudaFreeHost(h_status);
+    if (d_status) cudaFree(d_status);
+    if (d_bloom) cudaFree(d_bloom);
+    if (pool) cudaMemPoolDestroy(pool);
+    if (stream) cudaStreamDestroy(stream);
+}
+
+/* Host pages -> one consecutive device array. A run of pages that are
+ * already consecutive in host memory goes in one cudaMemcpyAsync (full PCIe
+ * speed when the memory is page-locked); scattered pages are gathered into
+ * one of two pinned staging buffers while the other is in flight. */
+void upload_pages(Context &ctx, const cj_column_desc &cd, ColumnPages &out, uint64_t *h2d_bytes) {
+    out.type = cd.type;
+    out.num_pages = cd.num_pages;
+    if (cd.num_pages == 0) return;
+    if (!cd.pages) fail(CJ_ERR_INVALID_ARGUMENT, "column has pages but no page array");
+    const size_t P = kPageSize;
+    out.owner = ctx.alloc(cd.num_pages * P);
+    uint8_t *dev = out.owner->as<uint8_t>();
+    out.dev = dev;
+    const uint64_t per_buf = ctx.staging_bytes / P;
+    int buf = 0;
+    uint64_t fill = 0, fill_first = 0;
+    auto flush = [&]() {
+        if (!fill) return;
+        check_cuda(cudaMemcpyAsync(dev + fill_first * P, ctx.staging[buf], fill * P, cudaMemcpyHostToDevice,
+                                   ctx.stream),
+                   "page upload");
+        check_cuda(cudaEventRecord(ctx.staging_ev[buf], ctx.stream), "event record");
+        buf ^= 1;
+        fill = 0;
+    };
+    uint64_t i = 0;
+    const uint64_t np = cd.num_pages;
+    while (i < np) {
+        const uint8_t *p0 = static_cast<const uint8_t *>(cd.pages[i]);
+        if (!p0) fail(CJ_ERR_INVALID_ARGUMENT, "null page pointer");
+        uint64_t j = i + 1;
+        while (j < np && static_cast<const uint8_t *>(cd.pages[j]) == p0 + (j - i) * P) ++j;
+        const uint64_t run = j - i;
+        if (run * P >= (1u << 20)) {
+            flush();
+            check_cuda(cudaMemcpyAsync(dev + i * P, p0, run * P, cudaMemcpyHostToDevice, ctx.stream),
+                       "page upload");
+        } else {
+            for (uint64_t k = i; k < j; ++k) {
+                if (fill == 0) {
+                    check_cuda(cudaEventSynchronize(ctx.staging_ev[buf]), "staging wait");
+                    fill_first = k;
+                }
+                std::memcpy(static_cast<uint8_t *>(ctx.staging[buf]) + fill * P, cd.pages[k], P);
+                if (++fill == per_buf) flush();
+            }
+        }
+        i = j;
+    }
+    flush();
+    if (h2d_bytes) *h2d_bytes += np * P;
+}
+
+} // namespace cj

@@ -1,0 +1,561 @@
+/*
+ * engine.cpp — plan executor: the depth-first join recursion of the
+ * reference (src/execute.cpp:84-325) over device-resident relations.
+ *
+ * A relation is either a scan (rows are base-table rows) or the output of
+ * a join. Join outputs are late-materialised: instead of copying values
+ * (construct_intermediate.h:121-220) a join output keeps one u32 row-id
+ * vector per contributing base table, and each of its columns names its
+ * base column and the vector that reaches it. Values are read only by the
+ * kernels that need them: join keys by build/probe, projected columns by
+ * the root's page writers.
+ */
+#include <algorithm>
+#include <chrono>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "engine.h"
+
+namespace cj {
+namespace {
+
+int ceil_log2(uint64_t x) {
+    int l = 0;
+    while ((1ull << l) < x) ++l;
+    return l;
+}
+
+struct Decoded {
+    int32_t type = CJ_INT32;
+    uint64_t rows = 0;
+    ColumnPages src;
+    DevPtr values, valid, desc;
+};
+
+/* A column of a relation: base column (input, col) reached through row-id
+ * vector `vec` of the relation (-1: the relation row is the base row). */
+struct RelCol {
+    int32_t type;
+    uint64_t input;
+    uint64_t col;
+    int vec;
+    bool sentinel; /* value left a non-root join: INT32_MIN reads as NULL */
+};
+
+struct Relation {
+    uint64_t rows = 0;
+    std::vector<DevPtr> vecs;
+    std::vector<RelCol> cols;
+};
+
+enum Phase { PH_UPLOAD, PH_DECODE, PH_BUILD, PH_PROBE, PH_NL, PH_INTER, PH_MAT, PH_DOWNLOAD, PH_COUNT };
+
+class Executor {
+  public:
+    Executor(Context &c, const cj_plan_desc &p, uint32_t f) : ctx(c), plan(p), flags(f), L(c.launch()) {}
+    ~Executor() {
+        for (auto &pe : phase_events) {
+            ctx.put_event(pe.a);
+            ctx.put_event(pe.b);
+        }
+    }
+    cj_result *run(cj_exec_stats *st);
+
+  private:
+    struct PhaseEv {
+        int phase;
+        cudaEvent_t a, b;
+    };
+    class PhaseScope {
+      public:
+        PhaseScope(Executor &e, int ph) : e_(e), ph_(ph) {
+            a_ = e.ctx.get_event();
+            cudaEventRecord(a_, e.ctx.stream);
+        }
+        ~PhaseScope() {
+            cudaEvent_t b = e_.ctx.get_event();
+            cudaEventRecord(b, e_.ctx.stream);
+            e_.phase_events.push_back({ph_, a_, b});
+        }
+
+      private:
+        Executor &e_;
+        int ph_;
+        cudaEvent_t a_;
+    };
+    /* Per-kernel timing when profiling is on. */
+    class KScope {
+      public:
+        KScope(Executor &e, const char *name) : e_(e) {
+            if (!e.ctx.opt.profile_kernels) return;
+            auto it = e.ctx.profile_index.find(name);
+            if (it == e.ctx.profile_index.end()) {
+                slot_ = e.ctx.profile.size();
+                e.ctx.profile.push_back({name, 0, 0.0});
+                e.ctx.profile_index[name] = slot_;
+            } else {
+                slot_ = it->second;
+            }
+            a_ = e.ctx.get_event();
+            cudaEventRecord(a_, e.ctx.stream);
+            on_ = true;
+        }
+        ~KScope() {
+            if (!on_) return;
+            cudaEvent_t b = e_.ctx.get_event();
+            cudaEventRecord(b, e_.ctx.stream);
+            e_.ctx.pending.push_back({slot_, a_, b});
+        }
+
+      private:
+        Executor &e_;
+        size_t slot_ = 0;
+        cudaEvent_t a_ = nullptr;
+        bool on_ = false;
+    };
+
+    Context &ctx;
+    const cj_plan_desc &plan;
+    uint32_t flags;
+    Launch L;
+    std::map<std::pair<uint64_t, uint64_t>, Decoded> decoded;
+    std::vector<PhaseEv> phase_events;
+    cj_exec_stats stats{};
+
+    const cj_table *resident(uint64_t t) const {
+        return plan.resident_inputs ? plan.resident_inputs[t] : nullptr;
+    }
+    uint64_t table_rows(uint64_t t) const {
+        const cj_table *r = resident(t);
+        return r ? r->num_rows : plan.inputs[t].num_rows;
+    }
+    uint64_t table_cols(uint64_t t) const {
+        const cj_table *r = resident(t);
+        return r ? r->cols.size() : plan.inputs[t].num_columns;
+    }
+    int32_t column_type(uint64_t t, uint64_t c) const {
+        const cj_table *r = resident(t);
+        return r ? r->cols[c].type : plan.inputs[t].columns[c].type;
+    }
+
+    void validate();
+    Decoded &decode(uint64_t t, uint64_t c);
+    Relation scan_relation(const cj_plan_node &n);
+    Relation resolve(uint64_t node, int depth);
+    Relation exec_join(uint64_t node, int depth, bool is_root, cj_result **out);
+    ColView view(const Relation &R, const RelCol &c, const uint32_t *rid_a);
+    cj_result *materialize(const std::vector<ColView> &cols, const std::vector<int32_t> &types,
+                           uint64_t rows);
+    void ck(cudaError_t e, const char *what) { check_cuda(e, what); }
+};
+
+void Executor::validate() {
+    if (plan.num_nodes == 0 || !plan.nodes) fail(CJ_ERR_INVALID_PLAN, "plan has no nodes");
+    if (plan.root >= plan.num_nodes) fail(CJ_ERR_INVALID_PLAN, "root index out of range");
+    if (plan.num_inputs && !plan.inputs && !plan.resident_inputs)
+        fail(CJ_ERR_INVALID_PLAN, "plan has inputs but no input tables");
+    for (uint64_t t = 0; t < plan.num_inputs; ++t) {
+        const cj_table *r = resident(t);
+        if (!r && !plan.inputs) fail(CJ_ERR_INVALID_PLAN, "input " + std::to_string(t) + " missing");
+        if (r && r->ctx != &ctx) fail(CJ_ERR_INVALID_ARGUMENT, "resident table from another context");
+        if (!r) {
+            const cj_table_desc &td = plan.inputs[t];
+            if (td.num_columns && !td.columns) fail(CJ_ERR_INVALID_PLAN, "table without column array");
+            for (uint64_t c = 0; c < td.num_columns; ++c)
+                if (td.columns[c].type < CJ_INT32 || td.columns[c].type > CJ_VARCHAR)
+                    fail(CJ_ERR_INVALID_PLAN, "unknown column type");
+        }
+    }
+    for (uint64_t i = 0; i < plan.num_nodes; ++i) {
+        const cj_plan_node &n = plan.nodes[i];
+        if (n.num_output_attrs && !n.output_attrs) fail(CJ_ERR_INVALID_PLAN, "node without attr array");
+        for (uint64_t a = 0; a < n.num_output_attrs; ++a)
+            if (n.output_attrs[a].type < CJ_INT32 || n.output_attrs[a].type > CJ_VARCHAR)
+                fail(CJ_ERR_INVALID_PLAN, "unknown attribute type");
+        if (n.node_type == CJ_NODE_SCAN) {
+            if (n.base_table_id >= plan.num_inputs) fail(CJ_ERR_INVALID_PLAN, "scan of missing table");
+            for (uint64_t a = 0; a < n.num_output_attrs; ++a) {
+                const cj_attr &at = n.output_attrs[a];
+                if (at.index >= table_cols(n.base_table_id)) fail(CJ_ERR_INVALID_PLAN, "scan column out of range");
+                if (column_type(n.base_table_id, at.index) != at.type)
+                    fail(CJ_ERR_INVALID_PLAN, "scan attribute type differs from column type");
+            }
+        } else if (n.node_type == CJ_NODE_HASH_JOIN) {
+            if (n.left >= plan.num_nodes || n.right >= plan.num_nodes)
+                fail(CJ_ERR_INVALID_PLAN, "join child out of range");
+        } else {
+            fail(CJ_ERR_INVALID_PLAN, "unknown node type");
+        }
+    }
+}
+
+Decoded &Executor::decode(uint64_t t, uint64_t c) {
+    auto key = std::make_pair(t, c);
+    auto it = decoded.find(key);
+    if (it != decoded.end()) return it->second;
+    Decoded d;
+    d.type = column_type(t, c);
+    d.rows = table_rows(t);
+    if (d.rows > 0xFFFFFFFFull) fail(CJ_ERR_LIMIT, "table exceeds 2^32-1 rows (u32 row ids)");
+    if (const cj_table *r = resident(t)) {
+        d.src = r->cols[c];
+    } else {
+        PhaseScope ph(*this, PH_UPLOAD);
+        upload_pages(ctx, plan.inputs[t].columns[c], d.src, &stats.h2d_bytes);
+    }
+    PhaseScope ph(*this, PH_DECODE);
+    const uint64_t np = d.src.num_pages;
+    DevPtr rows_pp = ctx.alloc(std::max<uint64_t>(np, 1) * 4);
+    DevPtr row_start = ctx.alloc((np + 1) * 8);
+    DevPtr scan_tmp = ctx.alloc(scan_temp_bytes(np));
+    {
+        KScope k(*this, "page_rows");
+        ck(launch_page_rows(L, d.src.dev, np, d.type, rows_pp->as<uint32_t>()), "page_rows");
+    }
+    {
+        KScope k(*this, "scan");
+        ck(scan_u32_to_u64(L, rows_pp->as<uint32_t>(), row_start->as<uint64_t>(), np, scan_tmp->ptr), "scan");
+    }
+    ck(launch_check_rows(L, row_start->as<uint64_t>() + np, d.rows), "check_rows");
+    const uint64_t words = (d.rows + 31) / 32;
+    d.valid = ctx.alloc(std::max<uint64_t>(words, 1) * 4);
+    ck(cudaMemsetAsync(d.valid->ptr, 0, std::max<uint64_t>(words, 1) * 4, ctx.stream), "memset");
+    if (d.type == CJ_VARCHAR) {
+        d.desc = ctx.alloc(d.rows * 8);
+        KScope k(*this, "decode_varchar");
+        ck(launch_decode_varchar(L, d.src.dev, np, row_start->as<uint64_t>(), d.rows, d.desc->as<uint64_t>(),
+                                 d.valid->as<uint32_t>()),
+           "decode_varchar");
+    } else {
+        const uint64_t w = d.type == CJ_INT32 ? 4 : 8;
+        d.values = ctx.alloc(d.rows * w);
+        KScope k(*this, d.type == CJ_INT32 ? "decode_int32" : "decode_8byte");
+        ck(launch_decode_fixed(L, d.src.dev, np, d.type, row_start->as<uint64_t>(), d.rows, d.values->ptr,
+                               d.valid->as<uint32_t>()),
+           "decode_fixed");
+    }
+    return decoded.emplace(key, std::move(d)).first->second;
+}
+
+ColView Executor::view(const Relation &R, const RelCol &c, const uint32_t *rid_a) {
+    Decoded &d = decode(c.input, c.col);
+    ColView v{};
+    v.type = c.type;
+    v.values = d.values ? d.values->ptr : nullptr;
+    v.valid = d.valid->as<uint32_t>();
+    v.str_desc = d.desc ? d.desc->as<uint64_t>() : nullptr;
+    v.pages = d.src.dev;
+    v.rid_a = rid_a;
+    v.rid_b = c.vec >= 0 ? R.vecs[c.vec]->as<uint32_t>() : nullptr;
+    v.null_sentinel = (c.sentinel && c.type == CJ_INT32) ? 1 : 0;
+    return v;
+}
+
+Relation Executor::scan_relation(const cj_plan_node &n) {
+    Relation r;
+    r.rows = table_rows(n.base_table_id);
+    for (uint64_t a = 0; a < n.num_output_attrs; ++a)
+        r.cols.push_back({n.output_attrs[a].type, n.base_table_id, n.output_attrs[a].index, -1, false});
+    return r;
+}
+
+Relation Executor::resolve(uint64_t node, int depth) {
+    if (depth > (int)plan.num_nodes) fail(CJ_ERR_INVALID_PLAN, "plan has a cycle");
+    const cj_plan_node &n = plan.nodes[node];
+    if (n.node_type == CJ_NODE_SCAN) return scan_relation(n);
+    return exec_join(node, depth, false, nullptr);
+}
+
+Relation Executor::exec_join(uint64_t node_idx, int depth, bool is_root, cj_result **out) {
+    const cj_plan_node &n = plan.nodes[node_idx];
+    Relation Lr = resolve(n.left, depth + 1);
+    Relation Rr = resolve(n.right, depth + 1);
+
+    /* select_build_probe_side (join_setup.h:108-136): the smaller relation
+     * builds, left wins ties; the plan's build_left hint is not used. */
+    const bool build_left = Lr.rows <= Rr.rows;
+    Relation &B = build_left ? Lr : Rr;
+    Relation &P = build_left ? Rr : Lr;
+    const uint64_t battr = build_left ? n.left_attr : n.right_attr;
+    const uint64_t pattr = build_left ? n.right_attr : n.left_attr;
+    if (battr >= B.cols.size() || pattr >= P.cols.size()) fail(CJ_ERR_INVALID_PLAN, "join key index out of range");
+    const RelCol bk = B.cols[battr], pk = P.cols[pattr];
+    auto key_ok = [](int32_t t) { return t == CJ_INT32 || t == CJ_INT64; };
+    if (!key_ok(bk.type) || !key_ok(pk.type)) fail(CJ_ERR_UNSUPPORTED, "join keys must be INT32 or INT64");
+    if (B.rows > 0xFFFFFFFFull || P.rows > 0xFFFFFFFFull) fail(CJ_ERR_LIMIT, "relation exceeds 2^32-1 rows");
+
+    /* Output columns over (left ++ right) and which match side each needs
+     * (determine_collection_mode, join_setup.h:146-173). */
+    struct OutRef {
+        bool from_build;
+        const Relation *rel;
+        RelCol col;
+    };
+    std::vector<OutRef> outs;
+    bool need_b = false, need_p = false;
+    const uint64_t lsz = Lr.cols.size();
+    for (uint64_t a = 0; a < n.num_output_attrs; ++a) {
+        const cj_attr &at = n.output_attrs[a];
+        if (at.index >= lsz + Rr.cols.size()) fail(CJ_ERR_INVALID_PLAN, "output attribute out of range");
+        const Relation *side = at.index < lsz ? &Lr : &Rr;
+        const RelCol &c = side->cols[at.index < lsz ? at.index : at.index - lsz];
+        if (c.type != at.type) fail(CJ_ERR_INVALID_PLAN, "output attribute type differs from its column");
+        bool fb = side == &B;
+        need_b |= fb;
+        need_p |= !fb;
+        outs.push_back({fb, side, c});
+    }
+
+    stats.num_joins++;
+    stats.probe_rows += P.rows;
+    uint64_t M = 0;
+    DevPtr mb, mp;
+    if (B.rows && P.rows) {
+        const ColView bv = view(B, bk, nullptr);
+        const ColView pv = view(P, pk, nullptr);
+        const uint64_t nl_max = std::min<int64_t>(std::max<int64_t>(ctx.opt.nested_loop_max_build, 0), kNestedLoopMax);
+        const bool nl = B.rows <= nl_max;
+        DevPtr dir, tuples, nlk, nlr, nlc;
+        int log2_slots = 0;
+        if (nl) {
+            stats.num_nested_loop_joins++;
+            PhaseScope ph(*this, PH_NL);
+            nlk = ctx.alloc(kNestedLoopMax * 8);
+            nlr = ctx.alloc(kNestedLoopMax * 4);
+            nlc = ctx.alloc(4);
+            KScope k(*this, "nl_collect");
+            ck(launch_nl_collect(L, bv, (uint32_t)B.rows, nlk->as<int64_t>(), nlr->as<uint32_t>(),
+                                 nlc->as<uint32_t>()),
+               "nl_collect");
+        } else {
+            stats.num_hash_joins++;
+            PhaseScope ph(*this, PH_BUILD);
+            BuildPlan bp;
+            bp.num_rows = (uint32_t)B.rows;
+            bp.log2_slots = std::max(11, ceil_log2(B.rows)); /* hashtable.h:255-264 */
+            int log2_spp = 11;
+            if (ctx.opt.slots_per_partition > 0) log2_spp = ceil_log2((uint64_t)ctx.opt.slots_per_partition);
+            log2_spp = std::min(log2_spp, bp.log2_slots);
+            bp.log2_parts = std::min(bp.log2_slots - log2_spp, 12);
+            if (bp.log2_slots - bp.log2_parts > 14)
+                fail(CJ_ERR_LIMIT, "build side too large for one radix pass (max 2^26 rows)");
+            log2_slots = bp.log2_slots;
+            const int kb = bk.type == CJ_INT32 ? 4 : 8;
+            dir = ctx.alloc((1ull << bp.log2_slots) * 8);
+            tuples = ctx.alloc(B.rows * build_tuple_bytes(kb));
+            DevPtr tmp = ctx.alloc(build_temp_bytes(L, bp, kb));
+            KScope k(*this, "build");
+            ck(launch_build(L, bp, bv, ctx.d_bloom, dir->as<uint64_t>(), tuples->ptr, tmp->ptr), "build");
+        }
+        uint64_t cap = P.rows;
+        for (int attempt = 0; attempt < 2; ++attempt) {
+            mb = need_b ? ctx.alloc(cap * 4) : nullptr;
+            mp = need_p ? ctx.alloc(cap * 4) : nullptr;
+            MatchOut mo;
+            mo.build_rids = mb ? mb->as<uint32_t>() : nullptr;
+            mo.probe_rids = mp ? mp->as<uint32_t>() : nullptr;
+            mo.capacity = (need_b || need_p) ? cap : 0;
+            mo.counter = &ctx.d_status->counter;
+            DevPtr sched = ctx.alloc(probe_sched_bytes((uint32_t)P.rows));
+            {
+                PhaseScope ph(*this, nl ? PH_NL : PH_PROBE);
+                if (nl) {
+                    KScope k(*this, "nl_probe");
+                    ck(launch_nl_probe_tiles(L, pv, (uint32_t)P.rows, nlk->as<int64_t>(), nlr->as<uint32_t>(),
+                                             nlc->as<uint32_t>(), mo, sched->ptr),
+                       "nl_probe");
+                } else {
+                    KScope k(*this, "probe_hash");
+                    ck(launch_probe_tiles_hash(L, pv, (uint32_t)P.rows, bk.type, dir->as<uint64_t>(), tuples->ptr,
+                                               log2_slots, ctx.d_bloom, mo, sched->ptr),
+                       "probe");
+                }
+            }
+            ctx.sync_status();
+            M = ctx.h_status->counter;
+            if (M <= cap || !(need_b || need_p)) break;
+            if (M > 0xFFFFFFFFull) fail(CJ_ERR_LIMIT, "join result exceeds 2^32-1 rows");
+            stats.probe_reruns++;
+            cap = M;
+        }
+    }
+    if (M > 0xFFFFFFFFull) fail(CJ_ERR_LIMIT, "join result exceeds 2^32-1 rows");
+    stats.matches += M;
+
+    if (is_root) {
+        std::vector<ColView> cols;
+        std::vector<int32_t> types;
+        for (auto &o : outs) {
+            const uint32_t *ra = o.from_build ? (mb ? mb->as<uint32_t>() : nullptr) : (mp ? mp->as<uint32_t>() : nullptr);
+            cols.push_back(view(*o.rel, o.col, ra));
+            types.push_back(o.col.type);
+        }
+        *out = materialize(cols, types, M);
+        return Relation{};
+    }
+
+    /* Intermediate: one row-id vector per (side, source vector). */
+    Relation res;
+    res.rows = M;
+    std::map<std::pair<int, int>, int> vecmap;
+    PhaseScope ph(*this, PH_INTER);
+    for (auto &o : outs) {
+        const int side = o.from_build ? 0 : 1;
+        auto key = std::make_pair(side, o.col.vec);
+        auto it = vecmap.find(key);
+        int vi;
+        if (it != vecmap.end()) {
+            vi = it->second;
+        } else {
+            const DevPtr &match = o.from_build ? mb : mp;
+            DevPtr nv;
+            if (M == 0) {
+                nv = ctx.alloc(0);
+            } else if (o.col.vec < 0) {
+                nv = match; /* scan side: the match row ids are base rows */
+            } else {
+                nv = ctx.alloc(M * 4);
+                KScope k(*this, "gather_rids");
+                ck(launch_gather_u32(L, o.rel->vecs[o.col.vec]->as<uint32_t>(), match->as<uint32_t>(), M,
+                                     nv->as<uint32_t>()),
+                   "gather");
+            }
+            vi = (int)res.vecs.size();
+            res.vecs.push_back(nv);
+            vecmap[key] = vi;
+        }
+        res.cols.push_back({o.col.type, o.col.input, o.col.col, vi, true});
+    }
+    return res;
+}
+
+cj_result *Executor::materialize(const std::vector<ColView> &cols, const std::vector<int32_t> &types,
+                                 uint64_t rows) {
+    auto *res = new cj_result;
+    std::unique_ptr<cj_result> guard(res);
+    res->ctx = &ctx;
+    res->num_rows = rows;
+    res->types = types;
+    const size_t nc = cols.size();
+    res->num_pages.assign(nc, 0);
+    res->dev_pages.resize(nc);
+    {
+        PhaseScope ph(*this, PH_MAT);
+        const uint32_t TR = (uint32_t)std::max<int64_t>(64, std::min<int64_t>(ctx.opt.varchar_tile_rows, 8192));
+        std::vector<DevPtr> vtemp(nc);
+        DevPtr totals;
+        size_t nvar = 0;
+        for (size_t c = 0; c < nc; ++c)
+            if (types[c] == CJ_VARCHAR) ++nvar;
+        if (rows && nvar) {
+            totals = ctx.alloc(nvar * 8);
+            size_t k = 0;
+            for (size_t c = 0; c < nc; ++c) {
+                if (types[c] != CJ_VARCHAR) continue;
+                vtemp[c] = ctx.alloc(varchar_temp_bytes(rows, TR));
+                KScope ks(*this, "varchar_plan");
+                ck(launch_varchar_plan(L, cols[c], rows, TR, vtemp[c]->ptr,
+                                       totals->as<unsigned long long>() + k),
+                   "varchar_plan");
+                ++k;
+            }
+            std::vector<unsigned long long> host(nvar);
+            ck(cudaMemcpyAsync(host.data(), totals->ptr, nvar * 8, cudaMemcpyDeviceToHost, ctx.stream), "copy");
+            ctx.sync_status();
+            k = 0;
+            for (size_t c = 0; c < nc; ++c)
+                if (types[c] == CJ_VARCHAR) res->num_pages[c] = host[k++];
+        }
+        for (size_t c = 0; c < nc; ++c) {
+            if (!rows) continue;
+            if (types[c] != CJ_VARCHAR) {
+                const uint32_t R = rows_per_page_fixed(types[c]);
+                res->num_pages[c] = (rows + R - 1) / R;
+                res->dev_pages[c] = ctx.alloc(res->num_pages[c] * kPageSize);
+                KScope ks(*this, types[c] == CJ_INT32 ? "write_pages_int32" : "write_pages_8byte");
+                ck(launch_write_fixed_pages(L, cols[c], rows, res->dev_pages[c]->as<uint8_t>()), "write_fixed");
+            } else {
+                res->dev_pages[c] = ctx.alloc(res->num_pages[c] * kPageSize);
+                KScope ks(*this, "varchar_write");
+                ck(launch_varchar_write(L, cols[c], rows, TR, vtemp[c]->ptr, res->dev_pages[c]->as<uint8_t>()),
+                   "varchar_write");
+            }
+        }
+    }
+    uint64_t total_pages = 0;
+    for (size_t c = 0; c < nc; ++c) total_pages += res->num_pages[c];
+    stats.output_rows = rows;
+    stats.output_pages = total_pages;
+    res->host_cols.assign(nc, nullptr);
+    if (!(flags & CJ_EXEC_RESULT_ON_DEVICE) && total_pages) {
+        PhaseScope ph(*this, PH_DOWNLOAD);
+        res->host = ctx.alloc_pinned(total_pages * kPageSize);
+        uint8_t *h = static_cast<uint8_t *>(res->host->ptr);
+        for (size_t c = 0; c < nc; ++c) {
+            res->host_cols[c] = h;
+            const size_t bytes = res->num_pages[c] * kPageSize;
+            if (bytes)
+                ck(cudaMemcpyAsync(h, res->dev_pages[c]->ptr, bytes, cudaMemcpyDeviceToHost, ctx.stream), "download");
+            h += bytes;
+        }
+        stats.d2h_bytes += total_pages * kPageSize;
+    }
+    return guard.release();
+}
+
+cj_result *Executor::run(cj_exec_stats *st) {
+    auto t0 = std::chrono::steady_clock::now();
+    const uint64_t launches0 = launches_so_far();
+    validate();
+    cj_result *res = nullptr;
+    const cj_plan_node &root = plan.nodes[plan.root];
+    if (root.node_type == CJ_NODE_SCAN) {
+        /* A scan root (the reference requires a join root) returns the
+         * projected table. */
+        Relation s = scan_relation(root);
+        if (s.rows > 0xFFFFFFFFull) fail(CJ_ERR_LIMIT, "table exceeds 2^32-1 rows");
+        std::vector<ColView> cols;
+        std::vector<int32_t> types;
+        for (auto &c : s.cols) {
+            cols.push_back(view(s, c, nullptr));
+            types.push_back(c.type);
+        }
+        res = materialize(cols, types, s.rows);
+    } else {
+        exec_join(plan.root, 0, true, &res);
+    }
+    std::unique_ptr<cj_result> guard(res);
+    ctx.sync_status();
+    double ph_us[PH_COUNT] = {0};
+    for (auto &pe : phase_events) {
+        float ms = 0;
+        if (cudaEventElapsedTime(&ms, pe.a, pe.b) == cudaSuccess) ph_us[pe.phase] += ms * 1000.0;
+    }
+    cudaGetLastError();
+    if (ctx.opt.profile_kernels) ctx.resolve_profile();
+    auto t1 = std::chrono::steady_clock::now();
+    stats.upload_us = ph_us[PH_UPLOAD];
+    stats.decode_us = ph_us[PH_DECODE];
+    stats.build_us = ph_us[PH_BUILD];
+    stats.probe_us = ph_us[PH_PROBE];
+    stats.nested_loop_us = ph_us[PH_NL];
+    stats.intermediate_us = ph_us[PH_INTER];
+    stats.materialize_us = ph_us[PH_MAT];
+    stats.download_us = ph_us[PH_DOWNLOAD];
+    stats.total_us = std::chrono::duration<double, std::micro>(t1 - t0).count();
+    stats.kernel_launches = launches_so_far() - launches0;
+    if (st) *st = stats;
+    return guard.release();
+}
+
+} // namespace
+
+cj_result *execute_plan(Context &ctx, const cj_plan_desc &plan, uint32_t flags, cj_exec_stats *stats) {
+    Executor ex(ctx, plan, flags);
+    return ex.run(stats);
+}
+
+} // namespace cj

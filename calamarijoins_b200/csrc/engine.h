@@ -1,0 +1,151 @@
+/*
+ * engine.h — host side of the library: the context (device, streams,
+ * stream-ordered memory pool, pinned staging, per-kernel profiler), device
+ * buffers, resident tables and results.
+ *
+ * The reference's context is a process-wide mmap arena reset on every
+ * execute() plus a persistent thread pool (include/platform/arena.h:88-372,
+ * worker_pool.h:44-149). Here the context owns a CUDA memory pool from
+ * which every per-plan buffer is taken and returned in stream order, so
+ * memory is recycled between plans without device synchronisation.
+ */
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "cj_internal.h"
+
+namespace cj {
+
+/* Internal error: thrown inside the library, turned into a status code at
+ * the C ABI. */
+struct Error {
+    int code;
+    std::string msg;
+};
+[[noreturn]] void fail(int code, const std::string &msg);
+void check_cuda(cudaError_t e, const char *what);
+
+struct Options {
+    int64_t nested_loop_max_build = 64;
+    int64_t slots_per_partition = 0; /* 0 = auto (2048) */
+    int64_t profile_kernels = 0;
+    int64_t block_threads = 0;
+    int64_t varchar_tile_rows = 2048;
+    int64_t ctas_per_sm = 0;
+};
+
+struct Context;
+
+/* A stream-ordered device allocation from the context's pool. */
+struct DevBuf {
+    Context *ctx = nullptr;
+    void *ptr = nullptr;
+    size_t bytes = 0;
+    ~DevBuf();
+    template <typename T> T *as() const { return reinterpret_cast<T *>(ptr); }
+};
+using DevPtr = std::shared_ptr<DevBuf>;
+
+/* Page-locked host block from the context's pinned pool. */
+struct PinnedBlock {
+    Context *ctx = nullptr;
+    void *ptr = nullptr;
+    size_t bytes = 0;
+    ~PinnedBlock();
+};
+using PinnedPtr = std::shared_ptr<PinnedBlock>;
+
+struct KernelProfile {
+    std::string name;
+    uint64_t launches = 0;
+    double total_us = 0;
+};
+
+struct Context {
+    int device = 0;
+    int num_sms = 148;
+    cudaStream_t stream = nullptr;
+    cudaMemPool_t pool = nullptr;
+    uint16_t *d_bloom = nullptr;      /* 2048 Bloom tags                  */
+    StatusBlock *d_status = nullptr;  /* device status word + counters     */
+    StatusBlock *h_status = nullptr;  /* pinned mirror                     */
+    void *staging[2] = {nullptr, nullptr};
+    cudaEvent_t staging_ev[2] = {nullptr, nullptr};
+    size_t staging_bytes = 16u << 20;
+    Options opt;
+
+    /* pinned pool: size class -> free blocks */
+    std::multimap<size_t, void *> pinned_free;
+    std::mutex pinned_mu;
+
+    /* profiler */
+    std::vector<KernelProfile> profile;
+    std::map<std::string, size_t> profile_index;
+    std::vector<cudaEvent_t> event_pool;
+    struct PendingTiming {
+        size_t slot;
+        cudaEvent_t a, b;
+    };
+    std::vector<PendingTiming> pending;
+
+    ~Context();
+
+    Launch launch() const {
+        Launch L;
+        L.stream = stream;
+        L.num_sms = num_sms;
+        L.block_threads = (int)opt.block_threads;
+        L.dev_errors = &d_status->errors;
+        return L;
+    }
+    DevPtr alloc(size_t bytes);
+    PinnedPtr alloc_pinned(size_t bytes);
+    cudaEvent_t get_event();
+    void put_event(cudaEvent_t e);
+    /* Copies the status block to the host, waits for the stream and throws
+     * on any device-side error bit. */
+    void sync_status();
+    void resolve_profile();
+};
+
+/* Device pages of one column. */
+struct ColumnPages {
+    int32_t type = CJ_INT32;
+    uint64_t num_pages = 0;
+    const uint8_t *dev = nullptr;
+    DevPtr owner; /* null when the memory is adopted from the caller */
+};
+
+void upload_pages(Context &ctx, const cj_column_desc &cd, ColumnPages &out, uint64_t *h2d_bytes);
+
+} // namespace cj
+
+struct cj_context : cj::Context {};
+
+struct cj_table {
+    cj::Context *ctx = nullptr;
+    uint64_t num_rows = 0;
+    std::vector<cj::ColumnPages> cols;
+};
+
+struct cj_result {
+    cj::Context *ctx = nullptr;
+    uint64_t num_rows = 0;
+    std::vector<int32_t> types;
+    std::vector<uint64_t> num_pages;
+    std::vector<cj::DevPtr> dev_pages;
+    cj::PinnedPtr host;
+    std::vector<uint8_t *> host_cols;
+};
+
+namespace cj {
+cj_result *execute_plan(Context &ctx, const cj_plan_desc &plan, uint32_t flags, cj_exec_stats *stats);
+}

@@ -1,0 +1,255 @@
+/*
+ * k_build.cu — unchained hash-table build with Bloom tags on sm_100a.
+ *
+ * The table is the reference's UnchainedHashtable (include/join_execution/
+ * hashtable.h:63-506): a power-of-two directory of u64 entries
+ * (end offset << 16 | OR of 16-bit Bloom tags, :197-246) over a contiguous,
+ * slot-ordered tuple array, so a probe reads [dir[s-1] >> 16, dir[s] >> 16)
+ * (:298-313). Directory size = pow2 >= max(2048, build rows) (:255-264).
+ *
+ * Build = radix partition + per-partition counting sort, the reference's
+ * two-pass build (:405-505) mapped to the GPU:
+ *   1. k_part_hist    one CTA per contiguous chunk of build rows builds a
+ *                     shared-memory histogram over the P partitions (top
+ *                     log2(P) hash bits) and stores it column-major in a
+ *                     P x G matrix;
+ *   2. exclusive scan of the matrix gives every (partition, CTA) pair its
+ *                     output range: a stable, atomic-free partitioning;
+ *   3. k_part_scatter each CTA re-reads its chunk and scatters {key, row id}
+ *                     tuples, ranking rows of one partition within a warp
+ *                     with __match_any_sync (warp-aggregated scatter);
+ *   4. k_part_build   one CTA per partition counts its S slots in shared
+ *                     memory, ORs the Bloom tags, scans, writes its S
+ *                     directory entries and scatters the tuples into slot
+ *                     order (build_partition, hashtable.h:197-246).
+ * NULL keys are skipped (hashtable.h:439-478).
+ */
+#include "cj_device.cuh"
+
+namespace cj {
+namespace {
+
+constexpr int kBuildThreads = 256;
+constexpr int kHistItems = 16;
+
+struct PartGeom {
+    uint32_t n;        /* build relation rows                */
+    int log2_parts;
+    int log2_slots;
+    uint32_t grid;     /* CTAs of the hist / scatter passes  */
+    uint32_t chunk;    /* rows per CTA                       */
+};
+
+CJ_DEV uint32_t part_of(uint64_t h, int log2_parts) {
+    return log2_parts ? (uint32_t)(h >> (64 - log2_parts)) : 0u;
+}
+
+__global__ void __launch_bounds__(kBuildThreads)
+    k_part_hist(ColView key, PartGeom g, uint32_t *__restrict__ matrix) {
+    extern __shared__ uint32_t s_hist[];
+    const uint32_t P = 1u << g.log2_parts;
+    for (uint32_t b = threadIdx.x; b < P; b += blockDim.x) s_hist[b] = 0;
+    __syncthreads();
+    const uint64_t r0 = (uint64_t)blockIdx.x * g.chunk;
+    const uint64_t r1 = min((uint64_t)g.n, r0 + g.chunk);
+    for (uint64_t i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+        int64_t k;
+        if (load_key(key, (uint32_t)i, &k)) atomicAdd(&s_hist[part_of(hash_key(k), g.log2_parts)], 1u);
+    }
+    __syncthreads();
+    for (uint32_t b = threadIdx.x; b < P; b += blockDim.x)
+        matrix[(uint64_t)b * g.grid + blockIdx.x] = s_hist[b];
+}
+
+template <typename K>
+__global__ void __launch_bounds__(kBuildThreads)
+    k_part_scatter(ColView key, PartGeom g, const uint64_t *__restrict__ offsets,
+                   Tuple<K> *__restrict__ out) {
+    extern __shared__ uint32_t smem[];
+    const uint32_t P = 1u << g.log2_parts;
+    uint32_t *s_cursor = smem;      /* next output slot per partition  */
+    uint32_t *s_tile = smem + P;    /* rows per partition in this tile */
+    for (uint32_t b = threadIdx.x; b < P; b += blockDim.x)
+        s_cursor[b] = (uint32_t)offsets[(uint64_t)b * g.grid + blockIdx.x];
+    const uint64_t r0 = (uint64_t)blockIdx.x * g.chunk;
+    const uint64_t r1 = min((uint64_t)g.n, r0 + g.chunk);
+    const uint32_t tile = blockDim.x * kHistItems;
+    for (uint64_t t0 = r0; t0 < r1; t0 += tile) {
+        for (uint32_t b = threadIdx.x; b < P; b += blockDim.x) s_tile[b] = 0;
+        __syncthreads();
+        uint32_t part[kHistItems], rank[kHistItems];
+        K keys[kHistItems];
+#pragma unroll
+        for (int it = 0; it < kHistItems; ++it) {
+            uint64_t i = t0 + (uint64_t)it * blockDim.x + threadIdx.x;
+            int64_t k = 0;
+            bool v = i < r1 && load_key(key, (uint32_t)i, &k);
+            uint32_t p = v ? part_of(hash_key(k), g.log2_parts) : 0xffffffffu;
+            uint32_t peers = __match_any_sync(0xffffffffu, p);
+            uint32_t leader = __ffs(peers) - 1;
+            uint32_t base = 0;
+            if (v && lane_id() == leader) base = atomicAdd(&s_tile[p], (uint32_t)__popc(peers));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            part[it] = p;
+            rank[it] = base + __popc(peers & lanemask_lt());
+            keys[it] = (K)k;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int it = 0; it < kHistItems; ++it) {
+            if (part[it] == 0xffffffffu) continue;
+            uint64_t i = t0 + (uint64_t)it * blockDim.x + threadIdx.x;
+            Tuple<K> tp;
+            tp.key = keys[it];
+            tp.rid = (uint32_t)i;
+            out[s_cursor[part[it]] + rank[it]] = tp;
+        }
+        __syncthreads();
+        for (uint32_t b = threadIdx.x; b < P; b += blockDim.x) s_cursor[b] += s_tile[b];
+        __syncthreads();
+    }
+}
+
+template <typename K>
+__global__ void __launch_bounds__(kBuildThreads)
+    k_part_build(const Tuple<K> *__restrict__ in, const uint64_t *__restrict__ offsets,
+                 uint32_t grid_hist, int log2_parts, int log2_slots,
+                 const uint16_t *__restrict__ g_bloom, uint64_t *__restrict__ dir,
+                 Tuple<K> *__restrict__ out) {
+    extern __shared__ uint32_t smem[];
+    __shared__ uint16_t s_bloom[2048];
+    __shared__ uint32_t wbuf[kBuildThreads / 32 + 1];
+    const uint32_t P = 1u << log2_parts;
+    const uint32_t S = 1u << (log2_slots - log2_parts);
+    uint32_t *s_cnt = smem;
+    uint32_t *s_tag = smem + S;
+    load_bloom(s_bloom, g_bloom);
+    for (uint32_t p = blockIdx.x; p < P; p += gridDim.x) {
+        for (uint32_t s = threadIdx.x; s < S; s += blockDim.x) {
+            s_cnt[s] = 0;
+            s_tag[s] = 0;
+        }
+        __syncthreads();
+        const uint64_t ps = offsets[(uint64_t)p * grid_hist];
+        const uint64_t pe = offsets[(uint64_t)(p + 1) * grid_hist];
+        for (uint64_t t = ps + threadIdx.x; t < pe; t += blockDim.x) {
+            uint64_t h = hash_key((int64_t)in[t].key);
+            uint32_t ls = slot_of(h, log2_slots) & (S - 1);
+            atomicAdd(&s_cnt[ls], 1u);
+            atomicOr(&s_tag[ls], (uint32_t)s_bloom[bloom_index(h)]);
+        }
+        __syncthreads();
+        /* exclusive scan of the S counts: each thread owns S/blockDim slots */
+        const uint32_t per = (S + blockDim.x - 1) / blockDim.x;
+        const uint32_t s0 = threadIdx.x * per;
+        uint32_t sum = 0;
+        for (uint32_t k = 0; k < per; ++k)
+            if (s0 + k < S) sum += s_cnt[s0 + k];
+        uint32_t tot;
+        uint32_t pre = block_exclusive_scan<uint32_t>(sum, wbuf, &tot);
+        for (uint32_t k = 0; k < per; ++k) {
+            uint32_t s = s0 + k;
+            if (s >= S) break;
+            uint32_t c = s_cnt[s];
+            uint64_t end = ps + pre + c;
+            dir[(uint64_t)p * S + s] = (end << 16) | (uint64_t)(s_tag[s] & 0xFFFFu);
+            s_cnt[s] = pre; /* becomes the scatter cursor */
+            pre += c;
+        }
+        __syncthreads();
+        for (uint64_t t = ps + threadIdx.x; t < pe; t += blockDim.x) {
+            Tuple<K> tp = in[t];
+            uint32_t ls = slot_of(hash_key((int64_t)tp.key), log2_slots) & (S - 1);
+            uint32_t pos = atomicAdd(&s_cnt[ls], 1u);
+            out[ps + pos] = tp;
+        }
+        __syncthreads();
+    }
+}
+
+PartGeom geometry(const Launch &L, const BuildPlan &bp) {
+    PartGeom g;
+    g.n = bp.num_rows;
+    g.log2_parts = bp.log2_parts;
+    g.log2_slots = bp.log2_slots;
+    uint64_t tiles = ((uint64_t)bp.num_rows + kBuildThreads * kHistItems - 1) / (kBuildThreads * kHistItems);
+    uint64_t grid = (uint64_t)L.num_sms * 2;
+    if (tiles < grid) grid = tiles;
+    if (grid == 0) grid = 1;
+    g.grid = (uint32_t)grid;
+    g.chunk = (uint32_t)(((uint64_t)bp.num_rows + grid - 1) / grid);
+    return g;
+}
+
+size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+template <typename K>
+cudaError_t build_impl(const Launch &L, const BuildPlan &bp, const ColView &key,
+                       const uint16_t *bloom, uint64_t *dir, Tuple<K> *tuples, void *temp) {
+    PartGeom g = geometry(L, bp);
+    const uint64_t P = 1ull << bp.log2_parts;
+    const uint64_t cells = P * g.grid;
+    char *t = reinterpret_cast<char *>(temp);
+    uint32_t *matrix = reinterpret_cast<uint32_t *>(t);
+    t += align256(cells * sizeof(uint32_t));
+    uint64_t *offsets = reinterpret_cast<uint64_t *>(t);
+    t += align256((cells + 1) * sizeof(uint64_t));
+    Tuple<K> *part_buf = reinterpret_cast<Tuple<K> *>(t);
+    t += align256((size_t)bp.num_rows * sizeof(Tuple<K>));
+    void *scan_tmp = t;
+
+    const size_t hist_smem = P * sizeof(uint32_t);
+    k_part_hist<<<g.grid, kBuildThreads, hist_smem, L.stream>>>(key, g, matrix);
+    count_launches(1);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    e = scan_u32_to_u64(L, matrix, offsets, cells, scan_tmp);
+    if (e != cudaSuccess) return e;
+    const size_t scat_smem = 2 * P * sizeof(uint32_t);
+    k_part_scatter<K><<<g.grid, kBuildThreads, scat_smem, L.stream>>>(key, g, offsets, part_buf);
+    count_launches(1);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    const uint64_t S = 1ull << (bp.log2_slots - bp.log2_parts);
+    const size_t build_smem = 2 * S * sizeof(uint32_t);
+    unsigned grid_b = (unsigned)(P < (uint64_t)L.num_sms * 16 ? P : (uint64_t)L.num_sms * 16);
+    k_part_build<K><<<grid_b, kBuildThreads, build_smem, L.stream>>>(
+        part_buf, offsets, g.grid, bp.log2_parts, bp.log2_slots, bloom, dir, tuples);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+bool g_attrs_set = false;
+void set_smem_attrs() {
+    if (g_attrs_set) return;
+    cudaFuncSetAttribute(k_part_hist, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
+    cudaFuncSetAttribute(k_part_scatter<int32_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
+    cudaFuncSetAttribute(k_part_scatter<int64_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
+    cudaFuncSetAttribute(k_part_build<int32_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
+    cudaFuncSetAttribute(k_part_build<int64_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
+    g_attrs_set = true;
+}
+
+} // namespace
+
+size_t build_temp_bytes(const Launch &L, const BuildPlan &bp, int key_bytes) {
+    PartGeom g = geometry(L, bp);
+    uint64_t cells = (1ull << bp.log2_parts) * g.grid;
+    size_t tuple = key_bytes == 4 ? sizeof(Tuple<int32_t>) : sizeof(Tuple<int64_t>);
+    return align256(cells * 4) + align256((cells + 1) * 8) + align256((size_t)bp.num_rows * tuple) +
+           scan_temp_bytes(cells) + 256;
+}
+
+size_t build_tuple_bytes(int key_bytes) {
+    return key_bytes == 4 ? sizeof(Tuple<int32_t>) : sizeof(Tuple<int64_t>);
+}
+
+cudaError_t launch_build(const Launch &L, const BuildPlan &bp, const ColView &key,
+                         const uint16_t *bloom, uint64_t *dir, void *tuples, void *temp) {
+    set_smem_attrs();
+    if (key.type == CJ_INT32)
+        return build_impl<int32_t>(L, bp, key, bloom, dir, reinterpret_cast<Tuple<int32_t> *>(tuples), temp);
+    return build_impl<int64_t>(L, bp, key, bloom, dir, reinterpret_cast<Tuple<int64_t> *>(tuples), temp);
+}
+
+} // namespace cj

@@ -1,0 +1,288 @@
+/*
+ * k_decode.cu — page decode: 8 KiB pages in HBM -> dense device columns.
+ *
+ * Follows the page format of the reference (include/data_model/plan.h:
+ * 75-142, 187-366; README.md "Data format") and its readers:
+ *   - row counts per page, long-string pages counting as one row (0xffff)
+ *     or none (0xfffe): PageIndex::build (include/data_access/
+ *     columnar_reader.h:122-200)
+ *   - dense pages (n_rows == n_values) read values in row order without
+ *     the bitmap, sparse pages locate a value by popcount of the bitmap
+ *     prefix: ColumnarReader::read_dense_int32 / read_sparse
+ *     (columnar_reader.h:385-393, 452-474)
+ *   - VARCHAR: n_values u16 end offsets at +4, characters after them
+ *     (include/materialization/page_builders.h:26-37)
+ *
+ * One CTA decodes one page at a time (grid-stride over pages); the page's
+ * bitmap and its popcount prefix live in shared memory. Value writes are
+ * coalesced; the validity bitmap is written with plain stores except for
+ * the (at most two) 32-row words a page shares with its neighbours, which
+ * use atomicOr on a zeroed bitmap.
+ */
+#include "cj_device.cuh"
+
+namespace cj {
+namespace {
+
+constexpr int kDecodeThreads = 256;
+constexpr uint32_t kMaxBitmapWords = 2048; /* 65535 rows */
+
+CJ_DEV uint16_t rd16(const uint8_t *p) { return *reinterpret_cast<const uint16_t *>(p); }
+
+__global__ void k_page_rows(const uint8_t *__restrict__ pages, uint64_t np, int32_t type,
+                            uint32_t *__restrict__ rows, unsigned int *err) {
+    for (uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; p < np;
+         p += (uint64_t)gridDim.x * blockDim.x) {
+        const uint8_t *pg = pages + p * kPageSize;
+        uint32_t nr = rd16(pg), nv = rd16(pg + 2);
+        uint32_t r = nr;
+        if (type == CJ_VARCHAR) {
+            if (nr == 0xffff) {
+                r = 1;
+                if (nv == 0 || nv > kLongChunk) atomicOr(err, DEV_ERR_PAGE_HEADER);
+            } else if (nr == 0xfffe) {
+                r = 0;
+                if (nv == 0 || nv > kLongChunk) atomicOr(err, DEV_ERR_PAGE_HEADER);
+            } else if (nv > nr || 4u + 2u * nv + (nr + 7) / 8 > kPageSize) {
+                atomicOr(err, DEV_ERR_PAGE_HEADER);
+            }
+        } else {
+            uint32_t w = type == CJ_INT32 ? 4u : 8u;
+            if (nv > nr || w + w * nv + (nr + 7) / 8 > kPageSize) atomicOr(err, DEV_ERR_PAGE_HEADER);
+        }
+        rows[p] = r;
+    }
+}
+
+/* Loads a sparse page's bitmap into s_bm (bits past n_rows cleared) and the
+ * exclusive popcount prefix per word into s_pre. Block-wide. */
+CJ_DEV void load_page_bitmap(const uint8_t *pg, uint32_t nr, uint32_t *s_bm, uint32_t *s_pre,
+                             uint32_t *wbuf) {
+    const uint32_t nbytes = (nr + 7) / 8, nwords = (nr + 31) / 32;
+    const uint8_t *bmb = pg + kPageSize - nbytes;
+    for (uint32_t w = threadIdx.x; w < nwords; w += blockDim.x) {
+        uint32_t v = 0;
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+            uint32_t bi = w * 4 + b;
+            if (bi < nbytes) v |= (uint32_t)bmb[bi] << (8 * b);
+        }
+        uint32_t live = nr - w * 32;
+        if (live < 32) v &= (1u << live) - 1u;
+        s_bm[w] = v;
+    }
+    __syncthreads();
+    const uint32_t per = (nwords + blockDim.x - 1) / blockDim.x;
+    const uint32_t w0 = threadIdx.x * per;
+    uint32_t s = 0;
+    for (uint32_t k = 0; k < per; ++k)
+        if (w0 + k < nwords) s += __popc(s_bm[w0 + k]);
+    uint32_t tot;
+    uint32_t pre = block_exclusive_scan<uint32_t>(s, wbuf, &tot);
+    for (uint32_t k = 0; k < per; ++k)
+        if (w0 + k < nwords) {
+            s_pre[w0 + k] = pre;
+            pre += __popc(s_bm[w0 + k]);
+        }
+    __syncthreads();
+}
+
+/* Value index of page row i of a sparse page, or -1 if the row is NULL. */
+CJ_DEV int value_index(const uint32_t *s_bm, const uint32_t *s_pre, uint32_t i) {
+    uint32_t w = i >> 5, b = i & 31;
+    uint32_t word = s_bm[w];
+    if (!((word >> b) & 1u)) return -1;
+    return (int)(s_pre[w] + __popc(word & ((1u << b) - 1u)));
+}
+
+/* 32 validity bits of the output word whose first row is page row `off`
+ * (off may be negative for the page's first word). */
+CJ_DEV uint32_t page_bits(bool dense, const uint32_t *s_bm, uint32_t nr, int64_t off) {
+    if (dense) {
+        int64_t lo = off < 0 ? -off : 0;
+        int64_t hi = (int64_t)nr - off;
+        if (hi > 32) hi = 32;
+        if (hi <= lo) return 0;
+        uint32_t width = (uint32_t)(hi - lo);
+        uint32_t m = width >= 32 ? 0xffffffffu : ((1u << width) - 1u);
+        return m << lo;
+    }
+    if (off < 0) return s_bm[0] << (uint32_t)(-off);
+    const uint32_t nwords = (nr + 31) / 32;
+    uint32_t w0 = (uint32_t)(off >> 5), s = (uint32_t)(off & 31);
+    uint32_t lo = w0 < nwords ? s_bm[w0] : 0u;
+    uint32_t hi = w0 + 1 < nwords ? s_bm[w0 + 1] : 0u;
+    return s ? (lo >> s) | (hi << (32 - s)) : lo;
+}
+
+CJ_DEV void write_validity(bool dense, const uint32_t *s_bm, uint32_t nr, uint64_t rs,
+                           uint32_t *valid) {
+    if (nr == 0) return;
+    const uint64_t fw = rs >> 5, lw = (rs + nr - 1) >> 5;
+    for (uint64_t ow = fw + threadIdx.x; ow <= lw; ow += blockDim.x) {
+        int64_t off = (int64_t)(ow * 32) - (int64_t)rs;
+        uint32_t bits = page_bits(dense, s_bm, nr, off);
+        if (off >= 0 && off + 32 <= (int64_t)nr)
+            valid[ow] = bits;
+        else if (bits)
+            atomicOr(valid + ow, bits);
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kDecodeThreads)
+    k_decode_fixed(const uint8_t *__restrict__ pages, uint64_t np,
+                   const uint64_t *__restrict__ row_start, uint64_t max_rows, T *__restrict__ values,
+                   uint32_t *__restrict__ valid, unsigned int *err) {
+    __shared__ uint32_t s_bm[kMaxBitmapWords];
+    __shared__ uint32_t s_pre[kMaxBitmapWords];
+    __shared__ uint32_t wbuf[kDecodeThreads / 32 + 1];
+    constexpr uint32_t DB = sizeof(T) == 4 ? 4u : 8u;
+    for (uint64_t p = blockIdx.x; p < np; p += gridDim.x) {
+        const uint8_t *pg = pages + p * kPageSize;
+        const uint32_t nr = rd16(pg), nv = rd16(pg + 2);
+        if (nv > nr || DB + (uint32_t)sizeof(T) * nv + (nr + 7) / 8 > kPageSize) continue;
+        const uint64_t rs = row_start[p];
+        if (rs + nr > max_rows) {
+            if (threadIdx.x == 0) atomicOr(err, DEV_ERR_ROW_COUNT);
+            continue;
+        }
+        const T *vals = reinterpret_cast<const T *>(pg + DB);
+        const bool dense = nr == nv;
+        if (!dense) load_page_bitmap(pg, nr, s_bm, s_pre, wbuf);
+        for (uint32_t i = threadIdx.x; i < nr; i += blockDim.x) {
+            T v = T(0);
+            if (dense) {
+                v = __ldcs(vals + i);
+            } else {
+                int idx = value_index(s_bm, s_pre, i);
+                if (idx >= (int)nv) atomicOr(err, DEV_ERR_PAGE_HEADER); /* bitmap holds > n_values bits */
+                else if (idx >= 0) v = __ldcs(vals + idx);
+            }
+            values[rs + i] = v;
+        }
+        write_validity(dense, s_bm, nr, rs, valid);
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(kDecodeThreads)
+    k_decode_varchar(const uint8_t *__restrict__ pages, uint64_t np,
+                     const uint64_t *__restrict__ row_start, uint64_t max_rows,
+                     uint64_t *__restrict__ desc, uint32_t *__restrict__ valid, unsigned int *err) {
+    __shared__ uint32_t s_bm[kMaxBitmapWords];
+    __shared__ uint32_t s_pre[kMaxBitmapWords];
+    __shared__ uint32_t wbuf[kDecodeThreads / 32 + 1];
+    for (uint64_t p = blockIdx.x; p < np; p += gridDim.x) {
+        const uint8_t *pg = pages + p * kPageSize;
+        const uint32_t nr = rd16(pg), nv = rd16(pg + 2);
+        const uint64_t rs = row_start[p];
+        if (nr == 0xfffe) {
+            if (threadIdx.x == 0) {
+                uint32_t prev = p ? rd16(pg - kPageSize) : 0u;
+                if (prev != 0xffff && prev != 0xfffe) atomicOr(err, DEV_ERR_LONG_CHAIN);
+            }
+            continue;
+        }
+        if (nr == 0xffff) {
+            if (threadIdx.x == 0 && rs >= max_rows) atomicOr(err, DEV_ERR_ROW_COUNT);
+            if (threadIdx.x == 0 && rs < max_rows) {
+                uint64_t q = p + 1;
+                while (q < np && rd16(pages + q * kPageSize) == 0xfffe) ++q;
+                uint64_t chain = q - p;
+                if (chain > 0xFFFFFFull) {
+                    atomicOr(err, DEV_ERR_LONG_CHAIN);
+                    chain = 0xFFFFFF;
+                }
+                desc[rs] = desc_long(p, (uint32_t)chain);
+                atomicOr(valid + (rs >> 5), 1u << (rs & 31));
+            }
+            continue;
+        }
+        if (nv > nr || 4u + 2u * nv + (nr + 7) / 8 > kPageSize) continue;
+        if (rs + nr > max_rows) {
+            if (threadIdx.x == 0) atomicOr(err, DEV_ERR_ROW_COUNT);
+            continue;
+        }
+        const bool dense = nr == nv;
+        if (!dense) load_page_bitmap(pg, nr, s_bm, s_pre, wbuf);
+        const uint16_t *offs = reinterpret_cast<const uint16_t *>(pg + 4);
+        const uint32_t chars_at = 4u + 2u * nv;
+        const uint32_t chars_cap = kPageSize - (nr + 7) / 8 - chars_at;
+        for (uint32_t i = threadIdx.x; i < nr; i += blockDim.x) {
+            int k = dense ? (int)i : value_index(s_bm, s_pre, i);
+            uint64_t d = 0;
+            if (k >= (int)nv) {
+                atomicOr(err, DEV_ERR_PAGE_HEADER); /* bitmap holds > n_values bits */
+            } else if (k >= 0) {
+                uint32_t start = k ? offs[k - 1] : 0u, end = offs[k];
+                if (end < start || end > chars_cap) {
+                    atomicOr(err, DEV_ERR_VARCHAR_OFFSETS);
+                } else {
+                    d = desc_short(p * kPageSize + chars_at + start, end - start);
+                }
+            }
+            desc[rs + i] = d;
+        }
+        write_validity(dense, s_bm, nr, rs, valid);
+        __syncthreads();
+    }
+}
+
+__global__ void k_check_rows(const uint64_t *total, uint64_t expected, unsigned int *err) {
+    if (*total != expected) atomicOr(err, DEV_ERR_ROW_COUNT);
+}
+
+unsigned grid_for(const Launch &L, uint64_t units, int per_sm) {
+    uint64_t g = (uint64_t)L.num_sms * per_sm;
+    if (units < g) g = units;
+    return (unsigned)(g ? g : 1);
+}
+
+} // namespace
+
+cudaError_t launch_page_rows(const Launch &L, const uint8_t *pages, uint64_t np, int32_t type,
+                             uint32_t *rows) {
+    if (np == 0) return cudaSuccess;
+    unsigned g = (unsigned)((np + 255) / 256);
+    if (g > (unsigned)L.num_sms * 8) g = L.num_sms * 8;
+    k_page_rows<<<g, 256, 0, L.stream>>>(pages, np, type, rows, L.dev_errors);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_decode_fixed(const Launch &L, const uint8_t *pages, uint64_t np, int32_t type,
+                                const uint64_t *row_start, uint64_t max_rows, void *values,
+                                uint32_t *valid) {
+    if (np == 0) return cudaSuccess;
+    unsigned g = grid_for(L, np, 6);
+    if (type == CJ_INT32) {
+        k_decode_fixed<int32_t><<<g, kDecodeThreads, 0, L.stream>>>(
+            pages, np, row_start, max_rows, reinterpret_cast<int32_t *>(values), valid, L.dev_errors);
+        count_launches(1);
+    } else {
+        k_decode_fixed<long long><<<g, kDecodeThreads, 0, L.stream>>>(
+            pages, np, row_start, max_rows, reinterpret_cast<long long *>(values), valid, L.dev_errors);
+        count_launches(1);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_decode_varchar(const Launch &L, const uint8_t *pages, uint64_t np,
+                                  const uint64_t *row_start, uint64_t max_rows, uint64_t *desc,
+                                  uint32_t *valid) {
+    if (np == 0) return cudaSuccess;
+    unsigned g = grid_for(L, np, 6);
+    k_decode_varchar<<<g, kDecodeThreads, 0, L.stream>>>(pages, np, row_start, max_rows, desc, valid,
+                                                          L.dev_errors);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_check_rows(const Launch &L, const uint64_t *total, uint64_t expected) {
+    k_check_rows<<<1, 1, 0, L.stream>>>(total, expected, L.dev_errors);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+} // namespace cj

@@ -1,0 +1,398 @@
+/*
+ * k_materialize.cu — late materialisation: gather matched rows back into
+ * 8 KiB result pages.
+ *
+ * The reference materialises the root join through per-thread page
+ * builders (include/materialization/materialize.h:85-321,
+ * page_builders.h:92-391) and non-root joins into 4-byte value_t columns
+ * (construct_intermediate.h:121-220). Here non-root joins only gather u32
+ * row-id vectors (k_gather_u32); values are read once, by the root's page
+ * writers, through up to two row-id indirections.
+ *
+ * Fixed-width pages (k_write_fixed): output page p holds rows
+ * [p*R, p*R+R) with R = 1984 (INT32) or 1007 (INT64 / FP64), the fill of
+ * ColumnInserter<T> (plan.h:241-250), so every page fits whatever the NULL
+ * pattern. One CTA builds one page in shared memory: values compacted by a
+ * ballot/scan over the validity bits, bitmap at the page end, header
+ * (n_rows, n_values), gap zeroed; then 16-byte stores write the page out.
+ *
+ * VARCHAR pages (k_varchar_plan / k_varchar_write): rows are cut into tiles;
+ * within a tile pages are packed greedily in row order like
+ * ColumnInserter<std::string> (plan.h:340-369): a page takes rows while
+ * 4 + 2*n_values + chars + ceil(n_rows/8) <= 8192, found by binary search on
+ * the tile's prefix sums. A string longer than 8185 bytes arrives as a chain
+ * of long-string pages and is copied verbatim, as VarcharPageBuilder::
+ * copy_long_string_pages does (page_builders.h:345-362). Pass 1 counts each
+ * tile's pages, a scan places them, pass 2 writes them.
+ */
+#include "cj_device.cuh"
+
+namespace cj {
+namespace {
+
+constexpr int kMatThreads = 256;
+
+__global__ void k_gather_u32(const uint32_t *__restrict__ src, const uint32_t *__restrict__ idx,
+                             uint64_t n, uint32_t *__restrict__ out) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * blockDim.x)
+        out[i] = __ldg(src + __ldcs(idx + i));
+}
+
+/* Warp-0 exclusive scan of the per-warp counts in s_warp; total lands in
+ * s_warp[nwarps]. Caller brackets with __syncthreads(). */
+CJ_DEV void scan_warp_counts(uint32_t *s_warp) {
+    const int nwarps = kMatThreads / 32;
+    if ((threadIdx.x >> 5) == 0) {
+        uint32_t lane = lane_id();
+        uint32_t w = lane < (uint32_t)nwarps ? s_warp[lane] : 0u;
+        uint32_t wi = warp_inclusive_scan(w);
+        if (lane < (uint32_t)nwarps) s_warp[lane] = wi - w;
+        if (lane == 31) s_warp[nwarps] = wi;
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kMatThreads)
+    k_write_fixed(ColView col, uint64_t rows, uint32_t R, uint64_t num_pages,
+                  uint8_t *__restrict__ out) {
+    __shared__ uint4 s_page[kPageSize / 16];
+    __shared__ uint32_t s_warp[kMatThreads / 32 + 1];
+    constexpr uint32_t DB = sizeof(T) == 4 ? 4u : 8u;
+    uint8_t *sp = reinterpret_cast<uint8_t *>(s_page);
+    const uint32_t warp = threadIdx.x >> 5, lane = lane_id();
+    for (uint64_t pg = blockIdx.x; pg < num_pages; pg += gridDim.x) {
+        for (uint32_t k = threadIdx.x; k < kPageSize / 16; k += blockDim.x) s_page[k] = make_uint4(0, 0, 0, 0);
+        __syncthreads();
+        const uint64_t r0 = pg * R;
+        const uint32_t nr = (uint32_t)min((uint64_t)R, rows - r0);
+        const uint32_t bm_bytes = (nr + 7) / 8;
+        uint8_t *bm = sp + kPageSize - bm_bytes;
+        T *vals = reinterpret_cast<T *>(sp + DB);
+        uint32_t running = 0;
+        for (uint32_t slab = 0; slab * kMatThreads < nr; ++slab) {
+            const uint32_t r = slab * kMatThreads + threadIdx.x;
+            bool v = false;
+            T val = T(0);
+            if (r < nr) {
+                uint32_t br = base_row(col, (uint32_t)(r0 + r));
+                v = valid_bit(col.valid, br);
+                if (v) {
+                    val = __ldg(reinterpret_cast<const T *>(col.values) + br);
+                    if (sizeof(T) == 4 && col.null_sentinel && (int32_t)val == INT32_MIN) v = false;
+                }
+            }
+            uint32_t ball = __ballot_sync(0xffffffffu, v);
+            if (lane == 0) s_warp[warp] = __popc(ball);
+            __syncthreads();
+            scan_warp_counts(s_warp);
+            __syncthreads();
+            if (v) vals[running + s_warp[warp] + __popc(ball & lanemask_lt())] = val;
+            if (lane < 4) {
+                uint32_t byte = (slab * kMatThreads + warp * 32) / 8 + lane;
+                if (byte < bm_bytes) bm[byte] = (uint8_t)(ball >> (8 * lane));
+            }
+            running += s_warp[kMatThreads / 32];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) {
+            reinterpret_cast<uint16_t *>(sp)[0] = (uint16_t)nr;
+            reinterpret_cast<uint16_t *>(sp)[1] = (uint16_t)running;
+        }
+        __syncthreads();
+        uint4 *dst = reinterpret_cast<uint4 *>(out + pg * kPageSize);
+        for (uint32_t k = threadIdx.x; k < kPageSize / 16; k += blockDim.x) dst[k] = s_page[k];
+        __syncthreads();
+    }
+}
+
+/* ---------------- VARCHAR ---------------- */
+struct VarSmem {
+    uint64_t *desc;     /* TR   row descriptors (0 = NULL)                 */
+    uint32_t *lpre;     /* TR+1 prefix of short-string bytes               */
+    uint32_t *vpre;     /* TR+1 prefix of short non-NULL rows              */
+    uint32_t *longpre;  /* TR+1 prefix of long-string rows                 */
+    uint32_t *seg;      /* TR+1 first row of each segment                  */
+    uint32_t *segpg;    /* TR+1 first output page of each segment          */
+};
+
+CJ_DEV VarSmem carve(uint8_t *base, uint32_t TR) {
+    VarSmem s;
+    s.desc = reinterpret_cast<uint64_t *>(base);
+    uint32_t *u = reinterpret_cast<uint32_t *>(base + (size_t)TR * 8);
+    s.lpre = u;
+    s.vpre = u + (TR + 1);
+    s.longpre = u + 2 * (TR + 1);
+    s.seg = u + 3 * (TR + 1);
+    s.segpg = u + 4 * (TR + 1);
+    return s;
+}
+
+/* Loads the tile's descriptors, builds the prefix sums and cuts the tile
+ * into segments (one normal page, or one long string's chain). Returns the
+ * segment count; the page count is in s.segpg[nseg]. Block-wide. */
+CJ_DEV uint32_t plan_tile(const ColView &col, uint64_t r0, uint32_t nt, uint32_t TR,
+                          const VarSmem &s, uint32_t *wbuf, uint32_t *s_nseg) {
+    for (uint32_t r = threadIdx.x; r < nt; r += blockDim.x) {
+        uint32_t br = base_row(col, (uint32_t)(r0 + r));
+        s.desc[r] = valid_bit(col.valid, br) ? __ldg(col.str_desc + br) : 0ull;
+    }
+    __syncthreads();
+    const uint32_t per = (TR + blockDim.x - 1) / blockDim.x;
+    const uint32_t q0 = threadIdx.x * per;
+    uint32_t lsum = 0, vsum = 0, gsum = 0;
+    for (uint32_t k = 0; k < per; ++k) {
+        uint32_t r = q0 + k;
+        if (r >= nt) break;
+        uint64_t d = s.desc[r];
+        if (!d) continue;
+        if (desc_is_long(d)) ++gsum;
+        else {
+            lsum += desc_len(d);
+            ++vsum;
+        }
+    }
+    uint32_t ltot, vtot, gtot;
+    uint32_t lp = block_exclusive_scan<uint32_t>(lsum, wbuf, &ltot);
+    uint32_t vp = block_exclusive_scan<uint32_t>(vsum, wbuf, &vtot);
+    uint32_t gp = block_exclusive_scan<uint32_t>(gsum, wbuf, &gtot);
+    for (uint32_t k = 0; k < per; ++k) {
+        uint32_t r = q0 + k;
+        if (r >= nt) break;
+        s.lpre[r] = lp;
+        s.vpre[r] = vp;
+        s.longpre[r] = gp;
+        uint64_t d = s.desc[r];
+        if (d) {
+            if (desc_is_long(d)) ++gp;
+            else {
+                lp += desc_len(d);
+                ++vp;
+            }
+        }
+    }
+    if (threadIdx.x == 0) {
+        s.lpre[nt] = ltot;
+        s.vpre[nt] = vtot;
+        s.longpre[nt] = gtot;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t a = 0, ns = 0, np = 0;
+        while (a < nt) {
+            s.seg[ns] = a;
+            s.segpg[ns] = np;
+            uint64_t d = s.desc[a];
+            if (d && desc_is_long(d)) {
+                np += desc_len(d);
+                a += 1;
+            } else {
+                uint32_t lo = a + 1, hi = nt;
+                while (lo < hi) {
+                    uint32_t mid = (lo + hi + 1) >> 1;
+                    uint32_t n = mid - a;
+                    bool ok = s.longpre[mid] == s.longpre[a] && n <= 65533u &&
+                              4u + 2u * (s.vpre[mid] - s.vpre[a]) + (s.lpre[mid] - s.lpre[a]) +
+                                      (n + 7) / 8 <= kPageSize;
+                    if (ok) lo = mid;
+                    else hi = mid - 1;
+                }
+                np += 1;
+                a = lo;
+            }
+            ++ns;
+        }
+        s.seg[ns] = nt;
+        s.segpg[ns] = np;
+        *s_nseg = ns;
+    }
+    __syncthreads();
+    return *s_nseg;
+}
+
+__global__ void __launch_bounds__(kMatThreads)
+    k_varchar_plan(ColView col, uint64_t rows, uint32_t TR, uint32_t *__restrict__ tile_pages) {
+    extern __shared__ __align__(16) uint8_t dsm[];
+    __shared__ uint32_t wbuf[kMatThreads / 32 + 1];
+    __shared__ uint32_t s_nseg;
+    VarSmem s = carve(dsm, TR);
+    const uint64_t tiles = (rows + TR - 1) / TR;
+    for (uint64_t t = blockIdx.x; t < tiles; t += gridDim.x) {
+        const uint64_t r0 = t * TR;
+        const uint32_t nt = (uint32_t)min((uint64_t)TR, rows - r0);
+        uint32_t ns = plan_tile(col, r0, nt, TR, s, wbuf, &s_nseg);
+        if (threadIdx.x == 0) tile_pages[t] = s.segpg[ns];
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(kMatThreads)
+    k_varchar_write(ColView col, uint64_t rows, uint32_t TR, const uint64_t *__restrict__ tile_base,
+                    uint8_t *__restrict__ out) {
+    extern __shared__ __align__(16) uint8_t dsm[];
+    __shared__ uint4 s_page[kPageSize / 16];
+    __shared__ uint32_t wbuf[kMatThreads / 32 + 1];
+    __shared__ uint32_t s_nseg;
+    VarSmem s = carve(dsm, TR);
+    uint8_t *sp = reinterpret_cast<uint8_t *>(s_page);
+    const uint32_t warp = threadIdx.x >> 5, lane = lane_id(), nwarps = blockDim.x >> 5;
+    const uint64_t tiles = (rows + TR - 1) / TR;
+    for (uint64_t t = blockIdx.x; t < tiles; t += gridDim.x) {
+        const uint64_t r0 = t * TR;
+        const uint32_t nt = (uint32_t)min((uint64_t)TR, rows - r0);
+        const uint32_t ns = plan_tile(col, r0, nt, TR, s, wbuf, &s_nseg);
+        const uint64_t base = tile_base[t];
+        for (uint32_t g = 0; g < ns; ++g) {
+            const uint32_t a = s.seg[g], b = s.seg[g + 1];
+            const uint64_t opg = base + s.segpg[g];
+            const uint64_t d0 = s.desc[a];
+            if (d0 && desc_is_long(d0)) {
+                const uint4 *src = reinterpret_cast<const uint4 *>(col.pages + desc_pos(d0) * kPageSize);
+                uint4 *dst = reinterpret_cast<uint4 *>(out + opg * kPageSize);
+                const uint64_t n16 = (uint64_t)desc_len(d0) * (kPageSize / 16);
+                for (uint64_t k = threadIdx.x; k < n16; k += blockDim.x) dst[k] = __ldg(src + k);
+                continue;
+            }
+            for (uint32_t k = threadIdx.x; k < kPageSize / 16; k += blockDim.x) s_page[k] = make_uint4(0, 0, 0, 0);
+            __syncthreads();
+            const uint32_t n = b - a, nv = s.vpre[b] - s.vpre[a];
+            const uint32_t chars_at = 4u + 2u * nv;
+            const uint32_t bm_bytes = (n + 7) / 8;
+            uint8_t *bm = sp + kPageSize - bm_bytes;
+            uint16_t *offs = reinterpret_cast<uint16_t *>(sp + 4);
+            /* offsets, bitmap and short strings */
+            for (uint32_t j0 = 0; j0 < n; j0 += blockDim.x) {
+                const uint32_t j = j0 + threadIdx.x;
+                bool v = false;
+                if (j < n) {
+                    const uint32_t r = a + j;
+                    const uint64_t d = s.desc[r];
+                    if (d) {
+                        v = true;
+                        const uint32_t k = s.vpre[r] - s.vpre[a];
+                        const uint32_t beg = s.lpre[r] - s.lpre[a];
+                        const uint32_t len = desc_len(d);
+                        offs[k] = (uint16_t)(beg + len);
+                        if (len <= 32) {
+                            const uint8_t *src = col.pages + desc_pos(d);
+                            uint8_t *dst = sp + chars_at + beg;
+                            for (uint32_t q = 0; q < len; ++q) dst[q] = __ldg(src + q);
+                        }
+                    }
+                }
+                uint32_t ball = __ballot_sync(0xffffffffu, v);
+                if (lane < 4) {
+                    uint32_t byte = (j0 + warp * 32) / 8 + lane;
+                    if (byte < bm_bytes) bm[byte] = (uint8_t)(ball >> (8 * lane));
+                }
+            }
+            /* longer strings: one warp per string */
+            for (uint32_t r = a + warp; r < b; r += nwarps) {
+                const uint64_t d = s.desc[r];
+                if (!d || desc_len(d) <= 32) continue;
+                const uint8_t *src = col.pages + desc_pos(d);
+                uint8_t *dst = sp + chars_at + (s.lpre[r] - s.lpre[a]);
+                const uint32_t len = desc_len(d);
+                for (uint32_t q = lane; q < len; q += 32) dst[q] = __ldg(src + q);
+            }
+            if (threadIdx.x == 0) {
+                reinterpret_cast<uint16_t *>(sp)[0] = (uint16_t)n;
+                reinterpret_cast<uint16_t *>(sp)[1] = (uint16_t)nv;
+            }
+            __syncthreads();
+            uint4 *dst = reinterpret_cast<uint4 *>(out + opg * kPageSize);
+            for (uint32_t k = threadIdx.x; k < kPageSize / 16; k += blockDim.x) dst[k] = s_page[k];
+            __syncthreads();
+        }
+        __syncthreads();
+    }
+}
+
+size_t var_dyn_smem(uint32_t TR) { return (size_t)TR * 8 + 5 * ((size_t)TR + 1) * 4; }
+
+bool g_var_attrs = false;
+void set_var_attrs() {
+    if (g_var_attrs) return;
+    cudaFuncSetAttribute(k_varchar_plan, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(k_varchar_write, cudaFuncAttributeMaxDynamicSharedMemorySize, 190 * 1024);
+    g_var_attrs = true;
+}
+
+size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+} // namespace
+
+cudaError_t launch_gather_u32(const Launch &L, const uint32_t *src, const uint32_t *idx, uint64_t n,
+                              uint32_t *out) {
+    if (n == 0) return cudaSuccess;
+    uint64_t g = (n + 255) / 256;
+    uint64_t cap = (uint64_t)L.num_sms * 8;
+    if (g > cap) g = cap;
+    k_gather_u32<<<(unsigned)g, 256, 0, L.stream>>>(src, idx, n, out);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+uint32_t rows_per_page_fixed(int32_t type) {
+    return type == CJ_INT32 ? kRowsPerPageInt32 : kRowsPerPage8B;
+}
+
+cudaError_t launch_write_fixed_pages(const Launch &L, const ColView &col, uint64_t rows,
+                                     uint8_t *out) {
+    if (rows == 0) return cudaSuccess;
+    const uint32_t R = rows_per_page_fixed(col.type);
+    const uint64_t np = (rows + R - 1) / R;
+    uint64_t g = np, cap = (uint64_t)L.num_sms * 6;
+    if (g > cap) g = cap;
+    if (col.type == CJ_INT32) {
+        k_write_fixed<int32_t><<<(unsigned)g, kMatThreads, 0, L.stream>>>(col, rows, R, np, out);
+        count_launches(1);
+    } else {
+        k_write_fixed<long long><<<(unsigned)g, kMatThreads, 0, L.stream>>>(col, rows, R, np, out);
+        count_launches(1);
+    }
+    return cudaGetLastError();
+}
+
+size_t varchar_temp_bytes(uint64_t rows, uint32_t TR) {
+    uint64_t tiles = (rows + TR - 1) / TR;
+    return align256(tiles * 4) + align256((tiles + 1) * 8) + scan_temp_bytes(tiles) + 256;
+}
+
+cudaError_t launch_varchar_plan(const Launch &L, const ColView &col, uint64_t rows, uint32_t TR,
+                                void *temp, unsigned long long *total_pages_dev) {
+    set_var_attrs();
+    const uint64_t tiles = (rows + TR - 1) / TR;
+    char *t = reinterpret_cast<char *>(temp);
+    uint32_t *tile_pages = reinterpret_cast<uint32_t *>(t);
+    uint64_t *tile_base = reinterpret_cast<uint64_t *>(t + align256(tiles * 4));
+    void *scan_tmp = t + align256(tiles * 4) + align256((tiles + 1) * 8);
+    if (tiles) {
+        uint64_t g = tiles, cap = (uint64_t)L.num_sms * 2;
+        if (g > cap) g = cap;
+        k_varchar_plan<<<(unsigned)g, kMatThreads, var_dyn_smem(TR), L.stream>>>(col, rows, TR, tile_pages);
+        count_launches(1);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    cudaError_t e = scan_u32_to_u64(L, tile_pages, tile_base, tiles, scan_tmp);
+    if (e != cudaSuccess) return e;
+    return cudaMemcpyAsync(total_pages_dev, tile_base + tiles, sizeof(unsigned long long),
+                           cudaMemcpyDeviceToDevice, L.stream);
+}
+
+cudaError_t launch_varchar_write(const Launch &L, const ColView &col, uint64_t rows, uint32_t TR,
+                                 void *temp, uint8_t *out) {
+    set_var_attrs();
+    const uint64_t tiles = (rows + TR - 1) / TR;
+    if (!tiles) return cudaSuccess;
+    const uint64_t *tile_base =
+        reinterpret_cast<const uint64_t *>(reinterpret_cast<char *>(temp) + align256(tiles * 4));
+    uint64_t g = tiles, cap = (uint64_t)L.num_sms * 2;
+    if (g > cap) g = cap;
+    k_varchar_write<<<(unsigned)g, kMatThreads, var_dyn_smem(TR), L.stream>>>(col, rows, TR, tile_base, out);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+} // namespace cj

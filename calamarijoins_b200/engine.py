@@ -1,0 +1,186 @@
+"""Execution entry points mirroring the reference's Contest namespace.
+
+  build_context()            Contest::build_context   (plan.h:380)
+  destroy_context(ctx)       Contest::destroy_context (plan.h:382)
+  execute(plan, ctx, stats)  Contest::execute         (plan.h:384; src/execute.cpp:311-325)
+  TimingStats                Contest::TimingStats     (plan.h:370-378)
+
+Errors raise CJError carrying the library's status code (the reference
+throws std::bad_alloc / std::runtime_error).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+from typing import Optional
+
+import numpy as np
+
+from . import _lib
+from ._lib import PAGE_SIZE, check, lib
+from .plan import Column, ColumnarTable, DataType, Plan, PlanDescriptor
+
+
+@dataclass
+class TimingStats:
+    hashtable_build_ms: int = 0
+    hash_join_probe_ms: int = 0
+    nested_loop_join_ms: int = 0
+    materialize_ms: int = 0
+    setup_ms: int = 0
+    total_execution_ms: int = 0
+    intermediate_ms: int = 0
+    # finer statistics of the call (cj_exec_stats)
+    exec: dict = field(default_factory=dict)
+
+
+class Context:
+    """A device context: CUDA device, stream, memory pool (cj_context)."""
+
+    def __init__(self, device: int = -1):
+        h = C.c_void_p()
+        check(lib().cj_context_create(int(device), C.byref(h)))
+        self.handle = h.value
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib().cj_context_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        self.close()
+
+    def set_option(self, option: int, value: int):
+        check(lib().cj_context_set_option(self.handle, int(option), int(value)))
+
+    def get_option(self, option: int) -> int:
+        v = C.c_int64()
+        check(lib().cj_context_get_option(self.handle, int(option), C.byref(v)))
+        return v.value
+
+    def memory(self):
+        u, r = C.c_uint64(), C.c_uint64()
+        check(lib().cj_context_memory(self.handle, C.byref(u), C.byref(r)))
+        return u.value, r.value
+
+    def profile(self) -> dict:
+        n = C.c_uint64()
+        check(lib().cj_profile_count(self.handle, C.byref(n)))
+        out = {}
+        for i in range(n.value):
+            name, launches, us = C.c_char_p(), C.c_uint64(), C.c_double()
+            check(lib().cj_profile_entry(self.handle, i, C.byref(name), C.byref(launches), C.byref(us)))
+            out[name.value.decode()] = (launches.value, us.value)
+        return out
+
+    def profile_reset(self):
+        check(lib().cj_profile_reset(self.handle))
+
+
+class ResidentTable:
+    """A table whose pages live in device memory (cj_table)."""
+
+    def __init__(self, ctx: Context, table: ColumnarTable):
+        self.ctx = ctx
+        self.num_rows = table.num_rows
+        self.types = [c.type for c in table.columns]
+        keep = []
+        cols = (_lib.ColumnDesc * max(len(table.columns), 1))()
+        for c, col in enumerate(table.columns):
+            ptrs = col.page_pointers()
+            keep.append(ptrs)
+            cols[c].type = int(col.type)
+            cols[c].num_pages = col.num_pages
+            cols[c].pages = C.cast(ptrs, C.POINTER(C.c_void_p))
+        td = _lib.TableDesc(table.num_rows, len(table.columns), cols)
+        h = C.c_void_p()
+        check(lib().cj_table_upload(ctx.handle, C.byref(td), C.byref(h)))
+        self.handle = h.value
+
+    def free(self):
+        if getattr(self, "handle", None):
+            lib().cj_table_free(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        self.free()
+
+
+class Result:
+    """A cj_result: the root output, pages on the host (pinned) or device."""
+
+    def __init__(self, handle: int):
+        self.handle = handle
+        n = C.c_uint64()
+        check(lib().cj_result_num_rows(handle, C.byref(n)))
+        self.num_rows = n.value
+        check(lib().cj_result_num_columns(handle, C.byref(n)))
+        self.num_columns = n.value
+
+    def column_info(self, c: int):
+        t, np_, hp = C.c_int32(), C.c_uint64(), C.c_void_p()
+        check(lib().cj_result_column(self.handle, c, C.byref(t), C.byref(np_), C.byref(hp)))
+        return DataType(t.value), np_.value, hp.value
+
+    def host_pages(self, c: int) -> np.ndarray:
+        """Zero-copy view of column c's pinned host pages (valid until free)."""
+        _, n, ptr = self.column_info(c)
+        if not n:
+            return np.zeros((0, PAGE_SIZE), dtype=np.uint8)
+        if not ptr:
+            raise ValueError("result kept on the device; use copy_column")
+        buf = (C.c_uint8 * (n * PAGE_SIZE)).from_address(ptr)
+        return np.frombuffer(buf, dtype=np.uint8).reshape(n, PAGE_SIZE)
+
+    def copy_column(self, c: int) -> np.ndarray:
+        _, n, _ = self.column_info(c)
+        out = np.zeros((n, PAGE_SIZE), dtype=np.uint8)
+        if n:
+            check(lib().cj_result_copy_column(self.handle, c, out.ctypes.data, out.nbytes))
+        return out
+
+    def to_columnar(self) -> ColumnarTable:
+        cols = []
+        for c in range(self.num_columns):
+            t, _, _ = self.column_info(c)
+            cols.append(Column(t, self.copy_column(c)))
+        return ColumnarTable(self.num_rows, cols)
+
+    def free(self):
+        if getattr(self, "handle", None):
+            lib().cj_result_free(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        self.free()
+
+
+def build_context(device: int = -1) -> Context:
+    return Context(device)
+
+
+def destroy_context(ctx: Context) -> None:
+    ctx.close()
+
+
+def execute_raw(plan: Plan, ctx: Context, flags: int = 0, desc: Optional[PlanDescriptor] = None):
+    """Runs a plan; returns (Result, TimingStats)."""
+    d = desc or PlanDescriptor(plan)
+    h = C.c_void_p()
+    ts, es = _lib.TimingStatsC(), _lib.ExecStatsC()
+    check(lib().cj_execute(ctx.handle, C.byref(d.desc), int(flags), C.byref(h), C.byref(ts), C.byref(es)))
+    stats = TimingStats(**{n: getattr(ts, n) for n, _ in _lib.TimingStatsC._fields_})
+    stats.exec = {n: getattr(es, n) for n, _ in _lib.ExecStatsC._fields_}
+    return Result(h.value), stats
+
+
+def execute(plan: Plan, ctx: Context, stats_out: Optional[TimingStats] = None) -> ColumnarTable:
+    """Contest::execute: runs the plan, returns the root's ColumnarTable."""
+    res, st = execute_raw(plan, ctx)
+    try:
+        out = res.to_columnar()
+    finally:
+        res.free()
+    if stats_out is not None:
+        stats_out.__dict__.update(st.__dict__)
+    return out

@@ -1,0 +1,310 @@
+/*
+ * cj_b200.h — C ABI of the B200 join-pipeline library (libcj_b200.so).
+ *
+ * The library executes CalamariJoins-style equi-join plans on one NVIDIA
+ * B200: paged columnar inputs (8 KiB pages, INT32 / INT64 / FP64 / VARCHAR,
+ * NULL bitmaps, long-string pages) go in, a paged columnar result comes out.
+ * Everything between (page decode, radix-partitioned hash build with Bloom
+ * tags, probe, nested-loop join for tiny build sides, late-materialised
+ * intermediates, page writing) runs as CUDA kernels on the device.
+ *
+ * Conventions
+ *   - Every entry point returns a cj_status (0 = CJ_OK) and never throws or
+ *     aborts. cj_last_error() returns a message for the calling thread.
+ *   - Only plain C types and pointers cross this boundary.
+ *   - Host page pointers may point to read-only memory; the library never
+ *     writes input pages.
+ *   - A cj_context is used by one host thread at a time (the reference's
+ *     execute() is not re-entrant either: src/execute.cpp:311-313 resets a
+ *     global arena). Different contexts may be used concurrently.
+ *
+ * Reference interfaces replaced (paths relative to the CalamariJoins tree):
+ *   Contest::build_context()   include/data_model/plan.h:380, src/execute.cpp:327
+ *   Contest::destroy_context() include/data_model/plan.h:382, src/execute.cpp:329
+ *   Contest::execute()         include/data_model/plan.h:384, src/execute.cpp:311-325
+ *   Contest::TimingStats       include/data_model/plan.h:370-378
+ *   Plan / PlanNode / ScanNode / JoinNode   include/data_model/plan.h:46-72, 149-185
+ *   ColumnarTable / Column / Page           include/data_model/plan.h:75-147
+ *   DataType                                include/foundation/attribute.h:7-12
+ *   ColumnInserter<T> (page encoder)        include/data_model/plan.h:187-366
+ */
+#ifndef CJ_B200_H
+#define CJ_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CJ_PAGE_SIZE 8192u
+#define CJ_ABI_VERSION 1u
+
+/* ------------------------------------------------------------------------ */
+/* Status codes                                                              */
+/* ------------------------------------------------------------------------ */
+typedef enum cj_status {
+    CJ_OK = 0,
+    CJ_ERR_INVALID_ARGUMENT = 1, /* null pointer, bad index, bad flag        */
+    CJ_ERR_INVALID_PLAN = 2,     /* plan refers to missing nodes/columns,
+                                    declared type differs from column type   */
+    CJ_ERR_MALFORMED_PAGE = 3,   /* page header/bitmap inconsistent with the
+                                    table's declared row count               */
+    CJ_ERR_OUT_OF_MEMORY = 4,    /* device or pinned-host allocation failed  */
+    CJ_ERR_CUDA = 5,             /* any other CUDA runtime error             */
+    CJ_ERR_UNSUPPORTED = 6,      /* e.g. FP64 or VARCHAR join keys           */
+    CJ_ERR_LIMIT = 7,            /* a documented size limit is exceeded      */
+    CJ_ERR_NO_DEVICE = 8,        /* no CUDA device visible                   */
+    CJ_ERR_REJECTED = 9,         /* serving: admission refused (budget)      */
+    CJ_ERR_TIMEOUT = 10,         /* serving: wait gave up                    */
+    CJ_ERR_CANCELLED = 11,       /* serving: request cancelled               */
+    CJ_ERR_INTERNAL = 12         /* library invariant violated               */
+} cj_status;
+
+/* Values equal DataType's enumerators (include/foundation/attribute.h:7-12). */
+typedef enum cj_data_type {
+    CJ_INT32 = 0,
+    CJ_INT64 = 1,
+    CJ_FP64 = 2,
+    CJ_VARCHAR = 3
+} cj_data_type;
+
+/* Values equal NodeType's enumerators (include/data_model/plan.h:46-49). */
+typedef enum cj_node_type {
+    CJ_NODE_HASH_JOIN = 0,
+    CJ_NODE_SCAN = 1
+} cj_node_type;
+
+/* ------------------------------------------------------------------------ */
+/* Plan description (POD mirror of Plan, include/data_model/plan.h:149-185)  */
+/* ------------------------------------------------------------------------ */
+
+/* One column of an input table: a type and an array of host pointers to
+ * CJ_PAGE_SIZE-byte pages (Column, plan.h:82-142). */
+typedef struct cj_column_desc {
+    int32_t type;             /* cj_data_type                               */
+    uint32_t reserved;
+    uint64_t num_pages;
+    const void *const *pages; /* num_pages host pointers                    */
+} cj_column_desc;
+
+/* ColumnarTable (plan.h:144-147). */
+typedef struct cj_table_desc {
+    uint64_t num_rows;
+    uint64_t num_columns;
+    const cj_column_desc *columns;
+} cj_table_desc;
+
+/* One entry of PlanNode::output_attrs: (column index, declared type). */
+typedef struct cj_attr {
+    uint64_t index;
+    int32_t type; /* cj_data_type */
+    uint32_t reserved;
+} cj_attr;
+
+/* PlanNode (plan.h:62-72): a ScanNode or a JoinNode plus output_attrs. */
+typedef struct cj_plan_node {
+    int32_t node_type;      /* cj_node_type                                 */
+    int32_t build_left;     /* JoinNode::build_left (a hint; results do not
+                               depend on it)                                */
+    uint64_t base_table_id; /* ScanNode::base_table_id                      */
+    uint64_t left, right;   /* JoinNode children (node indices)             */
+    uint64_t left_attr, right_attr; /* join keys, indices into the children's
+                                       output_attrs                          */
+    uint64_t num_output_attrs;
+    const cj_attr *output_attrs;
+} cj_plan_node;
+
+typedef struct cj_table cj_table; /* device-resident table (see below)    */
+
+/* Plan (plan.h:149-185). Input i is taken from resident_inputs[i] when that
+ * array is non-NULL and its entry is non-NULL, else from inputs[i]. */
+typedef struct cj_plan_desc {
+    uint64_t num_nodes;
+    const cj_plan_node *nodes;
+    uint64_t num_inputs;
+    const cj_table_desc *inputs;       /* may be NULL if all inputs resident */
+    cj_table *const *resident_inputs;  /* may be NULL                        */
+    uint64_t root;
+} cj_plan_desc;
+
+/* Contest::TimingStats (plan.h:370-378), same fields and order. */
+typedef struct cj_timing_stats {
+    int64_t hashtable_build_ms;
+    int64_t hash_join_probe_ms;
+    int64_t nested_loop_join_ms;
+    int64_t materialize_ms;
+    int64_t setup_ms;
+    int64_t total_execution_ms;
+    int64_t intermediate_ms;
+} cj_timing_stats;
+
+/* Finer-grained statistics of one cj_execute call (no reference
+ * counterpart; TimingStats' millisecond integers are too coarse for a GPU). */
+typedef struct cj_exec_stats {
+    double upload_us;        /* host->device page copies                    */
+    double decode_us;        /* page decode kernels                         */
+    double build_us;         /* hash-table build kernels                    */
+    double probe_us;         /* hash probe kernels                          */
+    double nested_loop_us;   /* nested-loop kernels                         */
+    double intermediate_us;  /* row-id gathers for non-root joins           */
+    double materialize_us;   /* output page writers                         */
+    double download_us;      /* device->host result copy                    */
+    double total_us;         /* wall time of the call                       */
+    uint64_t h2d_bytes;
+    uint64_t d2h_bytes;
+    uint64_t num_joins;
+    uint64_t num_hash_joins;
+    uint64_t num_nested_loop_joins;
+    uint64_t probe_rows;     /* probe-side rows over all joins              */
+    uint64_t matches;        /* match pairs over all joins                  */
+    uint64_t probe_reruns;   /* probes re-run after output overflow         */
+    uint64_t output_rows;
+    uint64_t output_pages;
+    uint64_t kernel_launches;
+} cj_exec_stats;
+
+/* ------------------------------------------------------------------------ */
+/* Context: device, streams and stream-ordered device memory pool            */
+/* ------------------------------------------------------------------------ */
+typedef struct cj_context cj_context;
+
+/* Creates a context on CUDA device `device` (-1 = current device).
+ * Replaces Contest::build_context() (plan.h:380), which returns nullptr in the
+ * reference (src/execute.cpp:327). */
+int cj_context_create(int device, cj_context **out);
+
+/* Replaces Contest::destroy_context(void*) (plan.h:382). Frees everything the
+ * context owns; results and resident tables must be freed first. */
+void cj_context_destroy(cj_context *ctx);
+
+/* Tunables, each also settable by environment variable CJ_<NAME>. */
+typedef enum cj_option {
+    CJ_OPT_NESTED_LOOP_MAX_BUILD = 0, /* build rows below which the nested-loop
+                                         kernel is used (reference: 8,
+                                         src/execute.cpp:236-238); default 64 */
+    CJ_OPT_SLOTS_PER_PARTITION = 1,   /* hash directory slots per radix
+                                         partition (power of two); 0 = auto */
+    CJ_OPT_PROFILE_KERNELS = 2,       /* 1 = time every kernel with events   */
+    CJ_OPT_BLOCK_THREADS = 3,         /* threads per CTA of streaming kernels;
+                                         0 = auto                           */
+    CJ_OPT_VARCHAR_TILE_ROWS = 4,     /* rows per VARCHAR page-packing tile  */
+    CJ_OPT_CTAS_PER_SM = 5            /* resident CTAs per SM for persistent
+                                         grids; 0 = auto                    */
+} cj_option;
+int cj_context_set_option(cj_context *ctx, int32_t option, int64_t value);
+int cj_context_get_option(const cj_context *ctx, int32_t option, int64_t *value);
+
+/* Per-kernel profile (enabled by CJ_OPT_PROFILE_KERNELS): `index`-th kernel
+ * name seen since the last reset, its launch count and total device time. */
+int cj_profile_reset(cj_context *ctx);
+int cj_profile_count(const cj_context *ctx, uint64_t *num_kernels);
+int cj_profile_entry(const cj_context *ctx, uint64_t index, const char **name,
+                     uint64_t *launches, double *total_us);
+
+/* The cudaStream_t every kernel of this context runs on (for callers that
+ * time or order their own work against it). */
+int cj_context_stream(const cj_context *ctx, void **stream);
+
+/* Device memory currently held by the context's pool (bytes in use, bytes
+ * reserved) — for admission control and leak tests. */
+int cj_context_memory(const cj_context *ctx, uint64_t *used_bytes,
+                      uint64_t *reserved_bytes);
+
+/* ------------------------------------------------------------------------ */
+/* Resident tables: pages uploaded once and kept in HBM                      */
+/* ------------------------------------------------------------------------ */
+
+/* Uploads every column of `table` into device memory. */
+int cj_table_upload(cj_context *ctx, const cj_table_desc *table,
+                    cj_table **out);
+
+/* Adopts pages that are already in device memory: column c's pages are
+ * num_pages[c] consecutive CJ_PAGE_SIZE-byte pages at device_pages[c]. The
+ * memory stays owned by the caller and must outlive the cj_table. */
+int cj_table_from_device(cj_context *ctx, uint64_t num_rows,
+                         uint64_t num_columns, const int32_t *types,
+                         const uint64_t *num_pages,
+                         const void *const *device_pages, cj_table **out);
+
+/* Device pointer of a resident column's pages (for tests and tools). */
+int cj_table_column_pages(const cj_table *table, uint64_t column,
+                          const void **device_pages, uint64_t *num_pages);
+
+void cj_table_free(cj_table *table);
+
+/* ------------------------------------------------------------------------ */
+/* Execution                                                                 */
+/* ------------------------------------------------------------------------ */
+typedef struct cj_result cj_result;
+
+typedef enum cj_exec_flags {
+    CJ_EXEC_DEFAULT = 0,
+    CJ_EXEC_RESULT_ON_DEVICE = 1 /* keep output pages in HBM; no D2H copy   */
+} cj_exec_flags;
+
+/* Runs `plan` to completion and returns its root result. Replaces
+ * Contest::execute(const Plan&, void*, TimingStats*) (plan.h:384;
+ * src/execute.cpp:311-325). `timing` and `stats` may be NULL.
+ * Semantics: inner equi-join; a NULL key never matches; output columns are
+ * the root's output_attrs over (left columns ++ right columns). An INT32
+ * value equal to INT32_MIN that leaves a non-root join is NULL from then on
+ * (the reference's intermediate encoding, include/data_model/intermediate.h:
+ * 40-63). */
+int cj_execute(cj_context *ctx, const cj_plan_desc *plan, uint32_t flags,
+               cj_result **out, cj_timing_stats *timing, cj_exec_stats *stats);
+
+int cj_result_num_rows(const cj_result *r, uint64_t *num_rows);
+int cj_result_num_columns(const cj_result *r, uint64_t *num_columns);
+
+/* Column `c` of a result: type, page count and, unless the result was kept on
+ * the device, a host pointer to its num_pages consecutive pages. */
+int cj_result_column(const cj_result *r, uint64_t c, int32_t *type,
+                     uint64_t *num_pages, const void **host_pages);
+
+/* Device pointer to column `c`'s consecutive pages (valid until free). */
+int cj_result_column_device(const cj_result *r, uint64_t c,
+                            const void **device_pages);
+
+/* Copies column `c`'s pages to caller memory (dst_bytes >= pages*8192). */
+int cj_result_copy_column(const cj_result *r, uint64_t c, void *dst,
+                          uint64_t dst_bytes);
+
+void cj_result_free(cj_result *r);
+
+/* ------------------------------------------------------------------------ */
+/* Host utilities                                                            */
+/* ------------------------------------------------------------------------ */
+
+/* Page-locked host memory for inputs whose upload should run at full PCIe
+ * speed. */
+int cj_host_alloc(uint64_t bytes, void **out);
+void cj_host_free(void *p);
+
+/* Number of pages ColumnInserter<T> (plan.h:187-366) produces for the given
+ * column; `valid` (one byte per row, nonzero = value present) may be NULL
+ * (no NULLs). For VARCHAR, `offsets` has n+1 entries delimiting the strings
+ * in `chars`. */
+int cj_encode_num_pages(int32_t type, const void *values,
+                        const uint64_t *offsets, const uint8_t *valid,
+                        uint64_t n, uint64_t *num_pages);
+
+/* Encodes a column exactly as ColumnInserter<T>::insert / insert_null /
+ * finalize would (plan.h:187-366), into `out_pages` (capacity pages). For
+ * fixed-width types `values` holds n elements (entries of NULL rows are
+ * ignored); for VARCHAR `values` is the character buffer. */
+int cj_encode_column(int32_t type, const void *values, const uint64_t *offsets,
+                     const uint8_t *valid, uint64_t n, void *out_pages,
+                     uint64_t capacity, uint64_t *num_pages);
+
+/* Message of the last failed call on this thread ("" if none). */
+const char *cj_last_error(void);
+
+/* Library and ABI version, e.g. "cj_b200 1 sm_100a". */
+const char *cj_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CJ_B200_H */

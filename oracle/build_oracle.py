@@ -1,0 +1,101 @@
+"""Build recipe for the oracle (test infrastructure).
+
+Produces
+  oracle/libcj_oracle.so            the C restatement (oracle/cj_oracle.c)
+  oracle/_ref/libcj_ref_t<N>.so     the reference's own execute()
+                                    (CalamariJoins src/execute.cpp), compiled
+                                    from its sources with N worker threads,
+                                    plus oracle/ref_bridge.cpp
+
+The reference is compiled only when its source tree is present (environment
+variable CJ_REFERENCE_DIR, default /root/reference). Its CMake build cannot
+run offline (FetchContent of Catch2, abseil, re2, fmt, range-v3, DuckDB), so
+this recipe compiles the one translation unit on the join path directly:
+fmt comes header-only from PyTorch's include tree, and oracle/ref_shim/
+stands in for re2 (unused on the join path), the range-v3 table loader
+(unused) and the hard-coded hardware constants. The build targets
+x86-64-v3 (AVX2 + SSE4.2 CRC32) instead of -march=native so that the library
+also runs on the GPU host, whose CPU model may differ from the build host.
+
+Usage: python oracle/build_oracle.py [--threads 32,64,...]
+"""
+from __future__ import annotations
+
+import argparse
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+DEFAULT_THREADS = (8, 32, 64, 128, 192, 256)
+
+
+def _run(cmd: list[str]) -> None:
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if res.returncode != 0:
+        raise RuntimeError("build failed: " + " ".join(cmd) + "\n" + res.stderr[-4000:])
+
+
+def _newer(target: str, sources: list[str]) -> bool:
+    if not os.path.exists(target):
+        return False
+    t = os.path.getmtime(target)
+    return all(os.path.getmtime(s) <= t for s in sources if os.path.exists(s))
+
+
+def build_oracle(force: bool = False) -> str:
+    src = os.path.join(HERE, "cj_oracle.c")
+    hdrs = [os.path.join(HERE, "cj_oracle.h"), os.path.join(HERE, "..", "include", "cj_b200.h")]
+    out = os.path.join(HERE, "libcj_oracle.so")
+    if force or not _newer(out, [src] + hdrs):
+        _run(["gcc", "-O2", "-g", "-std=gnu11", "-shared", "-fPIC", "-Wall", "-Wno-unused-function",
+              src, "-o", out])
+    return out
+
+
+def reference_dir() -> str | None:
+    ref = os.environ.get("CJ_REFERENCE_DIR", "/root/reference")
+    if os.path.isfile(os.path.join(ref, "src", "execute.cpp")):
+        return ref
+    return None
+
+
+def build_reference(threads=DEFAULT_THREADS, force: bool = False) -> list[str]:
+    ref = reference_dir()
+    if ref is None:
+        return []
+    try:
+        import torch  # only for the bundled header-only fmt
+        fmt_inc = os.path.join(os.path.dirname(torch.__file__), "include")
+    except Exception:  # pragma: no cover
+        return []
+    outdir = os.path.join(HERE, "_ref")
+    os.makedirs(outdir, exist_ok=True)
+    sources = [os.path.join(ref, "src", "execute.cpp"), os.path.join(HERE, "ref_bridge.cpp")]
+    shim = os.path.join(HERE, "ref_shim")
+    deps = sources + [os.path.join(shim, "platform", "hardware.h")]
+    built = []
+    for t in threads:
+        out = os.path.join(outdir, f"libcj_ref_t{t}.so")
+        if force or not _newer(out, deps):
+            _run(["g++", "-std=c++17", "-O3", "-march=x86-64-v3", "-fpermissive", "-w",
+                  "-DFMT_HEADER_ONLY", f"-DSPC__THREAD_COUNT={t}",
+                  "-I", shim, "-I", os.path.join(ref, "include"), "-I", fmt_inc,
+                  "-shared", "-fPIC", *sources, "-o", out, "-lpthread"])
+        built.append(out)
+    return built
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--threads", default=",".join(str(t) for t in DEFAULT_THREADS))
+    ap.add_argument("--force", action="store_true")
+    a = ap.parse_args(argv)
+    print(build_oracle(a.force))
+    for p in build_reference(tuple(int(x) for x in a.threads.split(",")), a.force):
+        print(p)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())
