@@ -77,6 +77,25 @@ class ExecStatsC(C.Structure):
             "kernel_launches")])
 
 
+class BatchStatsC(C.Structure):
+    _fields_ = ([(n, C.c_uint64) for n in (
+        "num_plans", "num_levels", "num_joins", "num_hash_joins", "num_nested_loop_joins", "probe_rows",
+        "matches", "probe_reruns", "kernel_launches", "syncs", "h2d_bytes", "d2h_bytes")]
+        + [("total_us", C.c_double)])
+
+
+class ServerConfigC(C.Structure):
+    _fields_ = [("device", C.c_int32), ("slots", C.c_uint32), ("memory_budget", C.c_uint64),
+                ("exec_flags", C.c_uint32), ("reserved", C.c_uint32)]
+
+
+class ServerStatsC(C.Structure):
+    _fields_ = ([(n, C.c_uint64) for n in (
+        "submitted", "completed", "failed", "rejected", "cancelled", "queued", "running", "admitted_bytes",
+        "peak_admitted_bytes", "memory_budget")]
+        + [(n, C.c_double) for n in ("p50_us", "p99_us", "mean_us", "max_us", "wall_s", "plans_per_s")])
+
+
 # every function of include/cj_b200.h: name -> (restype, argtypes)
 _P = C.c_void_p
 _SIGS = {
@@ -97,6 +116,8 @@ _SIGS = {
     "cj_table_free": (None, [_P]),
     "cj_execute": (C.c_int, [_P, C.POINTER(PlanDesc), C.c_uint32, C.POINTER(_P),
                              C.POINTER(TimingStatsC), C.POINTER(ExecStatsC)]),
+    "cj_execute_batch": (C.c_int, [_P, C.POINTER(PlanDesc), C.c_uint64, C.c_uint32, C.POINTER(_P),
+                                   C.POINTER(C.c_int32), C.POINTER(BatchStatsC)]),
     "cj_result_num_rows": (C.c_int, [_P, C.POINTER(C.c_uint64)]),
     "cj_result_num_columns": (C.c_int, [_P, C.POINTER(C.c_uint64)]),
     "cj_result_column": (C.c_int, [_P, C.c_uint64, C.POINTER(C.c_int32), C.POINTER(C.c_uint64),
@@ -104,6 +125,13 @@ _SIGS = {
     "cj_result_column_device": (C.c_int, [_P, C.c_uint64, C.POINTER(_P)]),
     "cj_result_copy_column": (C.c_int, [_P, C.c_uint64, _P, C.c_uint64]),
     "cj_result_free": (None, [_P]),
+    "cj_server_create": (C.c_int, [C.POINTER(ServerConfigC), C.POINTER(_P)]),
+    "cj_server_submit": (C.c_int, [_P, C.POINTER(PlanDesc), C.POINTER(C.c_uint64)]),
+    "cj_server_wait": (C.c_int, [_P, C.c_uint64, C.c_int64, C.POINTER(_P), C.POINTER(ExecStatsC)]),
+    "cj_server_cancel": (C.c_int, [_P, C.c_uint64]),
+    "cj_server_get_stats": (C.c_int, [_P, C.POINTER(ServerStatsC), C.c_int]),
+    "cj_server_estimate": (C.c_int, [C.POINTER(PlanDesc), C.POINTER(C.c_uint64)]),
+    "cj_server_destroy": (None, [_P]),
     "cj_host_alloc": (C.c_int, [C.c_uint64, C.POINTER(_P)]),
     "cj_host_free": (None, [_P]),
     "cj_encode_num_pages": (C.c_int, [C.c_int32, _P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint8),

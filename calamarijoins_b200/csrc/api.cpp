@@ -10,12 +10,7 @@
 
 namespace {
 
-thread_local std::string g_last_error;
-
-int set_error(int code, const std::string &msg) {
-    g_last_error = msg;
-    return code;
-}
+int set_error(int code, const std::string &msg) { return cj::set_last_error(code, msg); }
 
 #define API_BEGIN try {
 #define API_END                                                                 \
@@ -29,23 +24,8 @@ int set_error(int code, const std::string &msg) {
     catch (...) {                                                               \
         return set_error(CJ_ERR_INTERNAL, "unexpected exception");              \
     }                                                                           \
-    g_last_error.clear();                                                       \
+    cj::clear_last_error();                                                       \
     return CJ_OK;
-
-/* The 2048 smallest 16-bit values with exactly five bits set, ascending:
- * the Bloom tag table of the reference (include/join_execution/
- * bloom_tags.h:35-263), regenerated. */
-void make_bloom(uint16_t *out) {
-    int n = 0;
-    for (uint32_t v = 0; v < 65536 && n < 2048; ++v)
-        if (__builtin_popcount(v) == 5) out[n++] = (uint16_t)v;
-}
-
-int64_t env_opt(const char *name, int64_t dflt) {
-    const char *v = std::getenv(name);
-    if (!v || !*v) return dflt;
-    return std::strtoll(v, nullptr, 10);
-}
 
 void set_device(const cj::Context *ctx) { cudaSetDevice(ctx->device); }
 
@@ -53,66 +33,16 @@ void set_device(const cj::Context *ctx) { cudaSetDevice(ctx->device); }
 
 extern "C" {
 
-const char *cj_last_error(void) { return g_last_error.c_str(); }
+const char *cj_last_error(void) { return cj::last_error(); }
 
 const char *cj_version(void) { return "cj_b200 1 sm_100a"; }
 
 int cj_context_create(int device, cj_context **out) {
     if (!out) return set_error(CJ_ERR_INVALID_ARGUMENT, "out is null");
     *out = nullptr;
-    cj_context *c = nullptr;
     API_BEGIN
-    int n = 0;
-    cudaError_t e = cudaGetDeviceCount(&n);
-    if (e != cudaSuccess || n == 0) {
-        cudaGetLastError();
-        cj::fail(CJ_ERR_NO_DEVICE, "no CUDA device visible");
-    }
-    if (device < 0) cj::check_cuda(cudaGetDevice(&device), "cudaGetDevice");
-    if (device >= n) cj::fail(CJ_ERR_INVALID_ARGUMENT, "device ordinal out of range");
-    cj::check_cuda(cudaSetDevice(device), "cudaSetDevice");
-    c = new cj_context();
-    c->device = device;
-    cj::check_cuda(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device), "attr");
-    cj::check_cuda(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "stream");
-    cudaMemPoolProps props{};
-    props.allocType = cudaMemAllocationTypePinned;
-    props.location.type = cudaMemLocationTypeDevice;
-    props.location.id = device;
-    cj::check_cuda(cudaMemPoolCreate(&c->pool, &props), "cudaMemPoolCreate");
-    uint64_t keep = UINT64_MAX;
-    cj::check_cuda(cudaMemPoolSetAttribute(c->pool, cudaMemPoolAttrReleaseThreshold, &keep), "pool attr");
-    uint16_t bloom[2048];
-    make_bloom(bloom);
-    cj::check_cuda(cudaMalloc(&c->d_bloom, sizeof(bloom)), "cudaMalloc");
-    cj::check_cuda(cudaMemcpy(c->d_bloom, bloom, sizeof(bloom), cudaMemcpyHostToDevice), "bloom upload");
-    cj::check_cuda(cudaMalloc(&c->d_status, sizeof(cj::StatusBlock)), "cudaMalloc");
-    cj::check_cuda(cudaMemset(c->d_status, 0, sizeof(cj::StatusBlock)), "memset");
-    cj::check_cuda(cudaHostAlloc(reinterpret_cast<void **>(&c->h_status), sizeof(cj::StatusBlock), 0), "host");
-    std::memset(c->h_status, 0, sizeof(cj::StatusBlock));
-    for (int i = 0; i < 2; ++i) {
-        cj::check_cuda(cudaHostAlloc(&c->staging[i], c->staging_bytes, 0), "staging");
-        cj::check_cuda(cudaEventCreateWithFlags(&c->staging_ev[i], cudaEventDisableTiming), "event");
-    }
-    c->opt.nested_loop_max_build = env_opt("CJ_NESTED_LOOP_MAX_BUILD", c->opt.nested_loop_max_build);
-    c->opt.slots_per_partition = env_opt("CJ_SLOTS_PER_PARTITION", c->opt.slots_per_partition);
-    c->opt.profile_kernels = env_opt("CJ_PROFILE_KERNELS", c->opt.profile_kernels);
-    c->opt.block_threads = env_opt("CJ_BLOCK_THREADS", c->opt.block_threads);
-    c->opt.varchar_tile_rows = env_opt("CJ_VARCHAR_TILE_ROWS", c->opt.varchar_tile_rows);
-    c->opt.ctas_per_sm = env_opt("CJ_CTAS_PER_SM", c->opt.ctas_per_sm);
-    *out = c;
-    c = nullptr;
-    }
-    catch (const cj::Error &e) {
-        delete c;
-        return set_error(e.code, e.msg);
-    }
-    catch (...) {
-        delete c;
-        return set_error(CJ_ERR_INTERNAL, "unexpected exception");
-    }
-    g_last_error.clear();
-    return CJ_OK;
+    *out = static_cast<cj_context *>(cj::create_context(device, nullptr));
+    API_END
 }
 
 void cj_context_destroy(cj_context *ctx) {
@@ -290,7 +220,28 @@ int cj_execute(cj_context *ctx, const cj_plan_desc *plan, uint32_t flags, cj_res
         cudaStreamSynchronize(ctx->stream);
         return set_error(CJ_ERR_INTERNAL, "unexpected exception");
     }
-    g_last_error.clear();
+    cj::clear_last_error();
+    return CJ_OK;
+}
+
+int cj_execute_batch(cj_context *ctx, const cj_plan_desc *plans, uint64_t n, uint32_t flags, cj_result **results,
+                     int32_t *statuses, cj_batch_stats *stats) {
+    if (!ctx || (n && (!plans || !results))) return set_error(CJ_ERR_INVALID_ARGUMENT, "null argument");
+    set_device(ctx);
+    try {
+        cj::execute_batch(*ctx, plans, (size_t)n, flags, results, statuses, stats);
+    } catch (const cj::Error &e) {
+        cudaStreamSynchronize(ctx->stream);
+        cudaGetLastError();
+        return set_error(e.code, e.msg);
+    } catch (const std::bad_alloc &) {
+        cudaStreamSynchronize(ctx->stream);
+        return set_error(CJ_ERR_OUT_OF_MEMORY, "host allocation failed");
+    } catch (...) {
+        cudaStreamSynchronize(ctx->stream);
+        return set_error(CJ_ERR_INTERNAL, "unexpected exception");
+    }
+    cj::clear_last_error();
     return CJ_OK;
 }
 

@@ -142,6 +142,24 @@ cudaError_t launch_decode_varchar(const Launch &L, const uint8_t *pages,
                                   uint64_t num_pages,
                                   const uint64_t *row_start, uint64_t max_rows,
                                   uint64_t *desc, uint32_t *valid);
+/* Grouped decode of many columns: task k's pages are global pages
+ * [page_base, page_base + num_pages). rows_pp / row_start are scratch of
+ * total_pages / total_pages + 1 entries; scan_temp of
+ * scan_temp_bytes(total_pages). */
+struct DecodeTask {
+    const uint8_t *pages;
+    uint64_t num_pages;
+    uint64_t page_base;
+    uint64_t rows;
+    int32_t type;
+    int32_t pad;
+    void *values;
+    uint64_t *desc;
+    uint32_t *valid; /* zeroed */
+};
+cudaError_t launch_decode_grouped(const Launch &L, const DecodeTask *tasks_dev, uint32_t ntasks,
+                                  uint64_t total_pages, uint32_t *rows_pp, uint64_t *row_start,
+                                  void *scan_temp);
 /* Raises DEV_ERR_ROW_COUNT unless *total == expected. */
 cudaError_t launch_check_rows(const Launch &L, const uint64_t *total, uint64_t expected);
 
@@ -156,6 +174,35 @@ size_t build_tuple_bytes(int key_bytes);
 cudaError_t launch_build(const Launch &L, const BuildPlan &bp, const ColView &key,
                          const uint16_t *bloom, uint64_t *dir, void *tuples,
                          void *temp);
+
+/* Grouped build over the hash joins of one batch level. Each task
+ * partitions its own rows into its own part_buf; chunk_base / part_base /
+ * cell_base place its chunks, partitions and histogram cells in the global
+ * numbering (prefix sums over the tasks). */
+struct BuildGeometry {
+    uint32_t grid;  /* chunks of the hist / scatter passes */
+    uint32_t chunk; /* rows per chunk                      */
+    uint64_t cells; /* partitions x chunks                 */
+};
+BuildGeometry build_geometry(const Launch &L, const BuildPlan &bp);
+struct BuildTask {
+    ColView key;
+    uint32_t n;
+    int32_t log2_slots;
+    int32_t log2_parts;
+    uint32_t grid;
+    uint32_t chunk;
+    uint32_t chunk_base;
+    uint32_t part_base;
+    uint64_t cell_base;
+    uint64_t *dir;
+    void *tuples;
+    void *part_buf; /* n tuples of scratch */
+};
+size_t build_grouped_temp_bytes(uint64_t total_cells);
+cudaError_t launch_build_grouped(const Launch &L, const BuildTask *tasks_dev, uint32_t ntasks, uint32_t total_chunks,
+                                 uint32_t total_parts, uint64_t total_cells, uint32_t max_parts, uint32_t max_slots,
+                                 const uint16_t *bloom, void *temp);
 
 /* Probe and nested loop share one tiled kernel; `sched` is scratch of
  * probe_sched_bytes(n_probe) bytes (tile tickets and look-back status). */
@@ -173,9 +220,60 @@ cudaError_t launch_nl_probe_tiles(const Launch &L, const ColView &pkey, uint32_t
                                   const int64_t *keys, const uint32_t *rids,
                                   const uint32_t *count, const MatchOut &out, void *sched);
 
+/* Grouped probe over the joins of one batch level. */
+struct ProbeTask {
+    ColView pkey;
+    uint32_t n_probe;
+    int32_t kind;           /* 0 hash, 1 nested loop                       */
+    int32_t build_key_type; /* hash: CJ_INT32 / CJ_INT64 tuples            */
+    int32_t log2_slots;
+    const uint64_t *dir;
+    const void *tuples;
+    const int64_t *nl_keys;
+    const uint32_t *nl_rids;
+    const uint32_t *nl_count;
+    MatchOut out;
+    unsigned long long *status; /* num_tiles look-back words, zeroed        */
+    uint32_t num_tiles;
+    uint32_t tile_base;         /* first global tile of this task           */
+};
+uint32_t probe_tiles(uint32_t n_probe);
+/* `ticket` must be zeroed; each task's status and counter zeroed. */
+cudaError_t launch_probe_grouped(const Launch &L, const ProbeTask *tasks_dev, uint32_t ntasks,
+                                 uint32_t total_tiles, unsigned int *ticket, const uint16_t *bloom);
+struct NlCollectTask {
+    ColView bkey;
+    uint32_t n_build;
+    int64_t *keys;
+    uint32_t *rids;
+    uint32_t *count;
+};
+cudaError_t launch_nl_collect_grouped(const Launch &L, const NlCollectTask *tasks_dev, uint32_t ntasks);
+
 /* Intermediates: out[i] = src[idx[i]] */
 cudaError_t launch_gather_u32(const Launch &L, const uint32_t *src,
                               const uint32_t *idx, uint64_t n, uint32_t *out);
+
+/* Grouped variants for batches: each task's units are numbered from
+ * page_base / chunk_base in a global sequence (prefix sums over tasks). */
+constexpr uint64_t kGatherChunk = 8192;
+struct GatherTask {
+    const uint32_t *src;
+    const uint32_t *idx;
+    uint32_t *out;
+    uint64_t n;
+    uint64_t chunk_base;
+};
+cudaError_t launch_gather_grouped(const Launch &L, const GatherTask *tasks_dev, uint32_t ntasks,
+                                  uint64_t total_chunks);
+struct PageTask {
+    ColView col;
+    uint64_t rows;
+    uint8_t *out;
+    uint64_t page_base;
+};
+cudaError_t launch_write_fixed_grouped(const Launch &L, const PageTask *tasks_dev, uint32_t ntasks,
+                                      uint64_t total_pages);
 
 /* Output pages */
 uint32_t rows_per_page_fixed(int32_t type);

@@ -2,7 +2,9 @@
  * context.cpp — context resources: stream-ordered device pool, pinned
  * pool, events, status block, page upload.
  */
+#include <cstdlib>
 #include <cstring>
+#include <memory>
 #include <string>
 
 #include "engine.h"
@@ -16,6 +18,14 @@ void count_launches(uint64_t n) { g_launches.fetch_add(n, std::memory_order_rela
 uint64_t launches_so_far() { return g_launches.load(std::memory_order_relaxed); }
 
 void fail(int code, const std::string &msg) { throw Error{code, msg}; }
+
+static thread_local std::string g_last_error;
+int set_last_error(int code, const std::string &msg) {
+    g_last_error = msg;
+    return code;
+}
+void clear_last_error() { g_last_error.clear(); }
+const char *last_error() { return g_last_error.c_str(); }
 
 void check_cuda(cudaError_t e, const char *what) {
     if (e == cudaSuccess) return;
@@ -144,8 +154,76 @@ Context::~Context() {
     if (h_status) cudaFreeHost(h_status);
     if (d_status) cudaFree(d_status);
     if (d_bloom) cudaFree(d_bloom);
-    if (pool) cudaMemPoolDestroy(pool);
+    if (pool && owns_pool) cudaMemPoolDestroy(pool);
     if (stream) cudaStreamDestroy(stream);
+}
+
+static void make_bloom(uint16_t *out) {
+    /* The 2048 smallest 16-bit values with exactly five bits set, ascending:
+     * the Bloom tag table of the reference (include/join_execution/
+     * bloom_tags.h:35-263), regenerated. */
+    int n = 0;
+    for (uint32_t v = 0; v < 65536 && n < 2048; ++v)
+        if (__builtin_popcount(v) == 5) out[n++] = (uint16_t)v;
+}
+
+static int64_t env_opt(const char *name, int64_t dflt) {
+    const char *v = std::getenv(name);
+    if (!v || !*v) return dflt;
+    return std::strtoll(v, nullptr, 10);
+}
+
+cudaMemPool_t create_pool(int device) {
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    cudaMemPool_t pool = nullptr;
+    check_cuda(cudaMemPoolCreate(&pool, &props), "cudaMemPoolCreate");
+    uint64_t keep = UINT64_MAX;
+    check_cuda(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep), "pool attr");
+    return pool;
+}
+
+Context *create_context(int device, cudaMemPool_t shared_pool) {
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n == 0) {
+        cudaGetLastError();
+        fail(CJ_ERR_NO_DEVICE, "no CUDA device visible");
+    }
+    if (device < 0) check_cuda(cudaGetDevice(&device), "cudaGetDevice");
+    if (device >= n) fail(CJ_ERR_INVALID_ARGUMENT, "device ordinal out of range");
+    check_cuda(cudaSetDevice(device), "cudaSetDevice");
+    std::unique_ptr<Context> c(new cj_context());
+    c->device = device;
+    check_cuda(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device), "attr");
+    check_cuda(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "stream");
+    if (shared_pool) {
+        c->pool = shared_pool;
+        c->owns_pool = false;
+    } else {
+        c->pool = create_pool(device);
+    }
+    uint16_t bloom[2048];
+    make_bloom(bloom);
+    check_cuda(cudaMalloc(&c->d_bloom, sizeof(bloom)), "cudaMalloc");
+    check_cuda(cudaMemcpy(c->d_bloom, bloom, sizeof(bloom), cudaMemcpyHostToDevice), "bloom upload");
+    check_cuda(cudaMalloc(&c->d_status, sizeof(StatusBlock)), "cudaMalloc");
+    check_cuda(cudaMemset(c->d_status, 0, sizeof(StatusBlock)), "memset");
+    check_cuda(cudaHostAlloc(reinterpret_cast<void **>(&c->h_status), sizeof(StatusBlock), 0), "host");
+    std::memset(c->h_status, 0, sizeof(StatusBlock));
+    for (int i = 0; i < 2; ++i) {
+        check_cuda(cudaHostAlloc(&c->staging[i], c->staging_bytes, 0), "staging");
+        check_cuda(cudaEventCreateWithFlags(&c->staging_ev[i], cudaEventDisableTiming), "event");
+    }
+    c->opt.nested_loop_max_build = env_opt("CJ_NESTED_LOOP_MAX_BUILD", c->opt.nested_loop_max_build);
+    c->opt.slots_per_partition = env_opt("CJ_SLOTS_PER_PARTITION", c->opt.slots_per_partition);
+    c->opt.profile_kernels = env_opt("CJ_PROFILE_KERNELS", c->opt.profile_kernels);
+    c->opt.block_threads = env_opt("CJ_BLOCK_THREADS", c->opt.block_threads);
+    c->opt.varchar_tile_rows = env_opt("CJ_VARCHAR_TILE_ROWS", c->opt.varchar_tile_rows);
+    c->opt.ctas_per_sm = env_opt("CJ_CTAS_PER_SM", c->opt.ctas_per_sm);
+    return c.release();
 }
 
 /* Host pages -> one consecutive device array. A run of pages that are

@@ -19,37 +19,10 @@
 
 #include "engine.h"
 
+#include "exec_common.h"
+
 namespace cj {
 namespace {
-
-int ceil_log2(uint64_t x) {
-    int l = 0;
-    while ((1ull << l) < x) ++l;
-    return l;
-}
-
-struct Decoded {
-    int32_t type = CJ_INT32;
-    uint64_t rows = 0;
-    ColumnPages src;
-    DevPtr values, valid, desc;
-};
-
-/* A column of a relation: base column (input, col) reached through row-id
- * vector `vec` of the relation (-1: the relation row is the base row). */
-struct RelCol {
-    int32_t type;
-    uint64_t input;
-    uint64_t col;
-    int vec;
-    bool sentinel; /* value left a non-root join: INT32_MIN reads as NULL */
-};
-
-struct Relation {
-    uint64_t rows = 0;
-    std::vector<DevPtr> vecs;
-    std::vector<RelCol> cols;
-};
 
 enum Phase { PH_UPLOAD, PH_DECODE, PH_BUILD, PH_PROBE, PH_NL, PH_INTER, PH_MAT, PH_DOWNLOAD, PH_COUNT };
 
@@ -125,25 +98,12 @@ class Executor {
     std::vector<PhaseEv> phase_events;
     cj_exec_stats stats{};
 
-    const cj_table *resident(uint64_t t) const {
-        return plan.resident_inputs ? plan.resident_inputs[t] : nullptr;
-    }
-    uint64_t table_rows(uint64_t t) const {
-        const cj_table *r = resident(t);
-        return r ? r->num_rows : plan.inputs[t].num_rows;
-    }
-    uint64_t table_cols(uint64_t t) const {
-        const cj_table *r = resident(t);
-        return r ? r->cols.size() : plan.inputs[t].num_columns;
-    }
-    int32_t column_type(uint64_t t, uint64_t c) const {
-        const cj_table *r = resident(t);
-        return r ? r->cols[c].type : plan.inputs[t].columns[c].type;
-    }
+    const cj_table *resident(uint64_t t) const { return resident_input(plan, t); }
+    uint64_t table_rows(uint64_t t) const { return input_rows(plan, t); }
+    int32_t column_type(uint64_t t, uint64_t c) const { return input_col_type(plan, t, c); }
 
     void validate();
     Decoded &decode(uint64_t t, uint64_t c);
-    Relation scan_relation(const cj_plan_node &n);
     Relation resolve(uint64_t node, int depth);
     Relation exec_join(uint64_t node, int depth, bool is_root, cj_result **out);
     ColView view(const Relation &R, const RelCol &c, const uint32_t *rid_a);
@@ -152,45 +112,7 @@ class Executor {
     void ck(cudaError_t e, const char *what) { check_cuda(e, what); }
 };
 
-void Executor::validate() {
-    if (plan.num_nodes == 0 || !plan.nodes) fail(CJ_ERR_INVALID_PLAN, "plan has no nodes");
-    if (plan.root >= plan.num_nodes) fail(CJ_ERR_INVALID_PLAN, "root index out of range");
-    if (plan.num_inputs && !plan.inputs && !plan.resident_inputs)
-        fail(CJ_ERR_INVALID_PLAN, "plan has inputs but no input tables");
-    for (uint64_t t = 0; t < plan.num_inputs; ++t) {
-        const cj_table *r = resident(t);
-        if (!r && !plan.inputs) fail(CJ_ERR_INVALID_PLAN, "input " + std::to_string(t) + " missing");
-        if (r && r->ctx != &ctx) fail(CJ_ERR_INVALID_ARGUMENT, "resident table from another context");
-        if (!r) {
-            const cj_table_desc &td = plan.inputs[t];
-            if (td.num_columns && !td.columns) fail(CJ_ERR_INVALID_PLAN, "table without column array");
-            for (uint64_t c = 0; c < td.num_columns; ++c)
-                if (td.columns[c].type < CJ_INT32 || td.columns[c].type > CJ_VARCHAR)
-                    fail(CJ_ERR_INVALID_PLAN, "unknown column type");
-        }
-    }
-    for (uint64_t i = 0; i < plan.num_nodes; ++i) {
-        const cj_plan_node &n = plan.nodes[i];
-        if (n.num_output_attrs && !n.output_attrs) fail(CJ_ERR_INVALID_PLAN, "node without attr array");
-        for (uint64_t a = 0; a < n.num_output_attrs; ++a)
-            if (n.output_attrs[a].type < CJ_INT32 || n.output_attrs[a].type > CJ_VARCHAR)
-                fail(CJ_ERR_INVALID_PLAN, "unknown attribute type");
-        if (n.node_type == CJ_NODE_SCAN) {
-            if (n.base_table_id >= plan.num_inputs) fail(CJ_ERR_INVALID_PLAN, "scan of missing table");
-            for (uint64_t a = 0; a < n.num_output_attrs; ++a) {
-                const cj_attr &at = n.output_attrs[a];
-                if (at.index >= table_cols(n.base_table_id)) fail(CJ_ERR_INVALID_PLAN, "scan column out of range");
-                if (column_type(n.base_table_id, at.index) != at.type)
-                    fail(CJ_ERR_INVALID_PLAN, "scan attribute type differs from column type");
-            }
-        } else if (n.node_type == CJ_NODE_HASH_JOIN) {
-            if (n.left >= plan.num_nodes || n.right >= plan.num_nodes)
-                fail(CJ_ERR_INVALID_PLAN, "join child out of range");
-        } else {
-            fail(CJ_ERR_INVALID_PLAN, "unknown node type");
-        }
-    }
-}
+void Executor::validate() { validate_plan(ctx, plan); }
 
 Decoded &Executor::decode(uint64_t t, uint64_t c) {
     auto key = std::make_pair(t, c);
@@ -241,31 +163,13 @@ Decoded &Executor::decode(uint64_t t, uint64_t c) {
 }
 
 ColView Executor::view(const Relation &R, const RelCol &c, const uint32_t *rid_a) {
-    Decoded &d = decode(c.input, c.col);
-    ColView v{};
-    v.type = c.type;
-    v.values = d.values ? d.values->ptr : nullptr;
-    v.valid = d.valid->as<uint32_t>();
-    v.str_desc = d.desc ? d.desc->as<uint64_t>() : nullptr;
-    v.pages = d.src.dev;
-    v.rid_a = rid_a;
-    v.rid_b = c.vec >= 0 ? R.vecs[c.vec]->as<uint32_t>() : nullptr;
-    v.null_sentinel = (c.sentinel && c.type == CJ_INT32) ? 1 : 0;
-    return v;
-}
-
-Relation Executor::scan_relation(const cj_plan_node &n) {
-    Relation r;
-    r.rows = table_rows(n.base_table_id);
-    for (uint64_t a = 0; a < n.num_output_attrs; ++a)
-        r.cols.push_back({n.output_attrs[a].type, n.base_table_id, n.output_attrs[a].index, -1, false});
-    return r;
+    return make_view(decode(c.input, c.col), R, c, rid_a);
 }
 
 Relation Executor::resolve(uint64_t node, int depth) {
     if (depth > (int)plan.num_nodes) fail(CJ_ERR_INVALID_PLAN, "plan has a cycle");
     const cj_plan_node &n = plan.nodes[node];
-    if (n.node_type == CJ_NODE_SCAN) return scan_relation(n);
+    if (n.node_type == CJ_NODE_SCAN) return scan_relation(plan, n);
     return exec_join(node, depth, false, nullptr);
 }
 
@@ -515,7 +419,7 @@ cj_result *Executor::run(cj_exec_stats *st) {
     if (root.node_type == CJ_NODE_SCAN) {
         /* A scan root (the reference requires a join root) returns the
          * projected table. */
-        Relation s = scan_relation(root);
+        Relation s = scan_relation(plan, root);
         if (s.rows > 0xFFFFFFFFull) fail(CJ_ERR_LIMIT, "table exceeds 2^32-1 rows");
         std::vector<ColView> cols;
         std::vector<int32_t> types;

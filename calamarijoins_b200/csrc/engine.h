@@ -31,6 +31,10 @@ struct Error {
     std::string msg;
 };
 [[noreturn]] void fail(int code, const std::string &msg);
+/* Records the calling thread's last error (cj_last_error) and returns code. */
+int set_last_error(int code, const std::string &msg);
+void clear_last_error();
+const char *last_error();
 void check_cuda(cudaError_t e, const char *what);
 
 struct Options {
@@ -74,6 +78,7 @@ struct Context {
     int num_sms = 148;
     cudaStream_t stream = nullptr;
     cudaMemPool_t pool = nullptr;
+    bool owns_pool = true;            /* false: pool shared with a server   */
     uint16_t *d_bloom = nullptr;      /* 2048 Bloom tags                  */
     StatusBlock *d_status = nullptr;  /* device status word + counters     */
     StatusBlock *h_status = nullptr;  /* pinned mirror                     */
@@ -126,9 +131,15 @@ struct ColumnPages {
 
 void upload_pages(Context &ctx, const cj_column_desc &cd, ColumnPages &out, uint64_t *h2d_bytes);
 
+/* Creates a context on `device`; with `shared_pool` non-null the context
+ * allocates from that pool instead of creating its own. Throws Error. */
+Context *create_context(int device, cudaMemPool_t shared_pool);
+/* Creates a device memory pool that keeps freed memory for reuse. */
+cudaMemPool_t create_pool(int device);
+
 } // namespace cj
 
-struct cj_context : cj::Context {};
+
 
 struct cj_table {
     cj::Context *ctx = nullptr;
@@ -146,6 +157,10 @@ struct cj_result {
     std::vector<uint8_t *> host_cols;
 };
 
+struct cj_context : cj::Context {};
+
 namespace cj {
 cj_result *execute_plan(Context &ctx, const cj_plan_desc &plan, uint32_t flags, cj_exec_stats *stats);
+void execute_batch(Context &ctx, const cj_plan_desc *plans, size_t n, uint32_t flags, cj_result **results,
+                   int32_t *statuses, cj_batch_stats *stats);
 }

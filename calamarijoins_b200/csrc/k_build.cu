@@ -24,6 +24,8 @@
  *                     order (build_partition, hashtable.h:197-246).
  * NULL keys are skipped (hashtable.h:439-478).
  */
+#include <algorithm>
+
 #include "cj_device.cuh"
 
 namespace cj {
@@ -44,34 +46,37 @@ CJ_DEV uint32_t part_of(uint64_t h, int log2_parts) {
     return log2_parts ? (uint32_t)(h >> (64 - log2_parts)) : 0u;
 }
 
-__global__ void __launch_bounds__(kBuildThreads)
-    k_part_hist(ColView key, PartGeom g, uint32_t *__restrict__ matrix) {
-    extern __shared__ uint32_t s_hist[];
+/* ---- per-unit bodies (shared by the single-join and grouped kernels) ---- */
+
+/* Histogram of one chunk of build rows over the partitions; column-major
+ * into `matrix` (P x g.grid). */
+CJ_DEV void hist_chunk(const ColView &key, const PartGeom &g, uint32_t chunk, uint32_t *__restrict__ matrix,
+                       uint32_t *s_hist) {
     const uint32_t P = 1u << g.log2_parts;
     for (uint32_t b = threadIdx.x; b < P; b += blockDim.x) s_hist[b] = 0;
     __syncthreads();
-    const uint64_t r0 = (uint64_t)blockIdx.x * g.chunk;
+    const uint64_t r0 = (uint64_t)chunk * g.chunk;
     const uint64_t r1 = min((uint64_t)g.n, r0 + g.chunk);
     for (uint64_t i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
         int64_t k;
         if (load_key(key, (uint32_t)i, &k)) atomicAdd(&s_hist[part_of(hash_key(k), g.log2_parts)], 1u);
     }
     __syncthreads();
-    for (uint32_t b = threadIdx.x; b < P; b += blockDim.x)
-        matrix[(uint64_t)b * g.grid + blockIdx.x] = s_hist[b];
+    for (uint32_t b = threadIdx.x; b < P; b += blockDim.x) matrix[(uint64_t)b * g.grid + chunk] = s_hist[b];
+    __syncthreads();
 }
 
+/* Scatter of one chunk into the partitioned buffer. `offsets` is the
+ * exclusive scan of the matrix, `off_base` subtracted from every entry. */
 template <typename K>
-__global__ void __launch_bounds__(kBuildThreads)
-    k_part_scatter(ColView key, PartGeom g, const uint64_t *__restrict__ offsets,
-                   Tuple<K> *__restrict__ out) {
-    extern __shared__ uint32_t smem[];
+CJ_DEV void scatter_chunk(const ColView &key, const PartGeom &g, uint32_t chunk, const uint64_t *__restrict__ offsets,
+                          uint64_t off_base, Tuple<K> *__restrict__ out, uint32_t *smem) {
     const uint32_t P = 1u << g.log2_parts;
-    uint32_t *s_cursor = smem;      /* next output slot per partition  */
-    uint32_t *s_tile = smem + P;    /* rows per partition in this tile */
+    uint32_t *s_cursor = smem;   /* next output slot per partition  */
+    uint32_t *s_tile = smem + P; /* rows per partition in this tile */
     for (uint32_t b = threadIdx.x; b < P; b += blockDim.x)
-        s_cursor[b] = (uint32_t)offsets[(uint64_t)b * g.grid + blockIdx.x];
-    const uint64_t r0 = (uint64_t)blockIdx.x * g.chunk;
+        s_cursor[b] = (uint32_t)(offsets[(uint64_t)b * g.grid + chunk] - off_base);
+    const uint64_t r0 = (uint64_t)chunk * g.chunk;
     const uint64_t r1 = min((uint64_t)g.n, r0 + g.chunk);
     const uint32_t tile = blockDim.x * kHistItems;
     for (uint64_t t0 = r0; t0 < r1; t0 += tile) {
@@ -110,60 +115,157 @@ __global__ void __launch_bounds__(kBuildThreads)
     }
 }
 
+/* Counting sort of one partition into slot order + its directory entries
+ * (build_partition, hashtable.h:197-246). */
+template <typename K>
+CJ_DEV void build_partition(const Tuple<K> *__restrict__ in, const uint64_t *__restrict__ offsets, uint64_t off_base,
+                            uint32_t grid_hist, int log2_parts, int log2_slots, uint32_t p, const uint16_t *s_bloom,
+                            uint64_t *__restrict__ dir, Tuple<K> *__restrict__ out, uint32_t *s_cnt, uint32_t *s_tag,
+                            uint32_t *wbuf) {
+    const uint32_t S = 1u << (log2_slots - log2_parts);
+    for (uint32_t s = threadIdx.x; s < S; s += blockDim.x) {
+        s_cnt[s] = 0;
+        s_tag[s] = 0;
+    }
+    __syncthreads();
+    const uint64_t ps = offsets[(uint64_t)p * grid_hist] - off_base;
+    const uint64_t pe = offsets[(uint64_t)(p + 1) * grid_hist] - off_base;
+    for (uint64_t t = ps + threadIdx.x; t < pe; t += blockDim.x) {
+        uint64_t h = hash_key((int64_t)in[t].key);
+        uint32_t ls = slot_of(h, log2_slots) & (S - 1);
+        atomicAdd(&s_cnt[ls], 1u);
+        atomicOr(&s_tag[ls], (uint32_t)s_bloom[bloom_index(h)]);
+    }
+    __syncthreads();
+    /* exclusive scan of the S counts: each thread owns S/blockDim slots */
+    const uint32_t per = (S + blockDim.x - 1) / blockDim.x;
+    const uint32_t s0 = threadIdx.x * per;
+    uint32_t sum = 0;
+    for (uint32_t k = 0; k < per; ++k)
+        if (s0 + k < S) sum += s_cnt[s0 + k];
+    uint32_t tot;
+    uint32_t pre = block_exclusive_scan<uint32_t>(sum, wbuf, &tot);
+    for (uint32_t k = 0; k < per; ++k) {
+        uint32_t s = s0 + k;
+        if (s >= S) break;
+        uint32_t c = s_cnt[s];
+        uint64_t end = ps + pre + c;
+        dir[(uint64_t)p * S + s] = (end << 16) | (uint64_t)(s_tag[s] & 0xFFFFu);
+        s_cnt[s] = pre; /* becomes the scatter cursor */
+        pre += c;
+    }
+    __syncthreads();
+    for (uint64_t t = ps + threadIdx.x; t < pe; t += blockDim.x) {
+        Tuple<K> tp = in[t];
+        uint32_t ls = slot_of(hash_key((int64_t)tp.key), log2_slots) & (S - 1);
+        uint32_t pos = atomicAdd(&s_cnt[ls], 1u);
+        out[ps + pos] = tp;
+    }
+    __syncthreads();
+}
+
+/* ---- single-join kernels ---- */
+__global__ void __launch_bounds__(kBuildThreads)
+    k_part_hist(ColView key, PartGeom g, uint32_t *__restrict__ matrix) {
+    extern __shared__ uint32_t s_hist[];
+    hist_chunk(key, g, blockIdx.x, matrix, s_hist);
+}
+
 template <typename K>
 __global__ void __launch_bounds__(kBuildThreads)
-    k_part_build(const Tuple<K> *__restrict__ in, const uint64_t *__restrict__ offsets,
-                 uint32_t grid_hist, int log2_parts, int log2_slots,
-                 const uint16_t *__restrict__ g_bloom, uint64_t *__restrict__ dir,
+    k_part_scatter(ColView key, PartGeom g, const uint64_t *__restrict__ offsets, Tuple<K> *__restrict__ out) {
+    extern __shared__ uint32_t smem[];
+    scatter_chunk<K>(key, g, blockIdx.x, offsets, 0, out, smem);
+}
+
+template <typename K>
+__global__ void __launch_bounds__(kBuildThreads)
+    k_part_build(const Tuple<K> *__restrict__ in, const uint64_t *__restrict__ offsets, uint32_t grid_hist,
+                 int log2_parts, int log2_slots, const uint16_t *__restrict__ g_bloom, uint64_t *__restrict__ dir,
                  Tuple<K> *__restrict__ out) {
     extern __shared__ uint32_t smem[];
     __shared__ uint16_t s_bloom[2048];
     __shared__ uint32_t wbuf[kBuildThreads / 32 + 1];
     const uint32_t P = 1u << log2_parts;
     const uint32_t S = 1u << (log2_slots - log2_parts);
-    uint32_t *s_cnt = smem;
-    uint32_t *s_tag = smem + S;
     load_bloom(s_bloom, g_bloom);
-    for (uint32_t p = blockIdx.x; p < P; p += gridDim.x) {
-        for (uint32_t s = threadIdx.x; s < S; s += blockDim.x) {
-            s_cnt[s] = 0;
-            s_tag[s] = 0;
-        }
+    for (uint32_t p = blockIdx.x; p < P; p += gridDim.x)
+        build_partition<K>(in, offsets, 0, grid_hist, log2_parts, log2_slots, p, s_bloom, dir, out, smem, smem + S,
+                           wbuf);
+}
+
+/* ---- grouped kernels: every hash join of a batch level ---- */
+CJ_DEV uint32_t find_task(const BuildTask *tasks, uint32_t ntasks, uint32_t unit, bool by_partition) {
+    uint32_t lo = 0, hi = ntasks;
+    while (hi - lo > 1) {
+        uint32_t mid = (lo + hi) >> 1;
+        uint32_t b = by_partition ? tasks[mid].part_base : tasks[mid].chunk_base;
+        if (b <= unit) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+CJ_DEV PartGeom task_geom(const BuildTask &T) {
+    PartGeom g;
+    g.n = T.n;
+    g.log2_parts = T.log2_parts;
+    g.log2_slots = T.log2_slots;
+    g.grid = T.grid;
+    g.chunk = T.chunk;
+    return g;
+}
+
+__global__ void __launch_bounds__(kBuildThreads)
+    k_part_hist_grouped(const BuildTask *__restrict__ tasks, uint32_t ntasks, uint32_t *__restrict__ matrix) {
+    extern __shared__ uint32_t s_hist[];
+    __shared__ uint32_t s_task;
+    if (threadIdx.x == 0) s_task = find_task(tasks, ntasks, blockIdx.x, false);
+    __syncthreads();
+    const BuildTask &T = tasks[s_task];
+    hist_chunk(T.key, task_geom(T), blockIdx.x - T.chunk_base, matrix + T.cell_base, s_hist);
+}
+
+__global__ void __launch_bounds__(kBuildThreads)
+    k_part_scatter_grouped(const BuildTask *__restrict__ tasks, uint32_t ntasks,
+                           const uint64_t *__restrict__ offsets) {
+    extern __shared__ uint32_t smem[];
+    __shared__ uint32_t s_task;
+    if (threadIdx.x == 0) s_task = find_task(tasks, ntasks, blockIdx.x, false);
+    __syncthreads();
+    const BuildTask &T = tasks[s_task];
+    const uint64_t *off = offsets + T.cell_base;
+    if (T.key.type == CJ_INT32)
+        scatter_chunk<int32_t>(T.key, task_geom(T), blockIdx.x - T.chunk_base, off, off[0],
+                               reinterpret_cast<Tuple<int32_t> *>(T.part_buf), smem);
+    else
+        scatter_chunk<int64_t>(T.key, task_geom(T), blockIdx.x - T.chunk_base, off, off[0],
+                               reinterpret_cast<Tuple<int64_t> *>(T.part_buf), smem);
+}
+
+__global__ void __launch_bounds__(kBuildThreads)
+    k_part_build_grouped(const BuildTask *__restrict__ tasks, uint32_t ntasks, uint32_t total_parts,
+                         const uint64_t *__restrict__ offsets, const uint16_t *__restrict__ g_bloom) {
+    extern __shared__ uint32_t smem[];
+    __shared__ uint16_t s_bloom[2048];
+    __shared__ uint32_t wbuf[kBuildThreads / 32 + 1];
+    __shared__ uint32_t s_task;
+    load_bloom(s_bloom, g_bloom);
+    for (uint32_t u = blockIdx.x; u < total_parts; u += gridDim.x) {
         __syncthreads();
-        const uint64_t ps = offsets[(uint64_t)p * grid_hist];
-        const uint64_t pe = offsets[(uint64_t)(p + 1) * grid_hist];
-        for (uint64_t t = ps + threadIdx.x; t < pe; t += blockDim.x) {
-            uint64_t h = hash_key((int64_t)in[t].key);
-            uint32_t ls = slot_of(h, log2_slots) & (S - 1);
-            atomicAdd(&s_cnt[ls], 1u);
-            atomicOr(&s_tag[ls], (uint32_t)s_bloom[bloom_index(h)]);
-        }
+        if (threadIdx.x == 0) s_task = find_task(tasks, ntasks, u, true);
         __syncthreads();
-        /* exclusive scan of the S counts: each thread owns S/blockDim slots */
-        const uint32_t per = (S + blockDim.x - 1) / blockDim.x;
-        const uint32_t s0 = threadIdx.x * per;
-        uint32_t sum = 0;
-        for (uint32_t k = 0; k < per; ++k)
-            if (s0 + k < S) sum += s_cnt[s0 + k];
-        uint32_t tot;
-        uint32_t pre = block_exclusive_scan<uint32_t>(sum, wbuf, &tot);
-        for (uint32_t k = 0; k < per; ++k) {
-            uint32_t s = s0 + k;
-            if (s >= S) break;
-            uint32_t c = s_cnt[s];
-            uint64_t end = ps + pre + c;
-            dir[(uint64_t)p * S + s] = (end << 16) | (uint64_t)(s_tag[s] & 0xFFFFu);
-            s_cnt[s] = pre; /* becomes the scatter cursor */
-            pre += c;
-        }
-        __syncthreads();
-        for (uint64_t t = ps + threadIdx.x; t < pe; t += blockDim.x) {
-            Tuple<K> tp = in[t];
-            uint32_t ls = slot_of(hash_key((int64_t)tp.key), log2_slots) & (S - 1);
-            uint32_t pos = atomicAdd(&s_cnt[ls], 1u);
-            out[ps + pos] = tp;
-        }
-        __syncthreads();
+        const BuildTask &T = tasks[s_task];
+        const uint32_t S = 1u << (T.log2_slots - T.log2_parts);
+        const uint64_t *off = offsets + T.cell_base;
+        if (T.key.type == CJ_INT32)
+            build_partition<int32_t>(reinterpret_cast<const Tuple<int32_t> *>(T.part_buf), off, off[0], T.grid,
+                                     T.log2_parts, T.log2_slots, u - T.part_base, s_bloom, T.dir,
+                                     reinterpret_cast<Tuple<int32_t> *>(T.tuples), smem, smem + S, wbuf);
+        else
+            build_partition<int64_t>(reinterpret_cast<const Tuple<int64_t> *>(T.part_buf), off, off[0], T.grid,
+                                     T.log2_parts, T.log2_slots, u - T.part_base, s_bloom, T.dir,
+                                     reinterpret_cast<Tuple<int64_t> *>(T.tuples), smem, smem + S, wbuf);
     }
 }
 
@@ -227,6 +329,9 @@ void set_smem_attrs() {
     cudaFuncSetAttribute(k_part_scatter<int64_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
     cudaFuncSetAttribute(k_part_build<int32_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
     cudaFuncSetAttribute(k_part_build<int64_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
+    cudaFuncSetAttribute(k_part_hist_grouped, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
+    cudaFuncSetAttribute(k_part_scatter_grouped, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
+    cudaFuncSetAttribute(k_part_build_grouped, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
     g_attrs_set = true;
 }
 
@@ -238,6 +343,48 @@ size_t build_temp_bytes(const Launch &L, const BuildPlan &bp, int key_bytes) {
     size_t tuple = key_bytes == 4 ? sizeof(Tuple<int32_t>) : sizeof(Tuple<int64_t>);
     return align256(cells * 4) + align256((cells + 1) * 8) + align256((size_t)bp.num_rows * tuple) +
            scan_temp_bytes(cells) + 256;
+}
+
+BuildGeometry build_geometry(const Launch &L, const BuildPlan &bp) {
+    PartGeom g = geometry(L, bp);
+    BuildGeometry out;
+    out.grid = g.grid;
+    out.chunk = g.chunk;
+    out.cells = (1ull << bp.log2_parts) * g.grid;
+    return out;
+}
+
+cudaError_t launch_build_grouped(const Launch &L, const BuildTask *tasks_dev, uint32_t ntasks, uint32_t total_chunks,
+                                 uint32_t total_parts, uint64_t total_cells, uint32_t max_parts, uint32_t max_slots,
+                                 const uint16_t *bloom, void *temp) {
+    set_smem_attrs();
+    if (!ntasks) return cudaSuccess;
+    char *t = reinterpret_cast<char *>(temp);
+    uint32_t *matrix = reinterpret_cast<uint32_t *>(t);
+    t += align256(total_cells * sizeof(uint32_t));
+    uint64_t *offsets = reinterpret_cast<uint64_t *>(t);
+    t += align256((total_cells + 1) * sizeof(uint64_t));
+    k_part_hist_grouped<<<total_chunks, kBuildThreads, max_parts * sizeof(uint32_t), L.stream>>>(tasks_dev, ntasks,
+                                                                                                  matrix);
+    count_launches(1);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    e = scan_u32_to_u64(L, matrix, offsets, total_cells, t);
+    if (e != cudaSuccess) return e;
+    k_part_scatter_grouped<<<total_chunks, kBuildThreads, 2 * max_parts * sizeof(uint32_t), L.stream>>>(
+        tasks_dev, ntasks, offsets);
+    count_launches(1);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    unsigned grid_b = (unsigned)std::min<uint64_t>(total_parts, (uint64_t)L.num_sms * 16);
+    k_part_build_grouped<<<grid_b, kBuildThreads, 2 * max_slots * sizeof(uint32_t), L.stream>>>(
+        tasks_dev, ntasks, total_parts, offsets, bloom);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+size_t build_grouped_temp_bytes(uint64_t total_cells) {
+    return align256(total_cells * 4) + align256((total_cells + 1) * 8) + scan_temp_bytes(total_cells) + 256;
 }
 
 size_t build_tuple_bytes(int key_bytes) {

@@ -19,6 +19,8 @@
  * the (at most two) 32-row words a page shares with its neighbours, which
  * use atomicOr on a zeroed bitmap.
  */
+#include <algorithm>
+
 #include "cj_device.cuh"
 
 namespace cj {
@@ -29,29 +31,33 @@ constexpr uint32_t kMaxBitmapWords = 2048; /* 65535 rows */
 
 CJ_DEV uint16_t rd16(const uint8_t *p) { return *reinterpret_cast<const uint16_t *>(p); }
 
+/* Rows a page contributes (n_rows; 1 for a long-string start page, 0 for a
+ * continuation) and header checks. */
+CJ_DEV uint32_t page_rows_of(const uint8_t *pg, int32_t type, unsigned int *err) {
+    uint32_t nr = rd16(pg), nv = rd16(pg + 2);
+    uint32_t r = nr;
+    if (type == CJ_VARCHAR) {
+        if (nr == 0xffff) {
+            r = 1;
+            if (nv == 0 || nv > kLongChunk) atomicOr(err, DEV_ERR_PAGE_HEADER);
+        } else if (nr == 0xfffe) {
+            r = 0;
+            if (nv == 0 || nv > kLongChunk) atomicOr(err, DEV_ERR_PAGE_HEADER);
+        } else if (nv > nr || 4u + 2u * nv + (nr + 7) / 8 > kPageSize) {
+            atomicOr(err, DEV_ERR_PAGE_HEADER);
+        }
+    } else {
+        uint32_t w = type == CJ_INT32 ? 4u : 8u;
+        if (nv > nr || w + w * nv + (nr + 7) / 8 > kPageSize) atomicOr(err, DEV_ERR_PAGE_HEADER);
+    }
+    return r;
+}
+
 __global__ void k_page_rows(const uint8_t *__restrict__ pages, uint64_t np, int32_t type,
                             uint32_t *__restrict__ rows, unsigned int *err) {
     for (uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; p < np;
-         p += (uint64_t)gridDim.x * blockDim.x) {
-        const uint8_t *pg = pages + p * kPageSize;
-        uint32_t nr = rd16(pg), nv = rd16(pg + 2);
-        uint32_t r = nr;
-        if (type == CJ_VARCHAR) {
-            if (nr == 0xffff) {
-                r = 1;
-                if (nv == 0 || nv > kLongChunk) atomicOr(err, DEV_ERR_PAGE_HEADER);
-            } else if (nr == 0xfffe) {
-                r = 0;
-                if (nv == 0 || nv > kLongChunk) atomicOr(err, DEV_ERR_PAGE_HEADER);
-            } else if (nv > nr || 4u + 2u * nv + (nr + 7) / 8 > kPageSize) {
-                atomicOr(err, DEV_ERR_PAGE_HEADER);
-            }
-        } else {
-            uint32_t w = type == CJ_INT32 ? 4u : 8u;
-            if (nv > nr || w + w * nv + (nr + 7) / 8 > kPageSize) atomicOr(err, DEV_ERR_PAGE_HEADER);
-        }
-        rows[p] = r;
-    }
+         p += (uint64_t)gridDim.x * blockDim.x)
+        rows[p] = page_rows_of(pages + p * kPageSize, type, err);
 }
 
 /* Loads a sparse page's bitmap into s_bm (bits past n_rows cleared) and the
@@ -129,102 +135,164 @@ CJ_DEV void write_validity(bool dense, const uint32_t *s_bm, uint32_t nr, uint64
     }
 }
 
+struct DecodeSmem {
+    uint32_t bm[kMaxBitmapWords];
+    uint32_t pre[kMaxBitmapWords];
+    uint32_t wbuf[kDecodeThreads / 32 + 1];
+};
+
+/* Decodes fixed-width page p (of a column whose pages start at `pages`)
+ * whose first row is rs. Block-wide. */
+template <typename T>
+CJ_DEV void decode_fixed_page(const uint8_t *__restrict__ pages, uint64_t p, uint64_t rs, uint64_t max_rows,
+                              T *__restrict__ values, uint32_t *__restrict__ valid, unsigned int *err,
+                              DecodeSmem &sm) {
+    constexpr uint32_t DB = sizeof(T) == 4 ? 4u : 8u;
+    const uint8_t *pg = pages + p * kPageSize;
+    const uint32_t nr = rd16(pg), nv = rd16(pg + 2);
+    if (nv > nr || DB + (uint32_t)sizeof(T) * nv + (nr + 7) / 8 > kPageSize) return;
+    if (rs + nr > max_rows) {
+        if (threadIdx.x == 0) atomicOr(err, DEV_ERR_ROW_COUNT);
+        return;
+    }
+    const T *vals = reinterpret_cast<const T *>(pg + DB);
+    const bool dense = nr == nv;
+    if (!dense) load_page_bitmap(pg, nr, sm.bm, sm.pre, sm.wbuf);
+    for (uint32_t i = threadIdx.x; i < nr; i += blockDim.x) {
+        T v = T(0);
+        if (dense) {
+            v = __ldcs(vals + i);
+        } else {
+            int idx = value_index(sm.bm, sm.pre, i);
+            if (idx >= (int)nv) atomicOr(err, DEV_ERR_PAGE_HEADER); /* bitmap holds > n_values bits */
+            else if (idx >= 0) v = __ldcs(vals + idx);
+        }
+        values[rs + i] = v;
+    }
+    write_validity(dense, sm.bm, nr, rs, valid);
+    __syncthreads();
+}
+
+CJ_DEV void decode_varchar_page(const uint8_t *__restrict__ pages, uint64_t p, uint64_t np, uint64_t rs,
+                                uint64_t max_rows, uint64_t *__restrict__ desc, uint32_t *__restrict__ valid,
+                                unsigned int *err, DecodeSmem &sm) {
+    const uint8_t *pg = pages + p * kPageSize;
+    const uint32_t nr = rd16(pg), nv = rd16(pg + 2);
+    if (nr == 0xfffe) {
+        if (threadIdx.x == 0) {
+            uint32_t prev = p ? rd16(pg - kPageSize) : 0u;
+            if (prev != 0xffff && prev != 0xfffe) atomicOr(err, DEV_ERR_LONG_CHAIN);
+        }
+        return;
+    }
+    if (nr == 0xffff) {
+        if (threadIdx.x == 0 && rs >= max_rows) atomicOr(err, DEV_ERR_ROW_COUNT);
+        if (threadIdx.x == 0 && rs < max_rows) {
+            uint64_t q = p + 1;
+            while (q < np && rd16(pages + q * kPageSize) == 0xfffe) ++q;
+            uint64_t chain = q - p;
+            if (chain > 0xFFFFFFull) {
+                atomicOr(err, DEV_ERR_LONG_CHAIN);
+                chain = 0xFFFFFF;
+            }
+            desc[rs] = desc_long(p, (uint32_t)chain);
+            atomicOr(valid + (rs >> 5), 1u << (rs & 31));
+        }
+        return;
+    }
+    if (nv > nr || 4u + 2u * nv + (nr + 7) / 8 > kPageSize) return;
+    if (rs + nr > max_rows) {
+        if (threadIdx.x == 0) atomicOr(err, DEV_ERR_ROW_COUNT);
+        return;
+    }
+    const bool dense = nr == nv;
+    if (!dense) load_page_bitmap(pg, nr, sm.bm, sm.pre, sm.wbuf);
+    const uint16_t *offs = reinterpret_cast<const uint16_t *>(pg + 4);
+    const uint32_t chars_at = 4u + 2u * nv;
+    const uint32_t chars_cap = kPageSize - (nr + 7) / 8 - chars_at;
+    for (uint32_t i = threadIdx.x; i < nr; i += blockDim.x) {
+        int k = dense ? (int)i : value_index(sm.bm, sm.pre, i);
+        uint64_t d = 0;
+        if (k >= (int)nv) {
+            atomicOr(err, DEV_ERR_PAGE_HEADER); /* bitmap holds > n_values bits */
+        } else if (k >= 0) {
+            uint32_t start = k ? offs[k - 1] : 0u, end = offs[k];
+            if (end < start || end > chars_cap) {
+                atomicOr(err, DEV_ERR_VARCHAR_OFFSETS);
+            } else {
+                d = desc_short(p * kPageSize + chars_at + start, end - start);
+            }
+        }
+        desc[rs + i] = d;
+    }
+    write_validity(dense, sm.bm, nr, rs, valid);
+    __syncthreads();
+}
+
 template <typename T>
 __global__ void __launch_bounds__(kDecodeThreads)
-    k_decode_fixed(const uint8_t *__restrict__ pages, uint64_t np,
-                   const uint64_t *__restrict__ row_start, uint64_t max_rows, T *__restrict__ values,
-                   uint32_t *__restrict__ valid, unsigned int *err) {
-    __shared__ uint32_t s_bm[kMaxBitmapWords];
-    __shared__ uint32_t s_pre[kMaxBitmapWords];
-    __shared__ uint32_t wbuf[kDecodeThreads / 32 + 1];
-    constexpr uint32_t DB = sizeof(T) == 4 ? 4u : 8u;
-    for (uint64_t p = blockIdx.x; p < np; p += gridDim.x) {
-        const uint8_t *pg = pages + p * kPageSize;
-        const uint32_t nr = rd16(pg), nv = rd16(pg + 2);
-        if (nv > nr || DB + (uint32_t)sizeof(T) * nv + (nr + 7) / 8 > kPageSize) continue;
-        const uint64_t rs = row_start[p];
-        if (rs + nr > max_rows) {
-            if (threadIdx.x == 0) atomicOr(err, DEV_ERR_ROW_COUNT);
-            continue;
-        }
-        const T *vals = reinterpret_cast<const T *>(pg + DB);
-        const bool dense = nr == nv;
-        if (!dense) load_page_bitmap(pg, nr, s_bm, s_pre, wbuf);
-        for (uint32_t i = threadIdx.x; i < nr; i += blockDim.x) {
-            T v = T(0);
-            if (dense) {
-                v = __ldcs(vals + i);
-            } else {
-                int idx = value_index(s_bm, s_pre, i);
-                if (idx >= (int)nv) atomicOr(err, DEV_ERR_PAGE_HEADER); /* bitmap holds > n_values bits */
-                else if (idx >= 0) v = __ldcs(vals + idx);
-            }
-            values[rs + i] = v;
-        }
-        write_validity(dense, s_bm, nr, rs, valid);
-        __syncthreads();
+    k_decode_fixed(const uint8_t *__restrict__ pages, uint64_t np, const uint64_t *__restrict__ row_start,
+                   uint64_t max_rows, T *__restrict__ values, uint32_t *__restrict__ valid, unsigned int *err) {
+    __shared__ DecodeSmem sm;
+    for (uint64_t p = blockIdx.x; p < np; p += gridDim.x)
+        decode_fixed_page<T>(pages, p, row_start[p], max_rows, values, valid, err, sm);
+}
+
+__global__ void __launch_bounds__(kDecodeThreads)
+    k_decode_varchar(const uint8_t *__restrict__ pages, uint64_t np, const uint64_t *__restrict__ row_start,
+                     uint64_t max_rows, uint64_t *__restrict__ desc, uint32_t *__restrict__ valid, unsigned int *err) {
+    __shared__ DecodeSmem sm;
+    for (uint64_t p = blockIdx.x; p < np; p += gridDim.x)
+        decode_varchar_page(pages, p, np, row_start[p], max_rows, desc, valid, err, sm);
+}
+
+/* ---- grouped: every column a batch needs, one launch per pass ---- */
+CJ_DEV uint32_t find_column(const DecodeTask *tasks, uint32_t ntasks, uint64_t gpage) {
+    uint32_t lo = 0, hi = ntasks;
+    while (hi - lo > 1) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (tasks[mid].page_base <= gpage) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+__global__ void k_page_rows_grouped(const DecodeTask *__restrict__ tasks, uint32_t ntasks, uint64_t total_pages,
+                                    uint32_t *__restrict__ rows, unsigned int *err) {
+    for (uint64_t gp = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; gp < total_pages;
+         gp += (uint64_t)gridDim.x * blockDim.x) {
+        const DecodeTask &T = tasks[find_column(tasks, ntasks, gp)];
+        const uint8_t *pg = T.pages + (gp - T.page_base) * kPageSize;
+        rows[gp] = page_rows_of(pg, T.type, err);
+    }
+}
+
+__global__ void k_check_rows_grouped(const DecodeTask *__restrict__ tasks, uint32_t ntasks,
+                                     const uint64_t *__restrict__ row_start, unsigned int *err) {
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < ntasks; k += gridDim.x * blockDim.x) {
+        const DecodeTask &T = tasks[k];
+        if (row_start[T.page_base + T.num_pages] - row_start[T.page_base] != T.rows) atomicOr(err, DEV_ERR_ROW_COUNT);
     }
 }
 
 __global__ void __launch_bounds__(kDecodeThreads)
-    k_decode_varchar(const uint8_t *__restrict__ pages, uint64_t np,
-                     const uint64_t *__restrict__ row_start, uint64_t max_rows,
-                     uint64_t *__restrict__ desc, uint32_t *__restrict__ valid, unsigned int *err) {
-    __shared__ uint32_t s_bm[kMaxBitmapWords];
-    __shared__ uint32_t s_pre[kMaxBitmapWords];
-    __shared__ uint32_t wbuf[kDecodeThreads / 32 + 1];
-    for (uint64_t p = blockIdx.x; p < np; p += gridDim.x) {
-        const uint8_t *pg = pages + p * kPageSize;
-        const uint32_t nr = rd16(pg), nv = rd16(pg + 2);
-        const uint64_t rs = row_start[p];
-        if (nr == 0xfffe) {
-            if (threadIdx.x == 0) {
-                uint32_t prev = p ? rd16(pg - kPageSize) : 0u;
-                if (prev != 0xffff && prev != 0xfffe) atomicOr(err, DEV_ERR_LONG_CHAIN);
-            }
-            continue;
-        }
-        if (nr == 0xffff) {
-            if (threadIdx.x == 0 && rs >= max_rows) atomicOr(err, DEV_ERR_ROW_COUNT);
-            if (threadIdx.x == 0 && rs < max_rows) {
-                uint64_t q = p + 1;
-                while (q < np && rd16(pages + q * kPageSize) == 0xfffe) ++q;
-                uint64_t chain = q - p;
-                if (chain > 0xFFFFFFull) {
-                    atomicOr(err, DEV_ERR_LONG_CHAIN);
-                    chain = 0xFFFFFF;
-                }
-                desc[rs] = desc_long(p, (uint32_t)chain);
-                atomicOr(valid + (rs >> 5), 1u << (rs & 31));
-            }
-            continue;
-        }
-        if (nv > nr || 4u + 2u * nv + (nr + 7) / 8 > kPageSize) continue;
-        if (rs + nr > max_rows) {
-            if (threadIdx.x == 0) atomicOr(err, DEV_ERR_ROW_COUNT);
-            continue;
-        }
-        const bool dense = nr == nv;
-        if (!dense) load_page_bitmap(pg, nr, s_bm, s_pre, wbuf);
-        const uint16_t *offs = reinterpret_cast<const uint16_t *>(pg + 4);
-        const uint32_t chars_at = 4u + 2u * nv;
-        const uint32_t chars_cap = kPageSize - (nr + 7) / 8 - chars_at;
-        for (uint32_t i = threadIdx.x; i < nr; i += blockDim.x) {
-            int k = dense ? (int)i : value_index(s_bm, s_pre, i);
-            uint64_t d = 0;
-            if (k >= (int)nv) {
-                atomicOr(err, DEV_ERR_PAGE_HEADER); /* bitmap holds > n_values bits */
-            } else if (k >= 0) {
-                uint32_t start = k ? offs[k - 1] : 0u, end = offs[k];
-                if (end < start || end > chars_cap) {
-                    atomicOr(err, DEV_ERR_VARCHAR_OFFSETS);
-                } else {
-                    d = desc_short(p * kPageSize + chars_at + start, end - start);
-                }
-            }
-            desc[rs + i] = d;
-        }
-        write_validity(dense, s_bm, nr, rs, valid);
+    k_decode_grouped(const DecodeTask *__restrict__ tasks, uint32_t ntasks, uint64_t total_pages,
+                     const uint64_t *__restrict__ row_start, unsigned int *err) {
+    __shared__ DecodeSmem sm;
+    __shared__ uint32_t s_task;
+    for (uint64_t gp = blockIdx.x; gp < total_pages; gp += gridDim.x) {
+        if (threadIdx.x == 0) s_task = find_column(tasks, ntasks, gp);
+        __syncthreads();
+        const DecodeTask &T = tasks[s_task];
+        const uint64_t p = gp - T.page_base;
+        const uint64_t rs = row_start[gp] - row_start[T.page_base];
+        if (T.type == CJ_VARCHAR)
+            decode_varchar_page(T.pages, p, T.num_pages, rs, T.rows, T.desc, T.valid, err, sm);
+        else if (T.type == CJ_INT32)
+            decode_fixed_page<int32_t>(T.pages, p, rs, T.rows, reinterpret_cast<int32_t *>(T.values), T.valid, err, sm);
+        else
+            decode_fixed_page<long long>(T.pages, p, rs, T.rows, reinterpret_cast<long long *>(T.values), T.valid,
+                                         err, sm);
         __syncthreads();
     }
 }
@@ -276,6 +344,26 @@ cudaError_t launch_decode_varchar(const Launch &L, const uint8_t *pages, uint64_
     k_decode_varchar<<<g, kDecodeThreads, 0, L.stream>>>(pages, np, row_start, max_rows, desc, valid,
                                                           L.dev_errors);
     count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_decode_grouped(const Launch &L, const DecodeTask *tasks_dev, uint32_t ntasks, uint64_t total_pages,
+                                  uint32_t *rows_pp, uint64_t *row_start, void *scan_temp) {
+    if (!ntasks) return cudaSuccess;
+    if (total_pages) {
+        unsigned g = (unsigned)std::min<uint64_t>((total_pages + 255) / 256, (uint64_t)L.num_sms * 8);
+        k_page_rows_grouped<<<g, 256, 0, L.stream>>>(tasks_dev, ntasks, total_pages, rows_pp, L.dev_errors);
+        count_launches(1);
+    }
+    cudaError_t e = scan_u32_to_u64(L, rows_pp, row_start, total_pages, scan_temp);
+    if (e != cudaSuccess) return e;
+    k_check_rows_grouped<<<(ntasks + 127) / 128, 128, 0, L.stream>>>(tasks_dev, ntasks, row_start, L.dev_errors);
+    count_launches(1);
+    if (total_pages) {
+        unsigned g = grid_for(L, total_pages, 6);
+        k_decode_grouped<<<g, kDecodeThreads, 0, L.stream>>>(tasks_dev, ntasks, total_pages, row_start, L.dev_errors);
+        count_launches(1);
+    }
     return cudaGetLastError();
 }
 

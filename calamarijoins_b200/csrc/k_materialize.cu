@@ -25,12 +25,16 @@
  * copy_long_string_pages does (page_builders.h:345-362). Pass 1 counts each
  * tile's pages, a scan places them, pass 2 writes them.
  */
+#include <algorithm>
+
 #include "cj_device.cuh"
 
 namespace cj {
 namespace {
 
 constexpr int kMatThreads = 256;
+
+CJ_DEV uint32_t rows_per_page_dev(int32_t type) { return type == CJ_INT32 ? kRowsPerPageInt32 : kRowsPerPage8B; }
 
 __global__ void k_gather_u32(const uint32_t *__restrict__ src, const uint32_t *__restrict__ idx,
                              uint64_t n, uint32_t *__restrict__ out) {
@@ -52,56 +56,112 @@ CJ_DEV void scan_warp_counts(uint32_t *s_warp) {
     }
 }
 
+struct PageSmem {
+    uint4 page[kPageSize / 16];
+    uint32_t warp[kMatThreads / 32 + 1];
+};
+
+/* Builds output page `pg` (rows [pg*R, pg*R+R)) of a fixed-width column in
+ * shared memory and stores it. Block-wide. */
+template <typename T>
+CJ_DEV void write_fixed_page(const ColView &col, uint64_t rows, uint32_t R, uint64_t pg, uint8_t *__restrict__ out,
+                             PageSmem &sm) {
+    constexpr uint32_t DB = sizeof(T) == 4 ? 4u : 8u;
+    uint8_t *sp = reinterpret_cast<uint8_t *>(sm.page);
+    const uint32_t warp = threadIdx.x >> 5, lane = lane_id();
+    for (uint32_t k = threadIdx.x; k < kPageSize / 16; k += blockDim.x) sm.page[k] = make_uint4(0, 0, 0, 0);
+    __syncthreads();
+    const uint64_t r0 = pg * R;
+    const uint32_t nr = (uint32_t)min((uint64_t)R, rows - r0);
+    const uint32_t bm_bytes = (nr + 7) / 8;
+    uint8_t *bm = sp + kPageSize - bm_bytes;
+    T *vals = reinterpret_cast<T *>(sp + DB);
+    uint32_t running = 0;
+    for (uint32_t slab = 0; slab * kMatThreads < nr; ++slab) {
+        const uint32_t r = slab * kMatThreads + threadIdx.x;
+        bool v = false;
+        T val = T(0);
+        if (r < nr) {
+            uint32_t br = base_row(col, (uint32_t)(r0 + r));
+            v = valid_bit(col.valid, br);
+            if (v) {
+                val = __ldg(reinterpret_cast<const T *>(col.values) + br);
+                if (sizeof(T) == 4 && col.null_sentinel && (int32_t)val == INT32_MIN) v = false;
+            }
+        }
+        uint32_t ball = __ballot_sync(0xffffffffu, v);
+        if (lane == 0) sm.warp[warp] = __popc(ball);
+        __syncthreads();
+        scan_warp_counts(sm.warp);
+        __syncthreads();
+        if (v) vals[running + sm.warp[warp] + __popc(ball & lanemask_lt())] = val;
+        if (lane < 4) {
+            uint32_t byte = (slab * kMatThreads + warp * 32) / 8 + lane;
+            if (byte < bm_bytes) bm[byte] = (uint8_t)(ball >> (8 * lane));
+        }
+        running += sm.warp[kMatThreads / 32];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        reinterpret_cast<uint16_t *>(sp)[0] = (uint16_t)nr;
+        reinterpret_cast<uint16_t *>(sp)[1] = (uint16_t)running;
+    }
+    __syncthreads();
+    uint4 *dst = reinterpret_cast<uint4 *>(out + pg * kPageSize);
+    for (uint32_t k = threadIdx.x; k < kPageSize / 16; k += blockDim.x) dst[k] = sm.page[k];
+    __syncthreads();
+}
+
 template <typename T>
 __global__ void __launch_bounds__(kMatThreads)
-    k_write_fixed(ColView col, uint64_t rows, uint32_t R, uint64_t num_pages,
-                  uint8_t *__restrict__ out) {
-    __shared__ uint4 s_page[kPageSize / 16];
-    __shared__ uint32_t s_warp[kMatThreads / 32 + 1];
-    constexpr uint32_t DB = sizeof(T) == 4 ? 4u : 8u;
-    uint8_t *sp = reinterpret_cast<uint8_t *>(s_page);
-    const uint32_t warp = threadIdx.x >> 5, lane = lane_id();
-    for (uint64_t pg = blockIdx.x; pg < num_pages; pg += gridDim.x) {
-        for (uint32_t k = threadIdx.x; k < kPageSize / 16; k += blockDim.x) s_page[k] = make_uint4(0, 0, 0, 0);
-        __syncthreads();
-        const uint64_t r0 = pg * R;
-        const uint32_t nr = (uint32_t)min((uint64_t)R, rows - r0);
-        const uint32_t bm_bytes = (nr + 7) / 8;
-        uint8_t *bm = sp + kPageSize - bm_bytes;
-        T *vals = reinterpret_cast<T *>(sp + DB);
-        uint32_t running = 0;
-        for (uint32_t slab = 0; slab * kMatThreads < nr; ++slab) {
-            const uint32_t r = slab * kMatThreads + threadIdx.x;
-            bool v = false;
-            T val = T(0);
-            if (r < nr) {
-                uint32_t br = base_row(col, (uint32_t)(r0 + r));
-                v = valid_bit(col.valid, br);
-                if (v) {
-                    val = __ldg(reinterpret_cast<const T *>(col.values) + br);
-                    if (sizeof(T) == 4 && col.null_sentinel && (int32_t)val == INT32_MIN) v = false;
-                }
-            }
-            uint32_t ball = __ballot_sync(0xffffffffu, v);
-            if (lane == 0) s_warp[warp] = __popc(ball);
-            __syncthreads();
-            scan_warp_counts(s_warp);
-            __syncthreads();
-            if (v) vals[running + s_warp[warp] + __popc(ball & lanemask_lt())] = val;
-            if (lane < 4) {
-                uint32_t byte = (slab * kMatThreads + warp * 32) / 8 + lane;
-                if (byte < bm_bytes) bm[byte] = (uint8_t)(ball >> (8 * lane));
-            }
-            running += s_warp[kMatThreads / 32];
-            __syncthreads();
-        }
+    k_write_fixed(ColView col, uint64_t rows, uint32_t R, uint64_t num_pages, uint8_t *__restrict__ out) {
+    __shared__ PageSmem sm;
+    for (uint64_t pg = blockIdx.x; pg < num_pages; pg += gridDim.x) write_fixed_page<T>(col, rows, R, pg, out, sm);
+}
+
+/* Grouped page writer: every fixed-width output column of a batch. */
+__global__ void __launch_bounds__(kMatThreads)
+    k_write_fixed_grouped(const PageTask *__restrict__ tasks, uint32_t ntasks, uint64_t total_pages) {
+    __shared__ PageSmem sm;
+    __shared__ uint32_t s_task;
+    for (uint64_t gp = blockIdx.x; gp < total_pages; gp += gridDim.x) {
         if (threadIdx.x == 0) {
-            reinterpret_cast<uint16_t *>(sp)[0] = (uint16_t)nr;
-            reinterpret_cast<uint16_t *>(sp)[1] = (uint16_t)running;
+            uint32_t lo = 0, hi = ntasks;
+            while (hi - lo > 1) {
+                uint32_t mid = (lo + hi) >> 1;
+                if (tasks[mid].page_base <= gp) lo = mid;
+                else hi = mid;
+            }
+            s_task = lo;
         }
         __syncthreads();
-        uint4 *dst = reinterpret_cast<uint4 *>(out + pg * kPageSize);
-        for (uint32_t k = threadIdx.x; k < kPageSize / 16; k += blockDim.x) dst[k] = s_page[k];
+        const PageTask &T = tasks[s_task];
+        const uint64_t pg = gp - T.page_base;
+        if (T.col.type == CJ_INT32)
+            write_fixed_page<int32_t>(T.col, T.rows, rows_per_page_dev(CJ_INT32), pg, T.out, sm);
+        else
+            write_fixed_page<long long>(T.col, T.rows, rows_per_page_dev(CJ_INT64), pg, T.out, sm);
+    }
+}
+
+/* Grouped row-id gather: task k covers global chunks [chunk_base, ...). */
+__global__ void k_gather_grouped(const GatherTask *__restrict__ tasks, uint32_t ntasks, uint64_t total_chunks) {
+    __shared__ uint32_t s_task;
+    for (uint64_t gc = blockIdx.x; gc < total_chunks; gc += gridDim.x) {
+        if (threadIdx.x == 0) {
+            uint32_t lo = 0, hi = ntasks;
+            while (hi - lo > 1) {
+                uint32_t mid = (lo + hi) >> 1;
+                if (tasks[mid].chunk_base <= gc) lo = mid;
+                else hi = mid;
+            }
+            s_task = lo;
+        }
+        __syncthreads();
+        const GatherTask &T = tasks[s_task];
+        const uint64_t r0 = (gc - T.chunk_base) * kGatherChunk;
+        const uint64_t r1 = min(T.n, r0 + kGatherChunk);
+        for (uint64_t i = r0 + threadIdx.x; i < r1; i += blockDim.x) T.out[i] = __ldg(T.src + __ldcs(T.idx + i));
         __syncthreads();
     }
 }
@@ -329,6 +389,24 @@ cudaError_t launch_gather_u32(const Launch &L, const uint32_t *src, const uint32
     uint64_t cap = (uint64_t)L.num_sms * 8;
     if (g > cap) g = cap;
     k_gather_u32<<<(unsigned)g, 256, 0, L.stream>>>(src, idx, n, out);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_write_fixed_grouped(const Launch &L, const PageTask *tasks_dev, uint32_t ntasks,
+                                      uint64_t total_pages) {
+    if (!total_pages) return cudaSuccess;
+    uint64_t g = std::min<uint64_t>(total_pages, (uint64_t)L.num_sms * 6);
+    k_write_fixed_grouped<<<(unsigned)g, kMatThreads, 0, L.stream>>>(tasks_dev, ntasks, total_pages);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_gather_grouped(const Launch &L, const GatherTask *tasks_dev, uint32_t ntasks,
+                                  uint64_t total_chunks) {
+    if (!total_chunks) return cudaSuccess;
+    uint64_t g = std::min<uint64_t>(total_chunks, (uint64_t)L.num_sms * 8);
+    k_gather_grouped<<<(unsigned)g, 256, 0, L.stream>>>(tasks_dev, ntasks, total_chunks);
     count_launches(1);
     return cudaGetLastError();
 }

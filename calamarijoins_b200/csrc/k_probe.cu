@@ -149,60 +149,147 @@ struct LoopMatcher {
     }
 };
 
+struct ProbeSmem {
+    uint32_t warp[kProbeThreads / 32 + 1];
+    uint32_t tile;
+    uint32_t task;
+    unsigned long long base;
+};
+
+/* One probe tile: count, scan, look back, write. Block-wide. */
+template <class M>
+CJ_DEV void probe_tile(const ColView &pkey, uint32_t n, const M &m, const typename M::Shared &sh,
+                       const MatchOut &out, unsigned long long *status, uint32_t num_tiles, uint32_t tile,
+                       unsigned int *err, ProbeSmem &ps) {
+    const uint32_t warp = threadIdx.x >> 5, lane = lane_id();
+    const uint64_t row0 = (uint64_t)tile * kTileRows + (uint64_t)warp * 32 * kProbeItems;
+    int64_t key[kProbeItems];
+    uint32_t cnt[kProbeItems], pre[kProbeItems];
+    typename M::State st[kProbeItems];
+    uint32_t wrun = 0;
+#pragma unroll
+    for (int it = 0; it < kProbeItems; ++it) {
+        uint64_t i = row0 + (uint64_t)it * 32 + lane;
+        cnt[it] = 0;
+        key[it] = 0;
+        if (i < n && load_key_stream(pkey, (uint32_t)i, &key[it])) cnt[it] = m.count(sh, key[it], st[it]);
+        uint32_t incl = warp_inclusive_scan(cnt[it]);
+        pre[it] = wrun + incl - cnt[it];
+        wrun += __shfl_sync(0xffffffffu, incl, 31);
+    }
+    if (lane == 0) ps.warp[warp] = wrun;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t w = lane < kProbeThreads / 32 ? ps.warp[lane] : 0u;
+        uint32_t wi = warp_inclusive_scan(w);
+        if (lane < kProbeThreads / 32) ps.warp[lane] = wi - w;
+        if (lane == 31) ps.warp[kProbeThreads / 32] = wi;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        TileSched ts{nullptr, status, num_tiles};
+        uint32_t agg = ps.warp[kProbeThreads / 32];
+        unsigned long long b = tile_lookback(ts, tile, agg, err);
+        ps.base = b;
+        if (tile == num_tiles - 1) *out.counter = b + agg;
+    }
+    __syncthreads();
+    const unsigned long long base = ps.base + ps.warp[warp];
+#pragma unroll
+    for (int it = 0; it < kProbeItems; ++it) {
+        if (!cnt[it]) continue;
+        uint64_t i = row0 + (uint64_t)it * 32 + lane;
+        m.write(sh, key[it], st[it], base + pre[it], (uint32_t)i, out);
+    }
+    __syncthreads();
+}
+
 template <class M>
 __global__ void __launch_bounds__(kProbeThreads)
     k_probe_tiles(ColView pkey, uint32_t n, M m, MatchOut out, TileSched ts, unsigned int *err) {
     __shared__ typename M::Shared sh;
-    __shared__ uint32_t s_warp[kProbeThreads / 32 + 1];
-    __shared__ uint32_t s_tile;
-    __shared__ unsigned long long s_base;
+    __shared__ ProbeSmem ps;
     m.init(sh);
     __syncthreads();
-    const uint32_t warp = threadIdx.x >> 5, lane = lane_id();
     for (;;) {
-        if (threadIdx.x == 0) s_tile = atomicAdd(ts.ticket, 1u);
+        if (threadIdx.x == 0) ps.tile = atomicAdd(ts.ticket, 1u);
         __syncthreads();
-        const uint32_t tile = s_tile;
+        const uint32_t tile = ps.tile;
         if (tile >= ts.num_tiles) break;
-        const uint64_t row0 = (uint64_t)tile * kTileRows + (uint64_t)warp * 32 * kProbeItems;
-        int64_t key[kProbeItems];
-        uint32_t cnt[kProbeItems], pre[kProbeItems];
-        typename M::State st[kProbeItems];
-        uint32_t wrun = 0;
-#pragma unroll
-        for (int it = 0; it < kProbeItems; ++it) {
-            uint64_t i = row0 + (uint64_t)it * 32 + lane;
-            cnt[it] = 0;
-            key[it] = 0;
-            if (i < n && load_key_stream(pkey, (uint32_t)i, &key[it])) cnt[it] = m.count(sh, key[it], st[it]);
-            uint32_t incl = warp_inclusive_scan(cnt[it]);
-            pre[it] = wrun + incl - cnt[it];
-            wrun += __shfl_sync(0xffffffffu, incl, 31);
-        }
-        if (lane == 0) s_warp[warp] = wrun;
-        __syncthreads();
-        if (warp == 0) {
-            uint32_t w = lane < kProbeThreads / 32 ? s_warp[lane] : 0u;
-            uint32_t wi = warp_inclusive_scan(w);
-            if (lane < kProbeThreads / 32) s_warp[lane] = wi - w;
-            if (lane == 31) s_warp[kProbeThreads / 32] = wi;
-        }
-        __syncthreads();
+        probe_tile(pkey, n, m, sh, out, ts.status, ts.num_tiles, tile, err, ps);
+    }
+}
+
+/* Grouped probe: the tiles of every join of a batch level in one
+ * persistent launch. Task k owns global tiles [tile_base[k],
+ * tile_base[k+1]); tickets are global, so a tile's predecessors in its
+ * own join always hold earlier tickets. */
+struct GroupedShared {
+    union {
+        HashMatcher<int32_t>::Shared h;
+        LoopMatcher::Shared l;
+    };
+};
+
+__global__ void __launch_bounds__(kProbeThreads)
+    k_probe_grouped(const ProbeTask *__restrict__ tasks, uint32_t ntasks, uint32_t total_tiles,
+                    unsigned int *ticket, const uint16_t *__restrict__ g_bloom, unsigned int *err) {
+    __shared__ GroupedShared sh;
+    __shared__ ProbeSmem ps;
+    __shared__ uint32_t loaded_task;
+    if (threadIdx.x == 0) loaded_task = 0xffffffffu;
+    load_bloom(sh.h.bloom, g_bloom);
+    __syncthreads();
+    bool bloom_live = true;
+    for (;;) {
         if (threadIdx.x == 0) {
-            uint32_t agg = s_warp[kProbeThreads / 32];
-            unsigned long long b = tile_lookback(ts, tile, agg, err);
-            s_base = b;
-            if (tile == ts.num_tiles - 1) *out.counter = b + agg;
+            uint32_t t = atomicAdd(ticket, 1u);
+            ps.tile = t;
+            /* task = last k with tile_base[k] <= t */
+            uint32_t lo = 0, hi = ntasks;
+            while (hi - lo > 1) {
+                uint32_t mid = (lo + hi) >> 1;
+                if (tasks[mid].tile_base <= t) lo = mid;
+                else hi = mid;
+            }
+            ps.task = lo;
         }
         __syncthreads();
-        const unsigned long long base = s_base + s_warp[warp];
-#pragma unroll
-        for (int it = 0; it < kProbeItems; ++it) {
-            if (!cnt[it]) continue;
-            uint64_t i = row0 + (uint64_t)it * 32 + lane;
-            m.write(sh, key[it], st[it], base + pre[it], (uint32_t)i, out);
+        const uint32_t gt = ps.tile;
+        if (gt >= total_tiles) break;
+        const ProbeTask &T = tasks[ps.task];
+        const uint32_t tile = gt - T.tile_base;
+        if (T.kind == 1) {
+            LoopMatcher m{T.nl_keys, T.nl_rids, T.nl_count};
+            if (loaded_task != ps.task) {
+                __syncthreads();
+                m.init(sh.l);
+                __syncthreads();
+                if (threadIdx.x == 0) loaded_task = ps.task;
+                bloom_live = false;
+                __syncthreads();
+            }
+            probe_tile(T.pkey, T.n_probe, m, sh.l, T.out, T.status, T.num_tiles, tile, err, ps);
+        } else {
+            if (!bloom_live) {
+                __syncthreads();
+                load_bloom(sh.h.bloom, g_bloom);
+                if (threadIdx.x == 0) loaded_task = 0xffffffffu;
+                bloom_live = true;
+                __syncthreads();
+            }
+            if (T.build_key_type == CJ_INT32) {
+                HashMatcher<int32_t> m{{T.dir, reinterpret_cast<const Tuple<int32_t> *>(T.tuples), T.log2_slots},
+                                       g_bloom};
+                probe_tile(T.pkey, T.n_probe, m, sh.h, T.out, T.status, T.num_tiles, tile, err, ps);
+            } else {
+                HashMatcher<int64_t> m{{T.dir, reinterpret_cast<const Tuple<int64_t> *>(T.tuples), T.log2_slots},
+                                       g_bloom};
+                probe_tile(T.pkey, T.n_probe, m,
+                           *reinterpret_cast<const HashMatcher<int64_t>::Shared *>(&sh.h), T.out, T.status,
+                           T.num_tiles, tile, err, ps);
+            }
         }
-        __syncthreads();
     }
 }
 
@@ -272,6 +359,47 @@ cudaError_t launch_nl_collect(const Launch &L, const ColView &bkey, uint32_t n_b
                               int64_t *keys, uint32_t *rids, uint32_t *count) {
     if (n_build > kNestedLoopMax) return cudaErrorInvalidValue;
     k_nl_collect<<<1, 64, 0, L.stream>>>(bkey, n_build, keys, rids, count);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+uint32_t probe_tiles(uint32_t n_probe) { return (n_probe + kTileRows - 1) / kTileRows; }
+
+cudaError_t launch_probe_grouped(const Launch &L, const ProbeTask *tasks_dev, uint32_t ntasks, uint32_t total_tiles,
+                                 unsigned int *ticket, const uint16_t *bloom) {
+    if (total_tiles == 0) return cudaSuccess;
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_probe_grouped, kProbeThreads, 0);
+    if (per_sm < 1) per_sm = 1;
+    uint64_t grid = (uint64_t)L.num_sms * per_sm;
+    if (grid > total_tiles) grid = total_tiles;
+    k_probe_grouped<<<(unsigned)grid, kProbeThreads, 0, L.stream>>>(tasks_dev, ntasks, total_tiles, ticket, bloom,
+                                                                       L.dev_errors);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+__global__ void k_nl_collect_grouped(const NlCollectTask *__restrict__ tasks) {
+    const NlCollectTask &T = tasks[blockIdx.x];
+    __shared__ uint32_t s_w0;
+    const uint32_t i = threadIdx.x;
+    int64_t k = 0;
+    bool v = i < T.n_build && load_key(T.bkey, i, &k);
+    uint32_t ball = __ballot_sync(0xffffffffu, v);
+    uint32_t off = __popc(ball & lanemask_lt());
+    if (threadIdx.x == 31) s_w0 = __popc(ball);
+    __syncthreads();
+    if (threadIdx.x >= 32) off += s_w0;
+    if (v) {
+        T.keys[off] = k;
+        T.rids[off] = i;
+    }
+    if (threadIdx.x == 63) *T.count = off + (v ? 1u : 0u);
+}
+
+cudaError_t launch_nl_collect_grouped(const Launch &L, const NlCollectTask *tasks_dev, uint32_t ntasks) {
+    if (!ntasks) return cudaSuccess;
+    k_nl_collect_grouped<<<ntasks, 64, 0, L.stream>>>(tasks_dev);
     count_launches(1);
     return cudaGetLastError();
 }

@@ -1,0 +1,358 @@
+/*
+ * server.cpp — serving: plans submitted as they arrive run concurrently on
+ * one GPU (no reference counterpart; the reference runs one plan per
+ * execute() call).
+ *
+ * A server owns `slots` worker threads, each with its own context (CUDA
+ * stream, status block, staging) and all allocating from one shared,
+ * stream-ordered memory pool. Requests queue in arrival order; the head of
+ * the queue is admitted as soon as a slot is free and its estimated device
+ * footprint fits in the memory budget next to the plans already running,
+ * so work of different plans overlaps on the device while the sum of their
+ * estimates never exceeds the budget. A plan whose estimate alone exceeds
+ * the budget is rejected at submission (CJ_ERR_REJECTED). Latency is
+ * measured from submission to completion.
+ */
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <mutex>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "engine.h"
+
+namespace {
+
+double now_us() {
+    return std::chrono::duration<double, std::micro>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+uint64_t col_bytes_per_row(int32_t t) {
+    switch (t) {
+    case CJ_INT32: return 4;
+    case CJ_VARCHAR: return 8;
+    default: return 8;
+    }
+}
+
+struct Est {
+    uint64_t rows;
+    uint64_t cols;
+};
+
+/* Upper-bound style footprint of a plan: uploaded pages, decoded columns,
+ * per join the hash structures, match arrays and row-id vectors (join
+ * output rows estimated as the larger input, the foreign-key case), and the
+ * output pages. */
+uint64_t estimate_bytes(const cj_plan_desc &p) {
+    uint64_t bytes = 0;
+    for (uint64_t t = 0; t < p.num_inputs; ++t) {
+        const bool resident = p.resident_inputs && p.resident_inputs[t];
+        if (resident || !p.inputs) continue;
+        const cj_table_desc &td = p.inputs[t];
+        for (uint64_t c = 0; c < td.num_columns; ++c) {
+            bytes += td.columns[c].num_pages * CJ_PAGE_SIZE;
+            bytes += td.num_rows * col_bytes_per_row(td.columns[c].type) + td.num_rows / 8 + 16 * td.columns[c].num_pages;
+        }
+    }
+    std::vector<Est> memo(p.num_nodes, Est{0, 0});
+    std::vector<int> state(p.num_nodes, 0);
+    /* iterative post-order over the plan DAG */
+    std::vector<uint64_t> stack{p.root};
+    while (!stack.empty()) {
+        uint64_t n = stack.back();
+        if (n >= p.num_nodes) return UINT64_MAX;
+        const cj_plan_node &node = p.nodes[n];
+        if (state[n] == 2) {
+            stack.pop_back();
+            continue;
+        }
+        if (node.node_type == CJ_NODE_SCAN) {
+            uint64_t rows = 0;
+            if (node.base_table_id < p.num_inputs) {
+                if (p.resident_inputs && p.resident_inputs[node.base_table_id])
+                    rows = p.resident_inputs[node.base_table_id]->num_rows;
+                else if (p.inputs)
+                    rows = p.inputs[node.base_table_id].num_rows;
+            }
+            memo[n] = {rows, node.num_output_attrs};
+            state[n] = 2;
+            stack.pop_back();
+            continue;
+        }
+        if (state[n] == 0) {
+            state[n] = 1;
+            stack.push_back(node.left);
+            stack.push_back(node.right);
+            continue;
+        }
+        const Est &l = memo[node.left], &r = memo[node.right];
+        const uint64_t b = std::min(l.rows, r.rows), pr = std::max(l.rows, r.rows);
+        uint64_t slots = 2048;
+        while (slots < b) slots <<= 1;
+        bytes += slots * 8 + b * 32 + pr * 8 + pr * 4 * node.num_output_attrs;
+        memo[n] = {pr, node.num_output_attrs};
+        state[n] = 2;
+        stack.pop_back();
+    }
+    const cj_plan_node &root = p.nodes[p.root];
+    bytes += memo[p.root].rows * 9 * root.num_output_attrs + (64u << 20);
+    return bytes;
+}
+
+} // namespace
+
+struct cj_server {
+    int device = 0;
+    cudaMemPool_t pool = nullptr;
+    uint64_t budget = 0;
+    uint32_t flags = 0;
+    std::vector<std::unique_ptr<cj::Context>> workers;
+    std::vector<std::thread> threads;
+
+    struct Req {
+        const cj_plan_desc *plan = nullptr;
+        uint64_t est = 0;
+        int status = CJ_OK;
+        std::string err;
+        cj_result *res = nullptr;
+        cj_exec_stats stats{};
+        double t_submit = 0, t_start = 0, t_done = 0;
+        bool started = false, done = false, collected = false;
+    };
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::deque<uint64_t> queue;
+    std::unordered_map<uint64_t, Req> reqs;
+    uint64_t next_ticket = 1;
+    uint64_t admitted = 0, peak_admitted = 0;
+    uint32_t running = 0;
+    bool stop = false;
+    /* statistics */
+    uint64_t submitted = 0, completed = 0, failed = 0, rejected = 0, cancelled = 0;
+    std::vector<double> latencies;
+    double t_first = 0, t_last = 0;
+
+    void worker(size_t w) {
+        cj::Context &ctx = *workers[w];
+        cudaSetDevice(device);
+        for (;;) {
+            uint64_t ticket = 0;
+            const cj_plan_desc *plan = nullptr;
+            {
+                std::unique_lock<std::mutex> lk(mu);
+                cv_work.wait(lk, [&] {
+                    if (stop) return true;
+                    if (queue.empty()) return false;
+                    const Req &h = reqs[queue.front()];
+                    return admitted + h.est <= budget || running == 0;
+                });
+                if (stop) return;
+                ticket = queue.front();
+                queue.pop_front();
+                Req &r = reqs[ticket];
+                r.started = true;
+                r.t_start = now_us();
+                admitted += r.est;
+                peak_admitted = std::max(peak_admitted, admitted);
+                ++running;
+                plan = r.plan;
+            }
+            int status = CJ_OK;
+            std::string err;
+            cj_result *res = nullptr;
+            cj_exec_stats st{};
+            try {
+                res = cj::execute_plan(ctx, *plan, flags, &st);
+            } catch (const cj::Error &e) {
+                status = e.code;
+                err = e.msg;
+                cudaStreamSynchronize(ctx.stream);
+                cudaGetLastError();
+            } catch (const std::bad_alloc &) {
+                status = CJ_ERR_OUT_OF_MEMORY;
+                err = "host allocation failed";
+            } catch (...) {
+                status = CJ_ERR_INTERNAL;
+                err = "unexpected exception";
+            }
+            {
+                std::lock_guard<std::mutex> lk(mu);
+                Req &r = reqs[ticket];
+                r.status = status;
+                r.err = err;
+                r.res = res;
+                r.stats = st;
+                r.done = true;
+                r.t_done = now_us();
+                admitted -= r.est;
+                --running;
+                if (status == CJ_OK) {
+                    ++completed;
+                    latencies.push_back(r.t_done - r.t_submit);
+                } else {
+                    ++failed;
+                }
+                t_last = r.t_done;
+            }
+            cv_done.notify_all();
+            cv_work.notify_all();
+        }
+    }
+};
+
+namespace {
+int serr(int code, const std::string &m) { return cj::set_last_error(code, m); }
+} // namespace
+
+extern "C" {
+
+int cj_server_estimate(const cj_plan_desc *plan, uint64_t *bytes) {
+    if (!plan || !bytes || !plan->nodes || plan->root >= plan->num_nodes)
+        return serr(CJ_ERR_INVALID_ARGUMENT, "bad plan");
+    *bytes = estimate_bytes(*plan);
+    return CJ_OK;
+}
+
+int cj_server_create(const cj_server_config *cfg, cj_server **out) {
+    if (!cfg || !out) return serr(CJ_ERR_INVALID_ARGUMENT, "null argument");
+    *out = nullptr;
+    auto s = std::make_unique<cj_server>();
+    try {
+        int dev = cfg->device;
+        if (dev < 0) cj::check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
+        cj::check_cuda(cudaSetDevice(dev), "cudaSetDevice");
+        s->device = dev;
+        s->pool = cj::create_pool(dev);
+        s->flags = cfg->exec_flags;
+        size_t free_b = 0, total_b = 0;
+        cj::check_cuda(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo");
+        s->budget = cfg->memory_budget ? cfg->memory_budget : (uint64_t)(free_b * 0.85);
+        const uint32_t slots = cfg->slots ? cfg->slots : 4;
+        for (uint32_t w = 0; w < slots; ++w) s->workers.emplace_back(cj::create_context(dev, s->pool));
+    } catch (const cj::Error &e) {
+        for (auto &w : s->workers) w.reset();
+        if (s->pool) cudaMemPoolDestroy(s->pool);
+        return serr(e.code, e.msg);
+    }
+    for (size_t w = 0; w < s->workers.size(); ++w) s->threads.emplace_back(&cj_server::worker, s.get(), w);
+    *out = s.release();
+    return CJ_OK;
+}
+
+int cj_server_submit(cj_server *s, const cj_plan_desc *plan, uint64_t *ticket) {
+    if (!s || !plan || !ticket) return serr(CJ_ERR_INVALID_ARGUMENT, "null argument");
+    if (!plan->nodes || plan->root >= plan->num_nodes) return serr(CJ_ERR_INVALID_PLAN, "bad plan");
+    const uint64_t est = estimate_bytes(*plan);
+    cj::clear_last_error();
+    std::lock_guard<std::mutex> lk(s->mu);
+    ++s->submitted;
+    if (est > s->budget) {
+        ++s->rejected;
+        return serr(CJ_ERR_REJECTED, "estimated footprint " + std::to_string(est) + " bytes exceeds the budget");
+    }
+    const uint64_t t = s->next_ticket++;
+    cj_server::Req &r = s->reqs[t];
+    r.plan = plan;
+    r.est = est;
+    r.t_submit = now_us();
+    if (s->t_first == 0) s->t_first = r.t_submit;
+    s->queue.push_back(t);
+    *ticket = t;
+    s->cv_work.notify_one();
+    return CJ_OK;
+}
+
+int cj_server_wait(cj_server *s, uint64_t ticket, int64_t timeout_us, cj_result **out, cj_exec_stats *stats) {
+    if (!s || !out) return serr(CJ_ERR_INVALID_ARGUMENT, "null argument");
+    *out = nullptr;
+    std::unique_lock<std::mutex> lk(s->mu);
+    auto it = s->reqs.find(ticket);
+    if (it == s->reqs.end() || it->second.collected) return serr(CJ_ERR_INVALID_ARGUMENT, "unknown ticket");
+    auto pred = [&] { return s->reqs[ticket].done; };
+    if (timeout_us < 0) {
+        s->cv_done.wait(lk, pred);
+    } else if (!s->cv_done.wait_for(lk, std::chrono::microseconds(timeout_us), pred)) {
+        return serr(CJ_ERR_TIMEOUT, "plan still running");
+    }
+    cj_server::Req r = s->reqs[ticket];
+    s->reqs.erase(ticket);
+    if (stats) *stats = r.stats;
+    *out = r.res;
+    if (r.status != CJ_OK) return serr(r.status, r.err);
+    return CJ_OK;
+}
+
+int cj_server_cancel(cj_server *s, uint64_t ticket) {
+    if (!s) return serr(CJ_ERR_INVALID_ARGUMENT, "null argument");
+    std::lock_guard<std::mutex> lk(s->mu);
+    auto it = s->reqs.find(ticket);
+    if (it == s->reqs.end()) return serr(CJ_ERR_INVALID_ARGUMENT, "unknown ticket");
+    if (it->second.started) return serr(CJ_ERR_INVALID_ARGUMENT, "plan already running");
+    s->queue.erase(std::remove(s->queue.begin(), s->queue.end(), ticket), s->queue.end());
+    it->second.done = true;
+    it->second.status = CJ_ERR_CANCELLED;
+    it->second.err = "cancelled";
+    ++s->cancelled;
+    s->cv_done.notify_all();
+    s->cv_work.notify_all();
+    return CJ_OK;
+}
+
+int cj_server_get_stats(cj_server *s, cj_server_stats *out, int reset) {
+    if (!s || !out) return serr(CJ_ERR_INVALID_ARGUMENT, "null argument");
+    std::lock_guard<std::mutex> lk(s->mu);
+    cj_server_stats st{};
+    st.submitted = s->submitted;
+    st.completed = s->completed;
+    st.failed = s->failed;
+    st.rejected = s->rejected;
+    st.cancelled = s->cancelled;
+    st.queued = s->queue.size();
+    st.running = s->running;
+    st.admitted_bytes = s->admitted;
+    st.peak_admitted_bytes = s->peak_admitted;
+    st.memory_budget = s->budget;
+    std::vector<double> l = s->latencies;
+    std::sort(l.begin(), l.end());
+    if (!l.empty()) {
+        auto pct = [&](double q) { return l[std::min(l.size() - 1, (size_t)(q * (l.size() - 1) + 0.5))]; };
+        st.p50_us = pct(0.50);
+        st.p99_us = pct(0.99);
+        st.max_us = l.back();
+        double sum = 0;
+        for (double x : l) sum += x;
+        st.mean_us = sum / l.size();
+    }
+    st.wall_s = s->t_last > s->t_first ? (s->t_last - s->t_first) / 1e6 : 0;
+    st.plans_per_s = st.wall_s > 0 ? s->completed / st.wall_s : 0;
+    *out = st;
+    if (reset) {
+        s->latencies.clear();
+        s->completed = s->failed = s->rejected = s->cancelled = s->submitted = 0;
+        s->t_first = s->t_last = 0;
+        s->peak_admitted = s->admitted;
+    }
+    return CJ_OK;
+}
+
+void cj_server_destroy(cj_server *s) {
+    if (!s) return;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->stop = true;
+    }
+    s->cv_work.notify_all();
+    for (auto &t : s->threads) t.join();
+    cudaSetDevice(s->device);
+    for (auto &kv : s->reqs)
+        if (kv.second.res) cj_result_free(kv.second.res);
+    s->workers.clear();
+    if (s->pool) cudaMemPoolDestroy(s->pool);
+    delete s;
+}
+
+} /* extern "C" */

@@ -184,3 +184,73 @@ def execute(plan: Plan, ctx: Context, stats_out: Optional[TimingStats] = None) -
     if stats_out is not None:
         stats_out.__dict__.update(st.__dict__)
     return out
+
+
+def execute_batch(plans, ctx: Context, flags: int = 0, descs=None):
+    """Runs many plans together (cj_execute_batch). Returns (results,
+    statuses, stats): results[i] is a Result or None when plans[i] failed
+    validation (its status code in statuses[i])."""
+    descs = descs or [p if isinstance(p, PlanDescriptor) else PlanDescriptor(p) for p in plans]
+    n = len(descs)
+    arr = (_lib.PlanDesc * max(n, 1))()
+    for i, d in enumerate(descs):
+        arr[i] = d.desc
+    outs = (C.c_void_p * max(n, 1))()
+    sts = (C.c_int32 * max(n, 1))()
+    bs = _lib.BatchStatsC()
+    check(lib().cj_execute_batch(ctx.handle, arr, n, int(flags), outs, sts, C.byref(bs)))
+    results = [Result(outs[i]) if outs[i] else None for i in range(n)]
+    return results, [sts[i] for i in range(n)], {k: getattr(bs, k) for k, _ in _lib.BatchStatsC._fields_}
+
+
+class Server:
+    """Serving front end (cj_server): plans submitted as they arrive run
+    concurrently in `slots` worker streams, admitted in arrival order under
+    a device-memory budget."""
+
+    def __init__(self, device: int = -1, slots: int = 4, memory_budget: int = 0, flags: int = 0):
+        cfg = _lib.ServerConfigC(int(device), int(slots), int(memory_budget), int(flags), 0)
+        h = C.c_void_p()
+        check(lib().cj_server_create(C.byref(cfg), C.byref(h)))
+        self.handle = h.value
+        self._pending = {}
+
+    def submit(self, plan) -> int:
+        desc = plan if isinstance(plan, PlanDescriptor) else PlanDescriptor(plan)
+        t = C.c_uint64()
+        check(lib().cj_server_submit(self.handle, C.byref(desc.desc), C.byref(t)))
+        self._pending[t.value] = desc  # pages must stay alive until wait()
+        return t.value
+
+    def wait(self, ticket: int, timeout_us: int = -1):
+        h = C.c_void_p()
+        es = _lib.ExecStatsC()
+        rc = lib().cj_server_wait(self.handle, int(ticket), int(timeout_us), C.byref(h), C.byref(es))
+        if rc != 10:  # CJ_ERR_TIMEOUT keeps the ticket pending
+            self._pending.pop(ticket, None)
+        check(rc)
+        return Result(h.value), {n: getattr(es, n) for n, _ in _lib.ExecStatsC._fields_}
+
+    def cancel(self, ticket: int):
+        check(lib().cj_server_cancel(self.handle, int(ticket)))
+
+    def stats(self, reset: bool = False) -> dict:
+        st = _lib.ServerStatsC()
+        check(lib().cj_server_get_stats(self.handle, C.byref(st), 1 if reset else 0))
+        return {n: getattr(st, n) for n, _ in _lib.ServerStatsC._fields_}
+
+    @staticmethod
+    def estimate(plan) -> int:
+        desc = plan if isinstance(plan, PlanDescriptor) else PlanDescriptor(plan)
+        b = C.c_uint64()
+        check(lib().cj_server_estimate(C.byref(desc.desc), C.byref(b)))
+        return b.value
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib().cj_server_destroy(self.handle)
+            self.handle = None
+            self._pending.clear()
+
+    def __del__(self):
+        self.close()

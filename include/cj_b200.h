@@ -255,6 +255,27 @@ typedef enum cj_exec_flags {
 int cj_execute(cj_context *ctx, const cj_plan_desc *plan, uint32_t flags,
                cj_result **out, cj_timing_stats *timing, cj_exec_stats *stats);
 
+/* Statistics of one cj_execute_batch call. */
+typedef struct cj_batch_stats {
+    uint64_t num_plans, num_levels, num_joins, num_hash_joins, num_nested_loop_joins;
+    uint64_t probe_rows, matches, probe_reruns;
+    uint64_t kernel_launches, syncs;
+    uint64_t h2d_bytes, d2h_bytes;
+    double total_us;
+} cj_batch_stats;
+
+/* Runs `num_plans` independent plans together (no reference counterpart):
+ * plans advance level by level (a join's level = 1 + its children's), and
+ * every phase of a level (build, nested-loop collect, probe, row-id gather)
+ * is one grouped launch over all joins of that level in all plans, with one
+ * host synchronisation per level. results[i] equals what cj_execute would
+ * return for plans[i]; statuses[i] (may be NULL) is that plan's status
+ * (a plan failing validation gets a NULL result and its code). A device-
+ * side error fails the whole call. */
+int cj_execute_batch(cj_context *ctx, const cj_plan_desc *plans,
+                     uint64_t num_plans, uint32_t flags, cj_result **results,
+                     int32_t *statuses, cj_batch_stats *stats);
+
 int cj_result_num_rows(const cj_result *r, uint64_t *num_rows);
 int cj_result_num_columns(const cj_result *r, uint64_t *num_columns);
 
@@ -272,6 +293,57 @@ int cj_result_copy_column(const cj_result *r, uint64_t c, void *dst,
                           uint64_t dst_bytes);
 
 void cj_result_free(cj_result *r);
+
+/* ------------------------------------------------------------------------ */
+/* Serving: plans run concurrently as they arrive (no reference counterpart; */
+/* the reference executes one plan per execute() call)                       */
+/* ------------------------------------------------------------------------ */
+typedef struct cj_server cj_server;
+
+typedef struct cj_server_config {
+    int32_t device;          /* -1 = current device                          */
+    uint32_t slots;          /* plans running at once (worker streams); 0 = 4 */
+    uint64_t memory_budget;  /* device bytes that admitted plans may hold by
+                                estimate; 0 = 85% of the free memory         */
+    uint32_t exec_flags;     /* cj_exec_flags for every result               */
+    uint32_t reserved;
+} cj_server_config;
+
+typedef struct cj_server_stats {
+    uint64_t submitted, completed, failed, rejected, cancelled;
+    uint64_t queued, running;
+    uint64_t admitted_bytes, peak_admitted_bytes, memory_budget;
+    double p50_us, p99_us, mean_us, max_us; /* submit -> completion         */
+    double wall_s;                          /* first submit -> last finish  */
+    double plans_per_s;
+} cj_server_stats;
+
+int cj_server_create(const cj_server_config *config, cj_server **out);
+
+/* Queues a plan. The plan description and every page it points to must stay
+ * valid until cj_server_wait returns for the ticket. Plans whose estimated
+ * footprint (cj_server_estimate) exceeds the budget are refused with
+ * CJ_ERR_REJECTED; others wait in arrival order until a slot is free and
+ * their estimate fits beside the running plans. */
+int cj_server_submit(cj_server *server, const cj_plan_desc *plan,
+                     uint64_t *ticket);
+
+/* Waits up to timeout_us (-1 = forever) for a ticket; returns the plan's
+ * status and its result (caller frees it, before cj_server_destroy), or
+ * CJ_ERR_TIMEOUT if it is still queued or running. */
+int cj_server_wait(cj_server *server, uint64_t ticket, int64_t timeout_us,
+                   cj_result **out, cj_exec_stats *stats);
+
+/* Cancels a queued plan (its wait returns CJ_ERR_CANCELLED). */
+int cj_server_cancel(cj_server *server, uint64_t ticket);
+
+int cj_server_get_stats(cj_server *server, cj_server_stats *out, int reset);
+
+/* Estimated device footprint of a plan in bytes (admission control). */
+int cj_server_estimate(const cj_plan_desc *plan, uint64_t *bytes);
+
+/* Stops the workers after their running plans; queued plans are dropped. */
+void cj_server_destroy(cj_server *server);
 
 /* ------------------------------------------------------------------------ */
 /* Host utilities                                                            */

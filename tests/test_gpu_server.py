@@ -1,0 +1,87 @@
+"""GPU: serving. Plans submitted together run concurrently (several worker
+streams, one memory pool, admission by estimated bytes) and each result is
+the same as the plan run alone and as the oracle's."""
+import numpy as np
+import pytest
+
+from calamarijoins_b200 import CJError, DataType, PlanDescriptor, Server
+from calamarijoins_b200.datagen import chain_plan, join2
+from oracle import oracle_api as oa
+from tests.helpers import assert_same, run_oracle, run_product
+
+pytestmark = pytest.mark.gpu
+I, L, V = DataType.INT32, DataType.INT64, DataType.VARCHAR
+
+
+def mixed_plans(n, seed=1):
+    rng = np.random.default_rng(seed)
+    plans = []
+    for i in range(n):
+        if i % 3 == 0:
+            plans.append(join2(int(rng.integers(5, 5000)), int(rng.integers(1000, 60000)), seed=i,
+                               build_payload=(L, V), probe_payload=(I,), probe_null=0.05))
+        else:
+            ways = int(rng.integers(2, 5))
+            plans.append(chain_plan(ways, int(rng.integers(1000, 40000)), rng, max_build=20000,
+                                    key_types=[I if rng.random() < 0.7 else L for _ in range(ways - 1)],
+                                    varchar_frac=0.1))
+    return plans
+
+
+def test_alone_equals_in_the_mix(gpu_ctx):
+    plans = mixed_plans(24)
+    alone = [run_product(p, gpu_ctx)[0] for p in plans]
+    srv = Server(slots=4)
+    try:
+        tickets = [srv.submit(p) for p in plans]
+        mixed = []
+        for t in tickets:
+            res, _ = srv.wait(t)
+            mixed.append(oa.PagedResult.from_result(res))
+            res.free()
+        st = srv.stats()
+    finally:
+        srv.close()
+    assert st["completed"] == len(plans) and st["failed"] == 0
+    assert st["p99_us"] >= st["p50_us"] > 0
+    for i, (a, m) in enumerate(zip(alone, mixed)):
+        assert_same(m, a, f"plan {i} alone vs mix")
+    for i in (0, 1, 5):
+        assert_same(mixed[i], run_oracle(plans[i]), f"plan {i} vs oracle")
+
+
+def test_admission_budget_and_rejection():
+    plans = mixed_plans(6, seed=2)
+    est = [Server.estimate(p) for p in plans]
+    srv = Server(slots=4, memory_budget=max(est) + 1)
+    try:
+        tickets = [srv.submit(p) for p in plans]
+        for t in tickets:
+            res, _ = srv.wait(t)
+            res.free()
+        st = srv.stats()
+        assert st["peak_admitted_bytes"] <= st["memory_budget"]
+        big = join2(2_000_000, 4_000_000, seed=3)
+        with pytest.raises(CJError) as e:
+            srv.submit(big)
+        assert e.value.status == 9  # CJ_ERR_REJECTED
+    finally:
+        srv.close()
+
+
+def test_failure_is_isolated():
+    good = join2(1000, 5000, seed=4)
+    bad = join2(1000, 5000, seed=5)
+    bad.inputs[1].num_rows += 1  # pages hold one row fewer than declared
+    srv = Server(slots=2)
+    try:
+        tb, tg = srv.submit(bad), srv.submit(good)
+        with pytest.raises(CJError) as e:
+            srv.wait(tb)
+        assert e.value.status == 3
+        res, _ = srv.wait(tg)
+        r = oa.PagedResult.from_result(res)
+        res.free()
+        assert_same(r, run_oracle(good))
+    finally:
+        srv.close()
