@@ -176,25 +176,51 @@ def ref_threads():
     return best, cands
 
 
-def time_reference(plan, warmup: int, steps: int):
-    """Times oracle/_ref (the reference's execute()) on the host cores."""
+def log(msg: str) -> None:
+    print(f"[bench {time.strftime('%H:%M:%S')}] {msg}", file=sys.stderr, flush=True)
+
+
+def ref_worker(threads: int, scale: float, warmup: int, steps: int) -> None:
+    """Child process: times one reference variant (one variant per process:
+    every variant carries its own worker-pool singleton)."""
     from calamarijoins_b200 import PlanDescriptor
     from oracle import oracle_api as oa
+    plan = gen_workload(False, scale, int32_standin=True)
+    d = PlanDescriptor(plan)
+    for _ in range(max(warmup, 1)):
+        oa.ref_execute(d, threads)
+    ms = []
+    for _ in range(steps):
+        _, w, _ = oa.ref_execute(d, threads)
+        ms.append(w)
+    print(json.dumps({"threads": threads, "ms": statistics.median(ms), "probe_rows": plan.inputs[1].num_rows,
+                      "build_rows": plan.inputs[0].num_rows}))
+
+
+def time_reference(scale: float, warmup: int, steps: int, timeout_s: float = 900):
+    """Times oracle/_ref (the reference's execute()) on the host cores, each
+    thread-count candidate in its own process."""
     best, cands = ref_threads()
     if best is None:
         return None
-    d = PlanDescriptor(plan)
     results = {}
+    info = {}
     for t in cands:
-        for _ in range(max(warmup, 1)):
-            oa.ref_execute(d, t)
-        ms = []
-        for _ in range(steps):
-            _, w, _ = oa.ref_execute(d, t)
-            ms.append(w)
-        results[t] = statistics.median(ms)
+        log(f"reference: {t} threads, scale {scale}")
+        res = subprocess.run([sys.executable, os.path.abspath(__file__), "--ref-worker", str(t), "--scale", str(scale),
+                              "--warmup", str(warmup), "--steps", str(steps)], capture_output=True, text=True,
+                             timeout=timeout_s)
+        if res.returncode != 0:
+            log(f"reference variant {t} failed: {res.stderr[-500:]}")
+            continue
+        r = json.loads(res.stdout.strip().splitlines()[-1])
+        results[t] = r["ms"]
+        info = r
+    if not results:
+        return None
     t_best = min(results, key=results.get)
-    return {"threads": t_best, "ms": results[t_best], "all_ms": results}
+    return {"threads": t_best, "ms": results[t_best], "all_ms": results, "probe_rows": info["probe_rows"],
+            "build_rows": info["build_rows"]}
 
 
 def run_reference(args):
@@ -202,16 +228,15 @@ def run_reference(args):
     if rank != 0:
         return 0
     scale = args.scale
-    plan = gen_workload(False, scale, int32_standin=True)
-    r = time_reference(plan, args.warmup, args.steps)
+    r = time_reference(scale, args.warmup, args.steps)
     if r is None:
         print(json.dumps({"impl": "reference", "unavailable": "reference not compiled into oracle/_ref"}))
         return 0
-    npr = plan.inputs[1].num_rows
+    npr = r["probe_rows"]
     val = npr / (r["ms"] / 1000.0)
-    sample = (f"C2 shape at scale {scale}: {plan.inputs[0].num_rows} x {npr} rows, INT32 stand-ins for the "
+    sample = (f"C2 shape at scale {scale}: {r['build_rows']} x {npr} rows, INT32 stand-ins for the "
               f"INT64/FP64 payloads (the reference cannot emit them); median of {args.steps} runs after "
-              f"{max(args.warmup, 1)} warm-up; best of thread counts {sorted(r['all_ms'])}")
+              f"{max(args.warmup, 1)} warm-up; best of thread counts {sorted(r['all_ms'])} on {os.cpu_count()} CPUs")
     line = {"impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": 0, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": r["ms"], "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "int32", "data": "synthetic",
@@ -239,7 +264,9 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
     ctx = cj.Context(local)
+    log("generating workload")
     plan = gen_workload(True, args.scale)
+    log("uploading resident tables")
     info = plan_info(plan)
     resident = cj.Plan()
     resident.nodes, resident.root = plan.nodes, plan.root
@@ -255,8 +282,10 @@ def run_ours(args):
         res.free()
         return st
 
+    log("warm-up")
     for _ in range(args.warmup):
         st = step_device()
+    log("timed device steps")
     ctx.set_option(_lib.CJ_OPT_PROFILE_KERNELS, 1)
     ctx.profile_reset()
     if dist:
@@ -284,6 +313,7 @@ def run_ours(args):
     value = probe_rows / (ms_step / 1000.0)
 
     # e2e through the public API with host buffers
+    log("end-to-end steps")
     for _ in range(max(1, args.warmup)):
         res, st_h = cj.execute_raw(plan, ctx, 0, d_host)
         res.free()
@@ -304,6 +334,7 @@ def run_ours(args):
         e2e_s = float(t.item())
     e2e_value = probe_rows / e2e_s
 
+    log("cpu baseline")
     # roofline of the dominant kernel
     peak, peak_kind = measured_peaks()
     dom = max(prof.items(), key=lambda kv: kv[1][1]) if prof else None
@@ -324,16 +355,14 @@ def run_ours(args):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        sample_scale = args.cpu_scale
-        splan = gen_workload(False, sample_scale, int32_standin=True)
-        r = time_reference(splan, 1, 3)
+        r = time_reference(args.cpu_scale, 1, 3)
         if r is not None:
-            snp = splan.inputs[1].num_rows
+            snp = r["probe_rows"]
             cpu = {"value": snp / (r["ms"] / 1000.0), "unit": UNIT, "cores": r["threads"], "kind": "reference",
-                   "sample": (f"reference execute() (oracle/_ref) on the C2 shape at scale {sample_scale} "
-                              f"({splan.inputs[0].num_rows} x {snp} rows) with INT32 stand-ins for the "
-                              f"INT64/FP64 payloads; median of 3 runs after 1 warm-up; "
-                              f"{r['threads']} threads of {os.cpu_count()} host CPUs")}
+                   "sample": (f"reference execute() (oracle/_ref) on the C2 shape at scale {args.cpu_scale} "
+                              f"({r['build_rows']} x {snp} rows) with INT32 stand-ins for the INT64/FP64 payloads; "
+                              f"median of 3 runs after 1 warm-up; {r['threads']} threads (of {sorted(r['all_ms'])} "
+                              f"tried) on {os.cpu_count()} host CPUs")}
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
@@ -366,7 +395,13 @@ def main(argv=None):
     ap.add_argument("--scale", type=float, default=1.0, help="row-count scale of the workload")
     ap.add_argument("--cpu-scale", type=float, default=0.25, help="scale of the CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-worker", type=int, default=0, help=argparse.SUPPRESS)
     args = ap.parse_args(argv)
+    if args.ref_worker:
+        ref_worker(args.ref_worker, args.scale, args.warmup, args.steps)
+        return 0
+    import faulthandler
+    faulthandler.dump_traceback_later(600, repeat=True, file=sys.stderr)
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
     if args.impl == "reference":

@@ -16,6 +16,8 @@ stands in for re2 (unused on the join path), the range-v3 table loader
 (unused) and the hard-coded hardware constants. The build targets
 x86-64-v3 (AVX2 + SSE4.2 CRC32) instead of -march=native so that the library
 also runs on the GPU host, whose CPU model may differ from the build host.
+Each thread-count variant is self-contained (-fno-gnu-unique,
+-Wl,-Bsymbolic); still, callers load one variant per process.
 
 Usage: python oracle/build_oracle.py [--threads 32,64,...]
 """
@@ -27,7 +29,7 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-DEFAULT_THREADS = (8, 32, 64, 128, 192, 256)
+DEFAULT_THREADS = (8, 16, 32, 64, 128, 192, 256)
 
 
 def _run(cmd: list[str]) -> None:
@@ -78,7 +80,11 @@ def build_reference(threads=DEFAULT_THREADS, force: bool = False) -> list[str]:
     for t in threads:
         out = os.path.join(outdir, f"libcj_ref_t{t}.so")
         if force or not _newer(out, deps):
-            _run(["g++", "-std=c++17", "-O3", "-march=x86-64-v3", "-fpermissive", "-w",
+            # -fno-gnu-unique -Wl,-Bsymbolic: each variant keeps its own
+            # singletons (the worker pool is a function-local static, which
+            # GCC would otherwise merge across every loaded variant)
+            _run(["g++", "-std=c++17", "-O3", "-march=x86-64-v3", "-fpermissive", "-w", "-fno-gnu-unique",
+                  "-Wl,-Bsymbolic",
                   "-DFMT_HEADER_ONLY", f"-DSPC__THREAD_COUNT={t}",
                   "-I", shim, "-I", os.path.join(ref, "include"), "-I", fmt_inc,
                   "-shared", "-fPIC", *sources, "-o", out, "-lpthread"])
