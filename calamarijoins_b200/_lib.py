@@ -118,6 +118,8 @@ _SIGS = {
                              C.POINTER(TimingStatsC), C.POINTER(ExecStatsC)]),
     "cj_execute_batch": (C.c_int, [_P, C.POINTER(PlanDesc), C.c_uint64, C.c_uint32, C.POINTER(_P),
                                    C.POINTER(C.c_int32), C.POINTER(BatchStatsC)]),
+    "cj_hash_join_noalloc": (C.c_int, [_P, _P, C.c_uint32, _P, _P, C.c_uint32, _P, _P, C.c_uint64, _P,
+                                       C.POINTER(C.c_uint64), _P]),
     "cj_result_num_rows": (C.c_int, [_P, C.POINTER(C.c_uint64)]),
     "cj_result_num_columns": (C.c_int, [_P, C.POINTER(C.c_uint64)]),
     "cj_result_column": (C.c_int, [_P, C.c_uint64, C.POINTER(C.c_int32), C.POINTER(C.c_uint64),

@@ -276,6 +276,29 @@ int cj_execute_batch(cj_context *ctx, const cj_plan_desc *plans,
                      uint64_t num_plans, uint32_t flags, cj_result **results,
                      int32_t *statuses, cj_batch_stats *stats);
 
+/* Hash join of two INT32 key arrays already in device memory, for callers
+ * that must not have a library allocate device memory (an engine whose
+ * allocator or fixed budget owns all of the GPU's memory). No counterpart
+ * in the reference. All pointers are device pointers except h_count (host,
+ * may be NULL); valid arrays are bitmaps of ceil(n/32) u32 words, bit r set
+ * when row r has a key (NULL keys never match). The matching (build row,
+ * probe row) pairs are written in probe-row order to out_build_rows /
+ * out_probe_rows (at most `capacity` of them); *d_count receives the full
+ * match count, and *h_count too when given. Work runs on `stream`
+ * (a cudaStream_t) and the call returns after it completes.
+ * Allocates nothing: the hash table and every scratch buffer live in one
+ * fixed 8 MiB device array that each GPU loading the library holds until
+ * exit. Limits: n_build <= 262,144 and n_probe <= 134,217,728; larger inputs
+ * get CJ_ERR_LIMIT. The first call on a device looks up that array's device
+ * address, so make it before any stream capture. Calls share the array:
+ * calls that overlap on the GPU race and must not be issued concurrently. */
+int cj_hash_join_noalloc(const int32_t *build_keys, const uint32_t *build_valid,
+                         uint32_t n_build, const int32_t *probe_keys,
+                         const uint32_t *probe_valid, uint32_t n_probe,
+                         uint32_t *out_build_rows, uint32_t *out_probe_rows,
+                         uint64_t capacity, unsigned long long *d_count,
+                         uint64_t *h_count, void *stream);
+
 int cj_result_num_rows(const cj_result *r, uint64_t *num_rows);
 int cj_result_num_columns(const cj_result *r, uint64_t *num_columns);
 
