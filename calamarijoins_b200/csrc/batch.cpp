@@ -10,7 +10,7 @@
  *   build  (hist / scan / scatter / per-partition build over all hash joins)
  *   nested-loop collect (all joins with build sides <= 64 rows)
  *   probe  (one tile-ticket kernel over all joins; each join keeps its own
- *           look-back status and output arrays)
+ *           match counter and output arrays)
  *   gather (row-id vectors of every intermediate)
  * and one host synchronisation per level reads every join's match count.
  * The root pages of all plans are written by one grouped launch (VARCHAR
@@ -250,7 +250,7 @@ void BatchExecutor::run_level(int lvl) {
         w.log2_slots = bp.log2_slots;
         w.log2_parts = bp.log2_parts;
         const int kb = w.bk.type == CJ_INT32 ? 4 : 8;
-        w.dir = ctx.alloc((1ull << bp.log2_slots) * 8);
+        w.dir = ctx.alloc(build_dir_bytes(bp.log2_slots));
         w.tuples = ctx.alloc(w.B->rows * build_tuple_bytes(kb));
         w.part_buf = ctx.alloc(w.B->rows * build_tuple_bytes(kb));
         BuildGeometry g = build_geometry(L, bp);
@@ -288,7 +288,6 @@ void BatchExecutor::run_level(int lvl) {
         std::vector<ProbeTask> ptasks;
         std::vector<size_t> pidx;
         uint32_t tiles = 0;
-        size_t status_words = 0;
         for (size_t k = 0; k < work.size(); ++k) {
             auto &w = work[k];
             if (!w.B->rows || !w.P->rows) continue;
@@ -297,12 +296,12 @@ void BatchExecutor::run_level(int lvl) {
                 stats.probe_reruns++;
                 w.cap = w.M;
             }
-            status_words += probe_tiles((uint32_t)w.P->rows) + 1;
             pidx.push_back(k);
         }
         if (pidx.empty()) break;
-        DevPtr words = ctx.alloc((status_words + 1) * 8);
-        ck(cudaMemsetAsync(words->ptr, 0, (status_words + 1) * 8, ctx.stream), "memset");
+        const size_t nwords = pidx.size() + 1; /* ticket, then one match counter per join */
+        DevPtr words = ctx.alloc(nwords * 8);
+        ck(cudaMemsetAsync(words->ptr, 0, nwords * 8, ctx.stream), "memset");
         unsigned long long *wp = words->as<unsigned long long>();
         unsigned int *ticket = reinterpret_cast<unsigned int *>(wp);
         size_t off = 1;
@@ -324,18 +323,16 @@ void BatchExecutor::run_level(int lvl) {
             t.out.build_rids = w.mb ? w.mb->as<uint32_t>() : nullptr;
             t.out.probe_rids = w.mp ? w.mp->as<uint32_t>() : nullptr;
             t.out.capacity = (w.need_b || w.need_p) ? w.cap : 0;
-            t.out.counter = wp + off; /* first word of the task: counter */
+            t.out.counter = wp + off++;
             t.num_tiles = probe_tiles(t.n_probe);
-            t.status = wp + off + 1;
             t.tile_base = tiles;
             tiles += t.num_tiles;
-            off += t.num_tiles + 1;
             ptasks.push_back(t);
         }
         DevPtr pt = upload_tasks(ptasks);
         ck(launch_probe_grouped(L, pt->as<ProbeTask>(), (uint32_t)ptasks.size(), tiles, ticket, ctx.d_bloom),
            "probe_grouped");
-        std::vector<unsigned long long> counts(status_words + 1);
+        std::vector<unsigned long long> counts(nwords);
         ck(cudaMemcpyAsync(counts.data(), words->ptr, counts.size() * 8, cudaMemcpyDeviceToHost, ctx.stream), "counts");
         ctx.sync_status();
         stats.syncs++;

@@ -55,7 +55,6 @@ enum DevError : uint32_t {
     DEV_ERR_VARCHAR_OFFSETS = 1u << 1,
     DEV_ERR_LONG_CHAIN = 1u << 2,    /* 0xfffe page without a 0xffff start */
     DEV_ERR_BAD_PAGE_KIND = 1u << 3, /* 0xffff/0xfffe page in a fixed column */
-    DEV_ERR_LOOKBACK = 1u << 4,      /* a tile's look-back wait gave up      */
     DEV_ERR_ROW_COUNT = 1u << 5,     /* pages hold more/fewer rows than the
                                         table declares                       */
     DEV_ERR_INTERNAL = 1u << 31
@@ -165,10 +164,13 @@ cudaError_t launch_check_rows(const Launch &L, const uint64_t *total, uint64_t e
 
 /* Build */
 struct BuildPlan {
-    int log2_slots;      /* directory = 2^log2_slots u64 entries          */
+    int log2_slots;      /* directory = 2^log2_slots u64 entries + 1      */
     int log2_parts;      /* radix partitions                              */
     uint32_t num_rows;   /* rows of the build relation                    */
 };
+/* Directory entry: start (63..32) | count (31..16, saturated) | tags (15..0);
+ * one sentinel entry after the last slot. */
+inline size_t build_dir_bytes(int log2_slots) { return ((1ull << log2_slots) + 1) * sizeof(uint64_t); }
 size_t build_temp_bytes(const Launch &L, const BuildPlan &bp, int key_bytes);
 size_t build_tuple_bytes(int key_bytes);
 cudaError_t launch_build(const Launch &L, const BuildPlan &bp, const ColView &key,
@@ -205,7 +207,7 @@ cudaError_t launch_build_grouped(const Launch &L, const BuildTask *tasks_dev, ui
                                  const uint16_t *bloom, void *temp);
 
 /* Probe and nested loop share one tiled kernel; `sched` is scratch of
- * probe_sched_bytes(n_probe) bytes (tile tickets and look-back status). */
+ * probe_sched_bytes(n_probe) bytes (the tile ticket). */
 size_t probe_sched_bytes(uint32_t n_probe);
 cudaError_t launch_probe_tiles_hash(const Launch &L, const ColView &pkey, uint32_t n_probe,
                                     int32_t build_key_type, const uint64_t *dir,
@@ -232,13 +234,12 @@ struct ProbeTask {
     const int64_t *nl_keys;
     const uint32_t *nl_rids;
     const uint32_t *nl_count;
-    MatchOut out;
-    unsigned long long *status; /* num_tiles look-back words, zeroed        */
+    MatchOut out;               /* out.counter zeroed before launch         */
     uint32_t num_tiles;
     uint32_t tile_base;         /* first global tile of this task           */
 };
 uint32_t probe_tiles(uint32_t n_probe);
-/* `ticket` must be zeroed; each task's status and counter zeroed. */
+/* `ticket` must be zeroed, and each task's counter. */
 cudaError_t launch_probe_grouped(const Launch &L, const ProbeTask *tasks_dev, uint32_t ntasks,
                                  uint32_t total_tiles, unsigned int *ticket, const uint16_t *bloom);
 struct NlCollectTask {

@@ -118,9 +118,8 @@ void Context::sync_status() {
         if (err & DEV_ERR_LONG_CHAIN) what += " long-string continuation without start;";
         if (err & DEV_ERR_BAD_PAGE_KIND) what += " special page in fixed-width column;";
         if (err & DEV_ERR_ROW_COUNT) what += " pages hold a row count other than the table's;";
-        if (err & DEV_ERR_LOOKBACK) what += " tile look-back wait gave up;";
         if (err & DEV_ERR_INTERNAL) what += " internal;";
-        int code = (err & (DEV_ERR_LOOKBACK | DEV_ERR_INTERNAL)) ? CJ_ERR_INTERNAL : CJ_ERR_MALFORMED_PAGE;
+        int code = (err & DEV_ERR_INTERNAL) ? CJ_ERR_INTERNAL : CJ_ERR_MALFORMED_PAGE;
         fail(code, "device reported:" + what);
     }
 }

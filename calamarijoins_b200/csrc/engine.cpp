@@ -248,7 +248,7 @@ Relation Executor::exec_join(uint64_t node_idx, int depth, bool is_root, cj_resu
                 fail(CJ_ERR_LIMIT, "build side too large for one radix pass (max 2^26 rows)");
             log2_slots = bp.log2_slots;
             const int kb = bk.type == CJ_INT32 ? 4 : 8;
-            dir = ctx.alloc((1ull << bp.log2_slots) * 8);
+            dir = ctx.alloc(build_dir_bytes(bp.log2_slots));
             tuples = ctx.alloc(B.rows * build_tuple_bytes(kb));
             DevPtr tmp = ctx.alloc(build_temp_bytes(L, bp, kb));
             KScope k(*this, "build");

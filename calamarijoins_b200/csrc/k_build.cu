@@ -2,10 +2,16 @@
  * k_build.cu — unchained hash-table build with Bloom tags on sm_100a.
  *
  * The table is the reference's UnchainedHashtable (include/join_execution/
- * hashtable.h:63-506): a power-of-two directory of u64 entries
- * (end offset << 16 | OR of 16-bit Bloom tags, :197-246) over a contiguous,
- * slot-ordered tuple array, so a probe reads [dir[s-1] >> 16, dir[s] >> 16)
- * (:298-313). Directory size = pow2 >= max(2048, build rows) (:255-264).
+ * hashtable.h:63-506): a power-of-two directory of u64 entries over a
+ * contiguous, slot-ordered tuple array, each entry carrying the OR of the
+ * slot's 16-bit Bloom tags (:197-246). Directory size = pow2 >= max(2048,
+ * build rows) (:255-264). The reference stores the slot's END offset
+ * (end << 16 | tags) and reads [dir[s-1] >> 16, dir[s] >> 16) (:298-313),
+ * two dependent loads per probe; here an entry holds
+ *     start (bits 63..32) | count (31..16, saturated at 0xFFFF) | tags (15..0)
+ * so one load gives the candidate range. A saturated count is bounded by
+ * the next entry's start; one sentinel entry after the last slot holds the
+ * total tuple count as its start, so the directory has slots + 1 entries.
  *
  * Build = radix partition + per-partition counting sort, the reference's
  * two-pass build (:405-505) mapped to the GPU:
@@ -149,11 +155,13 @@ CJ_DEV void build_partition(const Tuple<K> *__restrict__ in, const uint64_t *__r
         uint32_t s = s0 + k;
         if (s >= S) break;
         uint32_t c = s_cnt[s];
-        uint64_t end = ps + pre + c;
-        dir[(uint64_t)p * S + s] = (end << 16) | (uint64_t)(s_tag[s] & 0xFFFFu);
+        const uint64_t start = ps + pre;
+        dir[(uint64_t)p * S + s] =
+            (start << 32) | ((uint64_t)min(c, 0xFFFFu) << 16) | (uint64_t)(s_tag[s] & 0xFFFFu);
         s_cnt[s] = pre; /* becomes the scatter cursor */
         pre += c;
     }
+    if (threadIdx.x == 0 && p == (1u << log2_parts) - 1) dir[(uint64_t)(p + 1) * S] = pe << 32; /* sentinel */
     __syncthreads();
     for (uint64_t t = ps + threadIdx.x; t < pe; t += blockDim.x) {
         Tuple<K> tp = in[t];

@@ -1,112 +1,96 @@
 /*
  * k_probe.cu — hash probe and nested-loop join on sm_100a.
  *
- * Both are one persistent kernel over probe tiles (NT x ITEMS rows):
- *   - a CTA takes tiles in order from an atomic ticket, so every earlier
- *     tile is already owned by a running CTA;
- *   - each lane counts the matches of ITEMS rows (keys read once, streamed
- *     with evict-first loads so the hash table stays in L2);
- *   - warp scans and a block scan give every row its offset inside the tile;
- *   - the tile's base offset comes from a decoupled look-back over the
- *     preceding tiles' published totals (bounded wait: a stuck predecessor
- *     sets DEV_ERR_LOOKBACK instead of hanging);
- *   - each lane writes its rows' (build row id, probe row id) pairs.
- * Matches therefore come out in probe-row order with no contended atomic,
- * and the last tile publishes the total match count.
+ * Both are one persistent kernel over probe tiles of kTileRows rows:
+ *   - a CTA takes tiles from an atomic ticket;
+ *   - each lane handles kProbeItems rows, one dependent chain each (key ->
+ *     directory entry -> candidate tuples), kept short and register-light so
+ *     that eight CTAs share an SM and their loads overlap;
+ *   - for every match count it remembers the first matching build row, so
+ *     the common case (at most one match) writes without a second lookup;
+ *   - warp scans and a block scan place every row's matches inside the tile,
+ *     and one atomicAdd per tile on the match counter reserves the tile's
+ *     output range (rows stay in probe order inside a tile);
+ *   - the counter ends as the total match count; pairs past the output
+ *     capacity are counted but not written, so the caller can size a re-run.
  *
- * Hash probe: Bloom-tag test on the directory entry, then a scan of the
- * slot's contiguous tuple range (find_indices, include/join_execution/
- * hashtable.h:298-313; probe_columnar / probe_intermediate, hash_join.h:
- * 87-244). NULL probe keys are skipped (hash_join.h:119, 215-218).
+ * Hash probe: Bloom-tag test on the directory entry, then the slot's
+ * contiguous tuple range (find_indices, include/join_execution/hashtable.h:
+ * 298-313; probe_columnar / probe_intermediate, hash_join.h:87-244). NULL
+ * probe keys are skipped (hash_join.h:119, 215-218).
  *
- * Nested loop: the (<= 64) non-NULL build keys sit in shared memory and
- * every warp sweeps them for 32 probe rows at once, the GPU form of the
- * reference's register-resident build side (nested_loop.h:107-244,
- * simd_compare.h:46-163).
+ * Nested loop: the (<= 64) non-NULL build keys sit in shared memory and each
+ * warp sweeps them for 32 probe rows at once, the GPU form of the reference's
+ * register-resident build side (nested_loop.h:107-244, simd_compare.h:46-163).
  */
 #include "cj_device.cuh"
 
 namespace cj {
-
 namespace {
 
+/* 2 rows per thread at 8 CTAs per SM measured fastest on the 4M x 64M
+ * workload (825 us vs 870 us for 4 rows, 1218 us for 8 rows at 4 CTAs). */
+#ifndef CJ_PROBE_ITEMS
+#define CJ_PROBE_ITEMS 2
+#endif
+#ifndef CJ_PROBE_MIN_BLOCKS
+#define CJ_PROBE_MIN_BLOCKS 8
+#endif
 constexpr int kProbeThreads = 256;
-constexpr int kProbeItems = 8;
+constexpr int kProbeItems = CJ_PROBE_ITEMS; /* rows per thread and tile pass            */
 constexpr uint32_t kTileRows = kProbeThreads * kProbeItems;
-constexpr unsigned long long kFlagAgg = 1ull << 62;
-constexpr unsigned long long kFlagPre = 2ull << 62;
-constexpr unsigned long long kValMask = (1ull << 62) - 1;
-constexpr uint64_t kSpinLimit = 1ull << 24;
+constexpr int kProbeMinBlocks = CJ_PROBE_MIN_BLOCKS; /* 8 x 256 threads = 64 warps/SM */
 
 struct TileSched {
-    unsigned int *ticket;         /* zeroed before launch              */
-    unsigned long long *status;   /* num_tiles entries, zeroed         */
+    unsigned int *ticket; /* zeroed before launch */
     uint32_t num_tiles;
 };
 
-/* Publishes this tile's aggregate, accumulates the predecessors' and
- * returns the exclusive prefix (single thread). */
-CJ_DEV unsigned long long tile_lookback(const TileSched &ts, uint32_t tile, uint32_t agg,
-                                        unsigned int *err) {
-    if (tile == 0) {
-        atomicExch(ts.status, kFlagPre | (unsigned long long)agg);
-        return 0;
-    }
-    atomicExch(ts.status + tile, kFlagAgg | (unsigned long long)agg);
-    unsigned long long excl = 0;
-    int64_t p = (int64_t)tile - 1;
-    uint64_t spins = 0;
-    while (p >= 0) {
-        unsigned long long v = *reinterpret_cast<volatile unsigned long long *>(ts.status + p);
-        unsigned long long f = v & ~kValMask;
-        if (f == 0) {
-            if (++spins > kSpinLimit) {
-                atomicOr(err, DEV_ERR_LOOKBACK);
-                break;
-            }
-            __nanosleep(64);
-            continue;
-        }
-        excl += v & kValMask;
-        if (f == kFlagPre) break;
-        --p;
-    }
-    atomicExch(ts.status + tile, kFlagPre | (excl + agg));
-    return excl;
-}
-
 /* ---------------- matchers ---------------- */
+
+/* Directory entry: start of the slot's tuples (bits 63..32), their count
+ * (31..16, saturated at 0xFFFF: then the next entry's start bounds them) and
+ * the OR of their Bloom tags (15..0). */
 template <typename KB> struct HashMatcher {
     HashTableView<KB> ht;
     const uint16_t *g_bloom;
     struct Shared {
         uint16_t bloom[2048];
     };
-    struct State {
-        uint32_t s, e;
-    };
     CJ_DEV void init(Shared &sh) const { load_bloom(sh.bloom, g_bloom); }
-    CJ_DEV uint32_t count(const Shared &sh, int64_t key, State &st) const {
-        uint64_t h = hash_key(key);
-        uint32_t slot = slot_of(h, ht.log2_slots);
-        uint64_t entry = __ldg(ht.dir + slot);
-        uint32_t tag = sh.bloom[bloom_index(h)];
-        st.s = st.e = 0;
-        if ((entry & tag) != tag) return 0;
-        st.e = (uint32_t)(entry >> 16);
-        st.s = slot ? (uint32_t)(__ldg(ht.dir + slot - 1) >> 16) : 0u;
-        uint32_t c = 0;
-        for (uint32_t j = st.s; j < st.e; ++j) c += (int64_t)ht.tuples[j].key == key;
+    CJ_DEV void range(const Shared &sh, int64_t key, uint32_t &s, uint32_t &n) const {
+        const uint64_t h = hash_key(key);
+        const uint32_t slot = slot_of(h, ht.log2_slots);
+        const uint64_t e = __ldg(ht.dir + slot);
+        const uint32_t tag = sh.bloom[bloom_index(h)];
+        n = 0;
+        s = (uint32_t)(e >> 32);
+        if (((uint32_t)e & tag) != tag) return;
+        n = (uint32_t)(e >> 16) & 0xFFFFu;
+        if (n == 0xFFFFu) n = (uint32_t)(__ldg(ht.dir + slot + 1) >> 32) - s;
+    }
+    CJ_DEV uint32_t count(const Shared &sh, int64_t key, uint32_t &first) const {
+        uint32_t s, n, c = 0;
+        range(sh, key, s, n);
+        for (uint32_t j = 0; j < n; ++j) {
+            const Tuple<KB> t = ht.tuples[s + j];
+            if ((int64_t)t.key == key) {
+                if (!c) first = t.rid;
+                ++c;
+            }
+        }
         return c;
     }
-    CJ_DEV void write(const Shared &, int64_t key, const State &st, unsigned long long pos,
-                      uint32_t probe_row, const MatchOut &out) const {
-        for (uint32_t j = st.s; j < st.e; ++j) {
-            Tuple<KB> t = ht.tuples[j];
+    CJ_DEV void write_all(const Shared &sh, int64_t key, unsigned long long pos, uint32_t prow,
+                          const MatchOut &out) const {
+        uint32_t s, n;
+        range(sh, key, s, n);
+        for (uint32_t j = 0; j < n; ++j) {
+            const Tuple<KB> t = ht.tuples[s + j];
             if ((int64_t)t.key != key) continue;
             if (pos < out.capacity) {
                 if (out.build_rids) out.build_rids[pos] = t.rid;
-                if (out.probe_rids) out.probe_rids[pos] = probe_row;
+                if (out.probe_rids) out.probe_rids[pos] = prow;
             }
             ++pos;
         }
@@ -122,91 +106,104 @@ struct LoopMatcher {
         uint32_t rids[kNestedLoopMax];
         uint32_t n;
     };
-    struct State {};
     CJ_DEV void init(Shared &sh) const {
-        uint32_t n = *g_count;
+        const uint32_t n = *g_count;
         if (threadIdx.x == 0) sh.n = n;
         for (uint32_t b = threadIdx.x; b < n; b += blockDim.x) {
             sh.keys[b] = g_keys[b];
             sh.rids[b] = g_rids[b];
         }
     }
-    CJ_DEV uint32_t count(const Shared &sh, int64_t key, State &) const {
+    CJ_DEV uint32_t count(const Shared &sh, int64_t key, uint32_t &first) const {
         uint32_t c = 0;
-        for (uint32_t b = 0; b < sh.n; ++b) c += sh.keys[b] == key;
+        for (uint32_t b = 0; b < sh.n; ++b)
+            if (sh.keys[b] == key) {
+                if (!c) first = sh.rids[b];
+                ++c;
+            }
         return c;
     }
-    CJ_DEV void write(const Shared &sh, int64_t key, const State &, unsigned long long pos,
-                      uint32_t probe_row, const MatchOut &out) const {
+    CJ_DEV void write_all(const Shared &sh, int64_t key, unsigned long long pos, uint32_t prow,
+                          const MatchOut &out) const {
         for (uint32_t b = 0; b < sh.n; ++b) {
             if (sh.keys[b] != key) continue;
             if (pos < out.capacity) {
                 if (out.build_rids) out.build_rids[pos] = sh.rids[b];
-                if (out.probe_rids) out.probe_rids[pos] = probe_row;
+                if (out.probe_rids) out.probe_rids[pos] = prow;
             }
             ++pos;
         }
     }
 };
 
+/* Per-row state between the counting and the writing pass lives in shared
+ * memory, not registers, so the kernel fits 32 registers (8 CTAs per SM). */
 struct ProbeSmem {
+    uint32_t first[kTileRows]; /* first matching build row (one-match rows) */
+    uint32_t pre[kTileRows];   /* row's match offset within its warp        */
     uint32_t warp[kProbeThreads / 32 + 1];
     uint32_t tile;
     uint32_t task;
     unsigned long long base;
 };
 
-/* One probe tile: count, scan, look back, write. Block-wide. */
+/* One probe tile. Block-wide. */
 template <class M>
 CJ_DEV void probe_tile(const ColView &pkey, uint32_t n, const M &m, const typename M::Shared &sh,
-                       const MatchOut &out, unsigned long long *status, uint32_t num_tiles, uint32_t tile,
-                       unsigned int *err, ProbeSmem &ps) {
+                       const MatchOut &out, uint32_t tile, ProbeSmem &ps) {
     const uint32_t warp = threadIdx.x >> 5, lane = lane_id();
     const uint64_t row0 = (uint64_t)tile * kTileRows + (uint64_t)warp * 32 * kProbeItems;
-    int64_t key[kProbeItems];
-    uint32_t cnt[kProbeItems], pre[kProbeItems];
-    typename M::State st[kProbeItems];
+    uint32_t kinds = 0; /* 2 bits per item: 0 none, 1 one match, 2 more */
     uint32_t wrun = 0;
 #pragma unroll
     for (int it = 0; it < kProbeItems; ++it) {
-        uint64_t i = row0 + (uint64_t)it * 32 + lane;
-        cnt[it] = 0;
-        key[it] = 0;
-        if (i < n && load_key_stream(pkey, (uint32_t)i, &key[it])) cnt[it] = m.count(sh, key[it], st[it]);
-        uint32_t incl = warp_inclusive_scan(cnt[it]);
-        pre[it] = wrun + incl - cnt[it];
+        const uint64_t i = row0 + (uint64_t)it * 32 + lane;
+        const uint32_t si = warp * 32 * kProbeItems + it * 32 + lane;
+        int64_t key;
+        uint32_t c = 0, first = 0;
+        if (i < n && load_key_stream(pkey, (uint32_t)i, &key)) c = m.count(sh, key, first);
+        kinds |= (c == 0 ? 0u : (c == 1 ? 1u : 2u)) << (2 * it);
+        const uint32_t incl = warp_inclusive_scan(c);
+        ps.first[si] = first;
+        ps.pre[si] = wrun + incl - c;
         wrun += __shfl_sync(0xffffffffu, incl, 31);
     }
     if (lane == 0) ps.warp[warp] = wrun;
     __syncthreads();
     if (warp == 0) {
-        uint32_t w = lane < kProbeThreads / 32 ? ps.warp[lane] : 0u;
-        uint32_t wi = warp_inclusive_scan(w);
+        const uint32_t w = lane < kProbeThreads / 32 ? ps.warp[lane] : 0u;
+        const uint32_t wi = warp_inclusive_scan(w);
         if (lane < kProbeThreads / 32) ps.warp[lane] = wi - w;
-        if (lane == 31) ps.warp[kProbeThreads / 32] = wi;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        TileSched ts{nullptr, status, num_tiles};
-        uint32_t agg = ps.warp[kProbeThreads / 32];
-        unsigned long long b = tile_lookback(ts, tile, agg, err);
-        ps.base = b;
-        if (tile == num_tiles - 1) *out.counter = b + agg;
+        if (lane == 31) {
+            ps.base = wi ? atomicAdd(out.counter, (unsigned long long)wi) : 0ull;
+        }
     }
     __syncthreads();
     const unsigned long long base = ps.base + ps.warp[warp];
 #pragma unroll
     for (int it = 0; it < kProbeItems; ++it) {
-        if (!cnt[it]) continue;
-        uint64_t i = row0 + (uint64_t)it * 32 + lane;
-        m.write(sh, key[it], st[it], base + pre[it], (uint32_t)i, out);
+        const uint32_t k = (kinds >> (2 * it)) & 3u;
+        if (!k) continue;
+        const uint32_t prow = (uint32_t)(row0 + (uint64_t)it * 32 + lane);
+        const uint32_t si = warp * 32 * kProbeItems + it * 32 + lane;
+        const unsigned long long pos = base + ps.pre[si];
+        if (k == 1) {
+            if (pos < out.capacity) {
+                if (out.build_rids) out.build_rids[pos] = ps.first[si];
+                if (out.probe_rids) out.probe_rids[pos] = prow;
+            }
+        } else {
+            int64_t key;
+            load_key(pkey, prow, &key);
+            m.write_all(sh, key, pos, prow, out);
+        }
     }
     __syncthreads();
 }
 
 template <class M>
-__global__ void __launch_bounds__(kProbeThreads)
-    k_probe_tiles(ColView pkey, uint32_t n, M m, MatchOut out, TileSched ts, unsigned int *err) {
+__global__ void __launch_bounds__(kProbeThreads, kProbeMinBlocks)
+    k_probe_tiles(ColView pkey, uint32_t n, M m, MatchOut out, TileSched ts) {
     __shared__ typename M::Shared sh;
     __shared__ ProbeSmem ps;
     m.init(sh);
@@ -216,14 +213,12 @@ __global__ void __launch_bounds__(kProbeThreads)
         __syncthreads();
         const uint32_t tile = ps.tile;
         if (tile >= ts.num_tiles) break;
-        probe_tile(pkey, n, m, sh, out, ts.status, ts.num_tiles, tile, err, ps);
+        probe_tile(pkey, n, m, sh, out, tile, ps);
     }
 }
 
 /* Grouped probe: the tiles of every join of a batch level in one
- * persistent launch. Task k owns global tiles [tile_base[k],
- * tile_base[k+1]); tickets are global, so a tile's predecessors in its
- * own join always hold earlier tickets. */
+ * persistent launch; task k owns global tiles [tile_base[k], tile_base[k+1]). */
 struct GroupedShared {
     union {
         HashMatcher<int32_t>::Shared h;
@@ -231,9 +226,9 @@ struct GroupedShared {
     };
 };
 
-__global__ void __launch_bounds__(kProbeThreads)
+__global__ void __launch_bounds__(kProbeThreads, kProbeMinBlocks)
     k_probe_grouped(const ProbeTask *__restrict__ tasks, uint32_t ntasks, uint32_t total_tiles,
-                    unsigned int *ticket, const uint16_t *__restrict__ g_bloom, unsigned int *err) {
+                    unsigned int *ticket, const uint16_t *__restrict__ g_bloom) {
     __shared__ GroupedShared sh;
     __shared__ ProbeSmem ps;
     __shared__ uint32_t loaded_task;
@@ -243,12 +238,11 @@ __global__ void __launch_bounds__(kProbeThreads)
     bool bloom_live = true;
     for (;;) {
         if (threadIdx.x == 0) {
-            uint32_t t = atomicAdd(ticket, 1u);
+            const uint32_t t = atomicAdd(ticket, 1u);
             ps.tile = t;
-            /* task = last k with tile_base[k] <= t */
             uint32_t lo = 0, hi = ntasks;
             while (hi - lo > 1) {
-                uint32_t mid = (lo + hi) >> 1;
+                const uint32_t mid = (lo + hi) >> 1;
                 if (tasks[mid].tile_base <= t) lo = mid;
                 else hi = mid;
             }
@@ -269,7 +263,7 @@ __global__ void __launch_bounds__(kProbeThreads)
                 bloom_live = false;
                 __syncthreads();
             }
-            probe_tile(T.pkey, T.n_probe, m, sh.l, T.out, T.status, T.num_tiles, tile, err, ps);
+            probe_tile(T.pkey, T.n_probe, m, sh.l, T.out, tile, ps);
         } else {
             if (!bloom_live) {
                 __syncthreads();
@@ -281,30 +275,28 @@ __global__ void __launch_bounds__(kProbeThreads)
             if (T.build_key_type == CJ_INT32) {
                 HashMatcher<int32_t> m{{T.dir, reinterpret_cast<const Tuple<int32_t> *>(T.tuples), T.log2_slots},
                                        g_bloom};
-                probe_tile(T.pkey, T.n_probe, m, sh.h, T.out, T.status, T.num_tiles, tile, err, ps);
+                probe_tile(T.pkey, T.n_probe, m, sh.h, T.out, tile, ps);
             } else {
                 HashMatcher<int64_t> m{{T.dir, reinterpret_cast<const Tuple<int64_t> *>(T.tuples), T.log2_slots},
                                        g_bloom};
-                probe_tile(T.pkey, T.n_probe, m,
-                           *reinterpret_cast<const HashMatcher<int64_t>::Shared *>(&sh.h), T.out, T.status,
-                           T.num_tiles, tile, err, ps);
+                probe_tile(T.pkey, T.n_probe, m, *reinterpret_cast<const HashMatcher<int64_t>::Shared *>(&sh.h),
+                           T.out, tile, ps);
             }
         }
     }
 }
 
 /* Compacts the non-NULL build keys (<= 64 rows) in row order. */
-__global__ void k_nl_collect(ColView bkey, uint32_t n, int64_t *keys, uint32_t *rids,
-                             uint32_t *count) {
-    __shared__ uint32_t s_w0;
+CJ_DEV void nl_collect(const ColView &bkey, uint32_t n, int64_t *keys, uint32_t *rids, uint32_t *count,
+                       uint32_t *s_w0) {
     const uint32_t i = threadIdx.x;
     int64_t k = 0;
-    bool v = i < n && load_key(bkey, i, &k);
-    uint32_t ball = __ballot_sync(0xffffffffu, v);
+    const bool v = i < n && load_key(bkey, i, &k);
+    const uint32_t ball = __ballot_sync(0xffffffffu, v);
     uint32_t off = __popc(ball & lanemask_lt());
-    if (threadIdx.x == 31) s_w0 = __popc(ball);
+    if (threadIdx.x == 31) *s_w0 = __popc(ball);
     __syncthreads();
-    if (threadIdx.x >= 32) off += s_w0;
+    if (threadIdx.x >= 32) off += *s_w0;
     if (v) {
         keys[off] = k;
         rids[off] = i;
@@ -312,23 +304,24 @@ __global__ void k_nl_collect(ColView bkey, uint32_t n, int64_t *keys, uint32_t *
     if (threadIdx.x == 63) *count = off + (v ? 1u : 0u);
 }
 
-} // namespace
+__global__ void k_nl_collect(ColView bkey, uint32_t n, int64_t *keys, uint32_t *rids, uint32_t *count) {
+    __shared__ uint32_t s_w0;
+    nl_collect(bkey, n, keys, rids, count, &s_w0);
+}
 
-static size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
-
-size_t probe_sched_bytes(uint32_t n_probe) {
-    uint32_t tiles = (n_probe + kTileRows - 1) / kTileRows;
-    return 256 + align256((size_t)tiles * sizeof(unsigned long long));
+__global__ void k_nl_collect_grouped(const NlCollectTask *__restrict__ tasks) {
+    __shared__ uint32_t s_w0;
+    const NlCollectTask &T = tasks[blockIdx.x];
+    nl_collect(T.bkey, T.n_build, T.keys, T.rids, T.count, &s_w0);
 }
 
 template <class M>
-static cudaError_t run_tiles(const Launch &L, const ColView &pkey, uint32_t n, const M &m,
-                             const MatchOut &out, void *sched_mem) {
+cudaError_t run_tiles(const Launch &L, const ColView &pkey, uint32_t n, const M &m, const MatchOut &out,
+                      void *sched_mem) {
     TileSched ts;
     ts.num_tiles = (n + kTileRows - 1) / kTileRows;
     ts.ticket = reinterpret_cast<unsigned int *>(sched_mem);
-    ts.status = reinterpret_cast<unsigned long long *>(reinterpret_cast<char *>(sched_mem) + 256);
-    cudaError_t e = cudaMemsetAsync(sched_mem, 0, probe_sched_bytes(n), L.stream);
+    cudaError_t e = cudaMemsetAsync(sched_mem, 0, sizeof(unsigned int), L.stream);
     if (e != cudaSuccess) return e;
     e = cudaMemsetAsync(out.counter, 0, sizeof(unsigned long long), L.stream);
     if (e != cudaSuccess) return e;
@@ -338,14 +331,19 @@ static cudaError_t run_tiles(const Launch &L, const ColView &pkey, uint32_t n, c
     if (per_sm < 1) per_sm = 1;
     uint64_t grid = (uint64_t)L.num_sms * per_sm;
     if (grid > ts.num_tiles) grid = ts.num_tiles;
-    k_probe_tiles<M><<<(unsigned)grid, kProbeThreads, 0, L.stream>>>(pkey, n, m, out, ts, L.dev_errors);
+    k_probe_tiles<M><<<(unsigned)grid, kProbeThreads, 0, L.stream>>>(pkey, n, m, out, ts);
     count_launches(1);
     return cudaGetLastError();
 }
 
-cudaError_t launch_probe_tiles_hash(const Launch &L, const ColView &pkey, uint32_t n_probe,
-                                    int32_t build_key_type, const uint64_t *dir,
-                                    const void *tuples, int log2_slots, const uint16_t *bloom,
+} // namespace
+
+size_t probe_sched_bytes(uint32_t) { return 256; }
+
+uint32_t probe_tiles(uint32_t n_probe) { return (n_probe + kTileRows - 1) / kTileRows; }
+
+cudaError_t launch_probe_tiles_hash(const Launch &L, const ColView &pkey, uint32_t n_probe, int32_t build_key_type,
+                                    const uint64_t *dir, const void *tuples, int log2_slots, const uint16_t *bloom,
                                     const MatchOut &out, void *sched_mem) {
     if (build_key_type == CJ_INT32) {
         HashMatcher<int32_t> m{{dir, reinterpret_cast<const Tuple<int32_t> *>(tuples), log2_slots}, bloom};
@@ -355,15 +353,20 @@ cudaError_t launch_probe_tiles_hash(const Launch &L, const ColView &pkey, uint32
     return run_tiles(L, pkey, n_probe, m, out, sched_mem);
 }
 
-cudaError_t launch_nl_collect(const Launch &L, const ColView &bkey, uint32_t n_build,
-                              int64_t *keys, uint32_t *rids, uint32_t *count) {
+cudaError_t launch_nl_collect(const Launch &L, const ColView &bkey, uint32_t n_build, int64_t *keys, uint32_t *rids,
+                              uint32_t *count) {
     if (n_build > kNestedLoopMax) return cudaErrorInvalidValue;
     k_nl_collect<<<1, 64, 0, L.stream>>>(bkey, n_build, keys, rids, count);
     count_launches(1);
     return cudaGetLastError();
 }
 
-uint32_t probe_tiles(uint32_t n_probe) { return (n_probe + kTileRows - 1) / kTileRows; }
+cudaError_t launch_nl_probe_tiles(const Launch &L, const ColView &pkey, uint32_t n_probe, const int64_t *keys,
+                                  const uint32_t *rids, const uint32_t *count, const MatchOut &out,
+                                  void *sched_mem) {
+    LoopMatcher m{keys, rids, count};
+    return run_tiles(L, pkey, n_probe, m, out, sched_mem);
+}
 
 cudaError_t launch_probe_grouped(const Launch &L, const ProbeTask *tasks_dev, uint32_t ntasks, uint32_t total_tiles,
                                  unsigned int *ticket, const uint16_t *bloom) {
@@ -373,28 +376,9 @@ cudaError_t launch_probe_grouped(const Launch &L, const ProbeTask *tasks_dev, ui
     if (per_sm < 1) per_sm = 1;
     uint64_t grid = (uint64_t)L.num_sms * per_sm;
     if (grid > total_tiles) grid = total_tiles;
-    k_probe_grouped<<<(unsigned)grid, kProbeThreads, 0, L.stream>>>(tasks_dev, ntasks, total_tiles, ticket, bloom,
-                                                                       L.dev_errors);
+    k_probe_grouped<<<(unsigned)grid, kProbeThreads, 0, L.stream>>>(tasks_dev, ntasks, total_tiles, ticket, bloom);
     count_launches(1);
     return cudaGetLastError();
-}
-
-__global__ void k_nl_collect_grouped(const NlCollectTask *__restrict__ tasks) {
-    const NlCollectTask &T = tasks[blockIdx.x];
-    __shared__ uint32_t s_w0;
-    const uint32_t i = threadIdx.x;
-    int64_t k = 0;
-    bool v = i < T.n_build && load_key(T.bkey, i, &k);
-    uint32_t ball = __ballot_sync(0xffffffffu, v);
-    uint32_t off = __popc(ball & lanemask_lt());
-    if (threadIdx.x == 31) s_w0 = __popc(ball);
-    __syncthreads();
-    if (threadIdx.x >= 32) off += s_w0;
-    if (v) {
-        T.keys[off] = k;
-        T.rids[off] = i;
-    }
-    if (threadIdx.x == 63) *T.count = off + (v ? 1u : 0u);
 }
 
 cudaError_t launch_nl_collect_grouped(const Launch &L, const NlCollectTask *tasks_dev, uint32_t ntasks) {
@@ -402,13 +386,6 @@ cudaError_t launch_nl_collect_grouped(const Launch &L, const NlCollectTask *task
     k_nl_collect_grouped<<<ntasks, 64, 0, L.stream>>>(tasks_dev);
     count_launches(1);
     return cudaGetLastError();
-}
-
-cudaError_t launch_nl_probe_tiles(const Launch &L, const ColView &pkey, uint32_t n_probe,
-                                  const int64_t *keys, const uint32_t *rids,
-                                  const uint32_t *count, const MatchOut &out, void *sched_mem) {
-    LoopMatcher m{keys, rids, count};
-    return run_tiles(L, pkey, n_probe, m, out, sched_mem);
 }
 
 } // namespace cj

@@ -17,8 +17,7 @@
  * device is current, on the first call on that device (that first call
  * should therefore be made before any stream capture). All calls share the
  * array and it keeps the previous call's contents: the parts that must
- * start at zero (error word, tile tickets and look-back status, match
- * counter) are cleared by every call, and two calls whose work overlaps on
+ * start at zero (error word, tile ticket, match counter) are cleared by every call, and two calls whose work overlaps on
  * the GPU (different streams or threads at the same time) race on it.
  */
 #include <cstring>
@@ -127,7 +126,7 @@ extern "C" int cj_hash_join_noalloc(const int32_t *build_keys, const uint32_t *b
         bp.num_rows = n_build;
         bp.log2_slots = ceil_log2(n_build) > 11 ? ceil_log2(n_build) : 11;
         bp.log2_parts = bp.log2_slots - 11 < 12 ? bp.log2_slots - 11 : 12;
-        const size_t dir_bytes = align256((1ull << bp.log2_slots) * 8);
+        const size_t dir_bytes = align256(cj::build_dir_bytes(bp.log2_slots));
         const size_t tup_off = kDirOff + dir_bytes;
         const size_t build_off = tup_off + align256((size_t)n_build * cj::build_tuple_bytes(4));
         const size_t probe_off = build_off + align256(cj::build_temp_bytes(L, bp, 4));
