@@ -31,6 +31,7 @@ the data path ("scaling": "weak").
 from __future__ import annotations
 
 import argparse
+import gc
 import json
 import os
 import statistics
@@ -55,54 +56,108 @@ def rank_info():
 
 
 class ClockSampler:
-    """nvidia-smi clock / throttle samples during the timed region."""
+    """SM clock and clock-event-reason samples during the timed region.
+
+    NVML is initialised in-process before the warm-up (start()), and a thread
+    polls it every 5 ms; mark() brackets the timed region so only samples
+    taken inside it count. Spawning nvidia-smi at the start of the timed
+    region stalled CUDA host calls for tens of ms while it initialised, so
+    the nvidia-smi line (same fields) is only the fallback when NVML is not
+    importable, and it is started before the warm-up as well."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40), ("sw_thermal_slowdown", 0x20),
+               ("sw_power_cap", 0x4))
 
     def __init__(self, gpu: int):
         self.gpu = gpu
-        self.rows = []
+        self.rows = []  # (time, sm_mhz, max_mhz, set of reasons)
         self.proc = None
+        self.stop_flag = threading.Event()
+        self.thread = None
+        self.source = None
+        self.t0 = self.t1 = None
 
-    def __enter__(self):
+    def _nvml_handle(self):
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        props = torch.cuda.get_device_properties(self.gpu)
         try:
+            return pynvml, pynvml.nvmlDeviceGetHandleByUUID("GPU-" + str(props.uuid))
+        except Exception:
+            bus = f"{props.pci_domain_id:08x}:{props.pci_bus_id:02x}:{props.pci_device_id:02x}.0"
+            return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+
+    def start(self):
+        try:
+            nv, h = self._nvml_handle()
+            mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+
+            def poll():
+                while not self.stop_flag.is_set():
+                    sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                    bits = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                    self.rows.append((time.perf_counter(), float(sm), float(mx),
+                                      {n for n, b in self.REASONS if bits & b}))
+                    self.stop_flag.wait(0.005)
+            self.source = "nvml"
+        except Exception:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.thread = threading.Thread(target=self._read, daemon=True)
-            self.thread.start()
-        except Exception:
-            self.proc = None
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+
+            def poll():
+                names = [n for n, _ in self.REASONS]
+                for line in self.proc.stdout:
+                    r = [x.strip() for x in line.split(",")]
+                    try:
+                        self.rows.append((time.perf_counter(), float(r[1]), float(r[2]),
+                                          {n for k, n in enumerate(names) if r[5 + k].lower() == "active"}))
+                    except (ValueError, IndexError):
+                        pass
+            self.source = "nvidia-smi"
+        self.thread = threading.Thread(target=poll, daemon=True)
+        self.thread.start()
+        deadline = time.time() + 10
+        while not self.rows and time.time() < deadline:
+            time.sleep(0.01)
         return self
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.rows.append([x.strip() for x in line.split(",")])
+    def mark(self, begin: bool):
+        if begin:
+            self.t0 = time.perf_counter()
+        else:
+            self.t1 = time.perf_counter()
 
-    def __exit__(self, *a):
+    def stop(self):
+        self.stop_flag.set()
         if self.proc:
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
             except Exception:
                 self.proc.kill()
+        if self.thread:
             self.thread.join(timeout=2)
 
     def summary(self):
-        if not self.rows:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(r[1]) for r in self.rows if len(r) > 2 and r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in self.rows if len(r) > 2 and r[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        t0, t1 = self.t0 or 0.0, self.t1 or float("inf")
+        inside = [r for r in self.rows if t0 <= r[0] <= t1]
+        rows = inside
+        if not rows and self.rows:  # region shorter than one poll: the samples either side
+            before = [r for r in self.rows if r[0] < t0][-1:]
+            after = [r for r in self.rows if r[0] > t1][:1]
+            rows = before + after
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
         reasons = set()
-        for r in self.rows:
-            for k, n in enumerate(names):
-                if len(r) > 5 + k and r[5 + k].lower() == "active":
-                    reasons.add(n)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": sorted(reasons), "samples": len(self.rows)}
+        for r in rows:
+            reasons |= r[3]
+        return {"sm_mhz": statistics.median(r[1] for r in rows), "sm_max_mhz": max(r[2] for r in rows),
+                "reasons": sorted(reasons), "samples": len(inside), "source": self.source}
 
 
 def measured_peaks():
@@ -132,6 +187,11 @@ def algorithmic_bytes(kernel: str, st: dict, plan_info: dict):
         # probe keys (4 B + 1 validity bit per row), one pass over the hash
         # table (8 B tuples + 8 B directory slots), 2 x 4 B row ids per match
         return npr * (4 + 1 / 8) + nb * 8 + slots * 8 + m * 8
+    if kernel == "probe_array":
+        # probe keys (4 B + validity bit), the direct-mapped table (4 B per
+        # slot; the C2 build keys are a permutation of [0, rows), so slots =
+        # build rows) once, 2 x 4 B row ids per match
+        return npr * (4 + 1 / 8) + nb * 4 + m * 8
     if kernel == "write_pages_int32":
         # per output row: 4 B match row id + 4 B value + validity bit read; page bytes written
         pages = (m + 1983) // 1984
@@ -282,30 +342,45 @@ def run_ours(args):
         res.free()
         return st
 
+    # The workload generator leaves millions of Python objects behind; a
+    # cyclic-GC pass over them in the middle of a step stalls the host for
+    # tens of ms. Collect once and freeze them out of later passes.
+    gc.collect()
+    gc.freeze()
+    clk = ClockSampler(local).start()
+    log(f"clock sampler: {clk.source}")
     log("warm-up")
     for _ in range(args.warmup):
         st = step_device()
     log("timed device steps")
-    ctx.set_option(_lib.CJ_OPT_PROFILE_KERNELS, 1)
-    ctx.profile_reset()
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
     launches = 0
-    with ClockSampler(local) as clk:
-        e0.record(stream)
-        for _ in range(args.steps):
-            st = step_device()
-            launches += st.exec["kernel_launches"]
-        e1.record(stream)
-        torch.cuda.synchronize()
-    ms_total = e0.elapsed_time(e1)
+    clk.mark(True)
+    ev[0].record(stream)
+    for i in range(args.steps):
+        st = step_device()
+        launches += st.exec["kernel_launches"]
+        ev[i + 1].record(stream)
+    torch.cuda.synchronize()
+    clk.mark(False)
+    clk.stop()
+    ms_total = ev[0].elapsed_time(ev[-1])
+    step_ms = [ev[i].elapsed_time(ev[i + 1]) for i in range(args.steps)]
     if dist:
         t = torch.tensor([ms_total], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms_total = float(t.item())
         dist.barrier()
+    # per-kernel times (CUDA events around every launch) from a separate
+    # pass over the same steps, so the headline steps carry no event records
+    ctx.set_option(_lib.CJ_OPT_PROFILE_KERNELS, 1)
+    step_device()
+    ctx.profile_reset()
+    for _ in range(args.steps):
+        step_device()
     prof = ctx.profile()
     ctx.set_option(_lib.CJ_OPT_PROFILE_KERNELS, 0)
     ms_step = ms_total / args.steps
@@ -328,6 +403,7 @@ def run_ours(args):
         res.free()
         h2d, d2h = st_h.exec["h2d_bytes"], st_h.exec["d2h_bytes"]
     e2e_s = statistics.mean(walls)
+    e2e_steps = {"min": min(walls) * 1e3, "median": statistics.median(walls) * 1e3, "max": max(walls) * 1e3}
     if dist:
         t = torch.tensor([e2e_s], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -367,13 +443,14 @@ def run_ours(args):
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+                "step_ms": {"min": min(step_ms), "median": statistics.median(step_ms), "max": max(step_ms)},
                 "config": {"workload": WORKLOAD, "scale": args.scale,
                            "inputs": "paged columns resident in HBM (device-resident cj_table)",
                            "l2": "inputs larger than L2 (1.1 GB of pages); no flush",
                            "parallelism": f"replicas x{world}",
                            "output_rows": st.exec["output_rows"], "output_pages": st.exec["output_pages"]},
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                        "ms_per_step": e2e_s * 1000.0},
+                        "ms_per_step": e2e_s * 1000.0, "step_ms": e2e_steps},
                 "roofline": roof, "cpu_baseline": cpu, "gpu_launches": launches,
                 "clocks": clk.summary(), "kernels": kernels,
                 "phases_us": {k: st.exec[k] for k in ("decode_us", "build_us", "probe_us", "materialize_us")}}

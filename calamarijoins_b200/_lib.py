@@ -32,6 +32,7 @@ CJ_OPT_PROFILE_KERNELS = 2
 CJ_OPT_BLOCK_THREADS = 3
 CJ_OPT_VARCHAR_TILE_ROWS = 4
 CJ_OPT_CTAS_PER_SM = 5
+CJ_OPT_DENSE_KEYS = 6
 
 
 class ColumnDesc(C.Structure):
@@ -74,7 +75,7 @@ class ExecStatsC(C.Structure):
         + [(n, C.c_uint64) for n in (
             "h2d_bytes", "d2h_bytes", "num_joins", "num_hash_joins", "num_nested_loop_joins",
             "probe_rows", "matches", "probe_reruns", "output_rows", "output_pages",
-            "kernel_launches")])
+            "kernel_launches", "num_direct_joins")])
 
 
 class BatchStatsC(C.Structure):

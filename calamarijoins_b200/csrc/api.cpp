@@ -66,6 +66,10 @@ int cj_context_set_option(cj_context *ctx, int32_t option, int64_t value) {
         ctx->opt.varchar_tile_rows = value;
         break;
     case CJ_OPT_CTAS_PER_SM: ctx->opt.ctas_per_sm = value; break;
+    case CJ_OPT_DENSE_KEYS:
+        if (value < 0 || value > 64) return set_error(CJ_ERR_INVALID_ARGUMENT, "dense key factor in [0, 64]");
+        ctx->opt.dense_keys = value;
+        break;
     default: return set_error(CJ_ERR_INVALID_ARGUMENT, "unknown option");
     }
     return CJ_OK;
@@ -80,6 +84,7 @@ int cj_context_get_option(const cj_context *ctx, int32_t option, int64_t *value)
     case CJ_OPT_BLOCK_THREADS: *value = ctx->opt.block_threads; break;
     case CJ_OPT_VARCHAR_TILE_ROWS: *value = ctx->opt.varchar_tile_rows; break;
     case CJ_OPT_CTAS_PER_SM: *value = ctx->opt.ctas_per_sm; break;
+    case CJ_OPT_DENSE_KEYS: *value = ctx->opt.dense_keys; break;
     default: return set_error(CJ_ERR_INVALID_ARGUMENT, "unknown option");
     }
     return CJ_OK;

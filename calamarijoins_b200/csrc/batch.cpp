@@ -207,9 +207,14 @@ void BatchExecutor::run_level(int lvl) {
                 const cj_attr &at = node.output_attrs[a];
                 if (at.index >= lsz + Rr.cols.size()) fail(CJ_ERR_INVALID_PLAN, "output attribute out of range");
                 const Relation *side = at.index < lsz ? &Lr : &Rr;
-                const RelCol &c = side->cols[at.index < lsz ? at.index : at.index - lsz];
+                RelCol c = side->cols[at.index < lsz ? at.index : at.index - lsz];
                 if (c.type != at.type) fail(CJ_ERR_INVALID_PLAN, "output attribute type differs from its column");
-                const bool fb = side == w.B;
+                bool fb = side == w.B;
+                if (key_from_probe_side(fb, c, w.bk, w.pk)) {
+                    fb = false;
+                    side = w.P;
+                    c = w.pk;
+                }
                 w.need_b |= fb;
                 w.need_p |= !fb;
                 w.outs.push_back({fb, side, c});

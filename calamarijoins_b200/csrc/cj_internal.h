@@ -80,6 +80,8 @@ struct ColView {
     const uint32_t *rid_b;
     int32_t type;
     int32_t null_sentinel; /* INT32: INT32_MIN reads as NULL (value_t) */
+    const uint32_t *has_nulls; /* device flag, 0: no row is NULL (validity
+                                  need not be read); null: unknown        */
 };
 
 template <typename K> struct Tuple;
@@ -128,9 +130,11 @@ cudaError_t scan_u32_to_u64(const Launch &L, const uint32_t *in, uint64_t *out,
                             size_t n, void *temp);
 
 /* Decode */
+/* Rows per page; *has_nulls (zeroed by the caller, may be null) becomes 1
+ * if any page holds a NULL (n_values < n_rows). */
 cudaError_t launch_page_rows(const Launch &L, const uint8_t *pages,
                              uint64_t num_pages, int32_t type,
-                             uint32_t *rows_per_page);
+                             uint32_t *rows_per_page, uint32_t *has_nulls);
 /* Rows past max_rows are never written; a page that would write them
  * raises DEV_ERR_ROW_COUNT instead. */
 cudaError_t launch_decode_fixed(const Launch &L, const uint8_t *pages,
@@ -205,6 +209,20 @@ size_t build_grouped_temp_bytes(uint64_t total_cells);
 cudaError_t launch_build_grouped(const Launch &L, const BuildTask *tasks_dev, uint32_t ntasks, uint32_t total_chunks,
                                  uint32_t total_parts, uint64_t total_cells, uint32_t max_parts, uint32_t max_slots,
                                  const uint16_t *bloom, void *temp);
+
+/* Direct-mapped build for unique keys spread densely over [lo, lo + span):
+ * slots[key - lo] = build row. `range` (3 u64, set by the caller to
+ * {~0, 0, 0}) receives the min and max non-NULL key, each XOR 2^63 so that
+ * unsigned order is signed order, and the non-NULL count. The build sets
+ * *dup to 1 if two rows share a key; slots start as kArrayEmpty. */
+constexpr uint32_t kArrayEmpty = 0xFFFFFFFFu;
+cudaError_t launch_key_range(const Launch &L, const ColView &key, uint32_t n, unsigned long long *range);
+cudaError_t launch_array_build(const Launch &L, const ColView &key, uint32_t n, int64_t lo, uint64_t span,
+                               uint32_t *slots, unsigned long long *dup);
+/* Probe of a direct-mapped table; does nothing when *dup is set. */
+cudaError_t launch_probe_tiles_array(const Launch &L, const ColView &pkey, uint32_t n_probe, const uint32_t *slots,
+                                     int64_t lo, uint64_t span, const unsigned long long *dup, const MatchOut &out,
+                                     void *sched);
 
 /* Probe and nested loop share one tiled kernel; `sched` is scratch of
  * probe_sched_bytes(n_probe) bytes (the tile ticket). */

@@ -3,6 +3,7 @@
  * pool, events, status block, page upload.
  */
 #include <cstdlib>
+#include <algorithm>
 #include <cstring>
 #include <memory>
 #include <string>
@@ -139,6 +140,8 @@ void Context::resolve_profile() {
 }
 
 Context::~Context() {
+    if (h2d_stream) cudaStreamSynchronize(h2d_stream);
+    if (d2h_stream) cudaStreamSynchronize(d2h_stream);
     if (stream) cudaStreamSynchronize(stream);
     for (auto &p : pending) {
         cudaEventDestroy(p.a);
@@ -155,6 +158,8 @@ Context::~Context() {
     if (d_bloom) cudaFree(d_bloom);
     if (pool && owns_pool) cudaMemPoolDestroy(pool);
     if (stream) cudaStreamDestroy(stream);
+    if (h2d_stream) cudaStreamDestroy(h2d_stream);
+    if (d2h_stream) cudaStreamDestroy(d2h_stream);
 }
 
 static void make_bloom(uint16_t *out) {
@@ -198,6 +203,8 @@ Context *create_context(int device, cudaMemPool_t shared_pool) {
     c->device = device;
     check_cuda(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device), "attr");
     check_cuda(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "stream");
+    check_cuda(cudaStreamCreateWithFlags(&c->h2d_stream, cudaStreamNonBlocking), "stream");
+    check_cuda(cudaStreamCreateWithFlags(&c->d2h_stream, cudaStreamNonBlocking), "stream");
     if (shared_pool) {
         c->pool = shared_pool;
         c->owns_pool = false;
@@ -222,14 +229,18 @@ Context *create_context(int device, cudaMemPool_t shared_pool) {
     c->opt.block_threads = env_opt("CJ_BLOCK_THREADS", c->opt.block_threads);
     c->opt.varchar_tile_rows = env_opt("CJ_VARCHAR_TILE_ROWS", c->opt.varchar_tile_rows);
     c->opt.ctas_per_sm = env_opt("CJ_CTAS_PER_SM", c->opt.ctas_per_sm);
+    c->opt.dense_keys = std::max<int64_t>(0, std::min<int64_t>(64, env_opt("CJ_DENSE_KEYS", c->opt.dense_keys)));
     return c.release();
 }
 
 /* Host pages -> one consecutive device array. A run of pages that are
  * already consecutive in host memory goes in one cudaMemcpyAsync (full PCIe
  * speed when the memory is page-locked); scattered pages are gathered into
- * one of two pinned staging buffers while the other is in flight. */
-void upload_pages(Context &ctx, const cj_column_desc &cd, ColumnPages &out, uint64_t *h2d_bytes) {
+ * one of two pinned staging buffers while the other is in flight. The
+ * copies go on `stream` (the context's stream when null); the device array
+ * is allocated on the context's stream and `stream` is ordered after that. */
+void upload_pages(Context &ctx, const cj_column_desc &cd, ColumnPages &out, uint64_t *h2d_bytes,
+                  cudaStream_t stream) {
     out.type = cd.type;
     out.num_pages = cd.num_pages;
     if (cd.num_pages == 0) return;
@@ -238,15 +249,21 @@ void upload_pages(Context &ctx, const cj_column_desc &cd, ColumnPages &out, uint
     out.owner = ctx.alloc(cd.num_pages * P);
     uint8_t *dev = out.owner->as<uint8_t>();
     out.dev = dev;
+    const cudaStream_t s = stream ? stream : ctx.stream;
+    if (s != ctx.stream) {
+        cudaEvent_t ready = ctx.get_event();
+        check_cuda(cudaEventRecord(ready, ctx.stream), "event record");
+        check_cuda(cudaStreamWaitEvent(s, ready, 0), "stream wait");
+        ctx.put_event(ready);
+    }
     const uint64_t per_buf = ctx.staging_bytes / P;
     int buf = 0;
     uint64_t fill = 0, fill_first = 0;
     auto flush = [&]() {
         if (!fill) return;
-        check_cuda(cudaMemcpyAsync(dev + fill_first * P, ctx.staging[buf], fill * P, cudaMemcpyHostToDevice,
-                                   ctx.stream),
+        check_cuda(cudaMemcpyAsync(dev + fill_first * P, ctx.staging[buf], fill * P, cudaMemcpyHostToDevice, s),
                    "page upload");
-        check_cuda(cudaEventRecord(ctx.staging_ev[buf], ctx.stream), "event record");
+        check_cuda(cudaEventRecord(ctx.staging_ev[buf], s), "event record");
         buf ^= 1;
         fill = 0;
     };
@@ -260,8 +277,7 @@ void upload_pages(Context &ctx, const cj_column_desc &cd, ColumnPages &out, uint
         const uint64_t run = j - i;
         if (run * P >= (1u << 20)) {
             flush();
-            check_cuda(cudaMemcpyAsync(dev + i * P, p0, run * P, cudaMemcpyHostToDevice, ctx.stream),
-                       "page upload");
+            check_cuda(cudaMemcpyAsync(dev + i * P, p0, run * P, cudaMemcpyHostToDevice, s), "page upload");
         } else {
             for (uint64_t k = i; k < j; ++k) {
                 if (fill == 0) {

@@ -13,7 +13,9 @@
 #include <algorithm>
 #include <chrono>
 #include <cstring>
+#include <functional>
 #include <map>
+#include <set>
 #include <string>
 #include <vector>
 
@@ -30,6 +32,12 @@ class Executor {
   public:
     Executor(Context &c, const cj_plan_desc &p, uint32_t f) : ctx(c), plan(p), flags(f), L(c.launch()) {}
     ~Executor() {
+        /* Pages still being uploaded (an error came first) are freed on the
+         * kernel stream: order those frees after the copies. */
+        for (auto &kv : prefetched) {
+            cudaStreamWaitEvent(ctx.stream, kv.second.done, 0);
+            ctx.put_event(kv.second.done);
+        }
         for (auto &pe : phase_events) {
             ctx.put_event(pe.a);
             ctx.put_event(pe.b);
@@ -95,6 +103,12 @@ class Executor {
     uint32_t flags;
     Launch L;
     std::map<std::pair<uint64_t, uint64_t>, Decoded> decoded;
+    /* Host columns whose pages are on their way on the upload stream. */
+    struct Prefetched {
+        ColumnPages pages;
+        cudaEvent_t done = nullptr;
+    };
+    std::map<std::pair<uint64_t, uint64_t>, Prefetched> prefetched;
     std::vector<PhaseEv> phase_events;
     cj_exec_stats stats{};
 
@@ -103,16 +117,74 @@ class Executor {
     int32_t column_type(uint64_t t, uint64_t c) const { return input_col_type(plan, t, c); }
 
     void validate();
+    void prefetch();
     Decoded &decode(uint64_t t, uint64_t c);
     Relation resolve(uint64_t node, int depth);
     Relation exec_join(uint64_t node, int depth, bool is_root, cj_result **out);
     ColView view(const Relation &R, const RelCol &c, const uint32_t *rid_a);
-    cj_result *materialize(const std::vector<ColView> &cols, const std::vector<int32_t> &types,
+    /* An output column of the root: its relation column and the match row
+     * ids that select its rows (null for a scan root). Decoded on use. */
+    struct OutCol {
+        const Relation *rel;
+        RelCol col;
+        const uint32_t *rid_a;
+    };
+    cj_result *materialize(const std::vector<OutCol> &cols, const std::vector<int32_t> &types,
                            uint64_t rows);
     void ck(cudaError_t e, const char *what) { check_cuda(e, what); }
 };
 
 void Executor::validate() { validate_plan(ctx, plan); }
+
+/* Starts the upload of every host column the plan will decode, on the
+ * context's upload stream, in the order the kernels need them: join keys
+ * bottom-up, then the root's outputs. The kernel stream waits for a
+ * column's copy only when it decodes that column, so later columns (the
+ * payloads) cross PCIe while the joins below the root run. */
+void Executor::prefetch() {
+    using TC = std::pair<uint64_t, uint64_t>;
+    std::vector<TC> order;
+    std::set<TC> seen;
+    auto add = [&](const TC &tc) {
+        if (seen.insert(tc).second) order.push_back(tc);
+    };
+    std::function<std::vector<TC>(uint64_t, int)> cols = [&](uint64_t node, int depth) -> std::vector<TC> {
+        if (depth > (int)plan.num_nodes) fail(CJ_ERR_INVALID_PLAN, "plan has a cycle");
+        const cj_plan_node &n = plan.nodes[node];
+        std::vector<TC> out;
+        if (n.node_type == CJ_NODE_SCAN) {
+            for (uint64_t a = 0; a < n.num_output_attrs; ++a) out.push_back({n.base_table_id, n.output_attrs[a].index});
+            return out;
+        }
+        std::vector<TC> both = cols(n.left, depth + 1);
+        const std::vector<TC> r = cols(n.right, depth + 1);
+        if (n.left_attr < both.size()) add(both[n.left_attr]);
+        if (n.right_attr < r.size()) add(r[n.right_attr]);
+        both.insert(both.end(), r.begin(), r.end());
+        for (uint64_t a = 0; a < n.num_output_attrs; ++a)
+            if (n.output_attrs[a].index < both.size()) out.push_back(both[n.output_attrs[a].index]);
+        return out;
+    };
+    for (const TC &tc : cols(plan.root, 0)) add(tc);
+    cudaEvent_t first = nullptr;
+    for (const TC &tc : order) {
+        if (resident(tc.first)) continue;
+        if (!first) {
+            first = ctx.get_event();
+            ck(cudaEventRecord(first, ctx.h2d_stream), "event record");
+        }
+        Prefetched pf;
+        upload_pages(ctx, plan.inputs[tc.first].columns[tc.second], pf.pages, &stats.h2d_bytes, ctx.h2d_stream);
+        pf.done = ctx.get_event();
+        ck(cudaEventRecord(pf.done, ctx.h2d_stream), "event record");
+        prefetched.emplace(tc, std::move(pf));
+    }
+    if (first) {
+        cudaEvent_t last = ctx.get_event();
+        ck(cudaEventRecord(last, ctx.h2d_stream), "event record");
+        phase_events.push_back({PH_UPLOAD, first, last});
+    }
+}
 
 Decoded &Executor::decode(uint64_t t, uint64_t c) {
     auto key = std::make_pair(t, c);
@@ -122,8 +194,14 @@ Decoded &Executor::decode(uint64_t t, uint64_t c) {
     d.type = column_type(t, c);
     d.rows = table_rows(t);
     if (d.rows > 0xFFFFFFFFull) fail(CJ_ERR_LIMIT, "table exceeds 2^32-1 rows (u32 row ids)");
+    auto pf = prefetched.find(key);
     if (const cj_table *r = resident(t)) {
         d.src = r->cols[c];
+    } else if (pf != prefetched.end()) {
+        d.src = pf->second.pages;
+        ck(cudaStreamWaitEvent(ctx.stream, pf->second.done, 0), "stream wait");
+        ctx.put_event(pf->second.done);
+        prefetched.erase(pf);
     } else {
         PhaseScope ph(*this, PH_UPLOAD);
         upload_pages(ctx, plan.inputs[t].columns[c], d.src, &stats.h2d_bytes);
@@ -133,9 +211,12 @@ Decoded &Executor::decode(uint64_t t, uint64_t c) {
     DevPtr rows_pp = ctx.alloc(std::max<uint64_t>(np, 1) * 4);
     DevPtr row_start = ctx.alloc((np + 1) * 8);
     DevPtr scan_tmp = ctx.alloc(scan_temp_bytes(np));
+    d.has_nulls = ctx.alloc(4);
+    ck(cudaMemsetAsync(d.has_nulls->ptr, 0, 4, ctx.stream), "memset");
     {
         KScope k(*this, "page_rows");
-        ck(launch_page_rows(L, d.src.dev, np, d.type, rows_pp->as<uint32_t>()), "page_rows");
+        ck(launch_page_rows(L, d.src.dev, np, d.type, rows_pp->as<uint32_t>(), d.has_nulls->as<uint32_t>()),
+           "page_rows");
     }
     {
         KScope k(*this, "scan");
@@ -205,9 +286,14 @@ Relation Executor::exec_join(uint64_t node_idx, int depth, bool is_root, cj_resu
         const cj_attr &at = n.output_attrs[a];
         if (at.index >= lsz + Rr.cols.size()) fail(CJ_ERR_INVALID_PLAN, "output attribute out of range");
         const Relation *side = at.index < lsz ? &Lr : &Rr;
-        const RelCol &c = side->cols[at.index < lsz ? at.index : at.index - lsz];
+        RelCol c = side->cols[at.index < lsz ? at.index : at.index - lsz];
         if (c.type != at.type) fail(CJ_ERR_INVALID_PLAN, "output attribute type differs from its column");
         bool fb = side == &B;
+        if (key_from_probe_side(fb, c, bk, pk)) {
+            fb = false;
+            side = &P;
+            c = pk;
+        }
         need_b |= fb;
         need_p |= !fb;
         outs.push_back({fb, side, c});
@@ -222,21 +308,13 @@ Relation Executor::exec_join(uint64_t node_idx, int depth, bool is_root, cj_resu
         const ColView pv = view(P, pk, nullptr);
         const uint64_t nl_max = std::min<int64_t>(std::max<int64_t>(ctx.opt.nested_loop_max_build, 0), kNestedLoopMax);
         const bool nl = B.rows <= nl_max;
-        DevPtr dir, tuples, nlk, nlr, nlc;
+        DevPtr dir, tuples, nlk, nlr, nlc, slots;
         int log2_slots = 0;
-        if (nl) {
-            stats.num_nested_loop_joins++;
-            PhaseScope ph(*this, PH_NL);
-            nlk = ctx.alloc(kNestedLoopMax * 8);
-            nlr = ctx.alloc(kNestedLoopMax * 4);
-            nlc = ctx.alloc(4);
-            KScope k(*this, "nl_collect");
-            ck(launch_nl_collect(L, bv, (uint32_t)B.rows, nlk->as<int64_t>(), nlr->as<uint32_t>(),
-                                 nlc->as<uint32_t>()),
-               "nl_collect");
-        } else {
-            stats.num_hash_joins++;
-            PhaseScope ph(*this, PH_BUILD);
+        bool direct = false; /* direct-mapped table instead of the hash table */
+        int64_t lo = 0;
+        uint64_t span = 0;
+        unsigned long long *d_dup = &ctx.d_status->aux[3];
+        auto build_hash = [&]() {
             BuildPlan bp;
             bp.num_rows = (uint32_t)B.rows;
             bp.log2_slots = std::max(11, ceil_log2(B.rows)); /* hashtable.h:255-264 */
@@ -253,9 +331,56 @@ Relation Executor::exec_join(uint64_t node_idx, int depth, bool is_root, cj_resu
             DevPtr tmp = ctx.alloc(build_temp_bytes(L, bp, kb));
             KScope k(*this, "build");
             ck(launch_build(L, bp, bv, ctx.d_bloom, dir->as<uint64_t>(), tuples->ptr, tmp->ptr), "build");
+        };
+        if (nl) {
+            stats.num_nested_loop_joins++;
+            PhaseScope ph(*this, PH_NL);
+            nlk = ctx.alloc(kNestedLoopMax * 8);
+            nlr = ctx.alloc(kNestedLoopMax * 4);
+            nlc = ctx.alloc(4);
+            KScope k(*this, "nl_collect");
+            ck(launch_nl_collect(L, bv, (uint32_t)B.rows, nlk->as<int64_t>(), nlr->as<uint32_t>(),
+                                 nlc->as<uint32_t>()),
+               "nl_collect");
+        } else {
+            stats.num_hash_joins++;
+            PhaseScope ph(*this, PH_BUILD);
+            if (ctx.opt.dense_keys > 0) {
+                /* Key range of the build side (one host round trip). Unique
+                 * keys spread over at most dense_keys x rows values get a
+                 * direct-mapped table: one random access per probe row
+                 * instead of a directory entry and a tuple. */
+                ck(cudaMemsetAsync(&ctx.d_status->aux[0], 0xFF, 8, ctx.stream), "memset");
+                ck(cudaMemsetAsync(&ctx.d_status->aux[1], 0, 24, ctx.stream), "memset");
+                {
+                    KScope k(*this, "key_range");
+                    ck(launch_key_range(L, bv, (uint32_t)B.rows, &ctx.d_status->aux[0]), "key_range");
+                }
+                ctx.sync_status();
+                const uint64_t cnt = ctx.h_status->aux[2];
+                if (cnt == 0) {
+                    direct = true; /* no non-NULL build key: nothing can match */
+                } else {
+                    lo = (int64_t)(ctx.h_status->aux[0] ^ (1ull << 63));
+                    const int64_t hi = (int64_t)(ctx.h_status->aux[1] ^ (1ull << 63));
+                    const uint64_t width = (uint64_t)hi - (uint64_t)lo; /* span - 1, no overflow */
+                    if (width < 0xFFFFFFFFull && width + 1 <= (uint64_t)ctx.opt.dense_keys * B.rows) {
+                        direct = true;
+                        span = width + 1;
+                    }
+                }
+                if (direct && span) {
+                    slots = ctx.alloc(span * 4);
+                    ck(cudaMemsetAsync(slots->ptr, 0xFF, span * 4, ctx.stream), "memset");
+                    KScope k(*this, "array_build");
+                    ck(launch_array_build(L, bv, (uint32_t)B.rows, lo, span, slots->as<uint32_t>(), d_dup),
+                       "array_build");
+                }
+            }
+            if (!direct) build_hash();
         }
         uint64_t cap = P.rows;
-        for (int attempt = 0; attempt < 2; ++attempt) {
+        for (;;) {
             mb = need_b ? ctx.alloc(cap * 4) : nullptr;
             mp = need_p ? ctx.alloc(cap * 4) : nullptr;
             MatchOut mo;
@@ -271,6 +396,11 @@ Relation Executor::exec_join(uint64_t node_idx, int depth, bool is_root, cj_resu
                     ck(launch_nl_probe_tiles(L, pv, (uint32_t)P.rows, nlk->as<int64_t>(), nlr->as<uint32_t>(),
                                              nlc->as<uint32_t>(), mo, sched->ptr),
                        "nl_probe");
+                } else if (direct) {
+                    KScope k(*this, "probe_array");
+                    ck(launch_probe_tiles_array(L, pv, (uint32_t)P.rows, slots ? slots->as<uint32_t>() : nullptr,
+                                                lo, span, d_dup, mo, sched->ptr),
+                       "probe_array");
                 } else {
                     KScope k(*this, "probe_hash");
                     ck(launch_probe_tiles_hash(L, pv, (uint32_t)P.rows, bk.type, dir->as<uint64_t>(), tuples->ptr,
@@ -279,22 +409,32 @@ Relation Executor::exec_join(uint64_t node_idx, int depth, bool is_root, cj_resu
                 }
             }
             ctx.sync_status();
+            if (direct && ctx.h_status->aux[3]) {
+                /* a key repeats: the direct-mapped table cannot hold the
+                 * build side (the probe did nothing); use the hash table */
+                direct = false;
+                slots.reset();
+                PhaseScope ph(*this, PH_BUILD);
+                build_hash();
+                continue;
+            }
             M = ctx.h_status->counter;
             if (M <= cap || !(need_b || need_p)) break;
             if (M > 0xFFFFFFFFull) fail(CJ_ERR_LIMIT, "join result exceeds 2^32-1 rows");
             stats.probe_reruns++;
             cap = M;
         }
+        if (direct) stats.num_direct_joins++;
     }
     if (M > 0xFFFFFFFFull) fail(CJ_ERR_LIMIT, "join result exceeds 2^32-1 rows");
     stats.matches += M;
 
     if (is_root) {
-        std::vector<ColView> cols;
+        std::vector<OutCol> cols;
         std::vector<int32_t> types;
         for (auto &o : outs) {
             const uint32_t *ra = o.from_build ? (mb ? mb->as<uint32_t>() : nullptr) : (mp ? mp->as<uint32_t>() : nullptr);
-            cols.push_back(view(*o.rel, o.col, ra));
+            cols.push_back({o.rel, o.col, ra});
             types.push_back(o.col.type);
         }
         *out = materialize(cols, types, M);
@@ -336,7 +476,10 @@ Relation Executor::exec_join(uint64_t node_idx, int depth, bool is_root, cj_resu
     return res;
 }
 
-cj_result *Executor::materialize(const std::vector<ColView> &cols, const std::vector<int32_t> &types,
+/* Writes the root's result pages. For a host result each column's pages
+ * go down on the context's download stream as soon as its writer is done,
+ * so the copy of one column overlaps the writing of the next. */
+cj_result *Executor::materialize(const std::vector<OutCol> &cols, const std::vector<int32_t> &types,
                                  uint64_t rows) {
     auto *res = new cj_result;
     std::unique_ptr<cj_result> guard(res);
@@ -346,6 +489,27 @@ cj_result *Executor::materialize(const std::vector<ColView> &cols, const std::ve
     const size_t nc = cols.size();
     res->num_pages.assign(nc, 0);
     res->dev_pages.resize(nc);
+    res->host_cols.assign(nc, nullptr);
+    const bool to_host = !(flags & CJ_EXEC_RESULT_ON_DEVICE);
+    /* Orders the kernel stream (and so every later free) after the copies
+     * issued so far, also when an error leaves this scope early. */
+    struct DownloadJoin {
+        Context &ctx;
+        cudaEvent_t first = nullptr, last = nullptr;
+        bool timed = false; /* events handed to the phase timer */
+        ~DownloadJoin() {
+            if (!first) return;
+            if (!last) {
+                last = ctx.get_event();
+                cudaEventRecord(last, ctx.d2h_stream);
+            }
+            cudaStreamWaitEvent(ctx.stream, last, 0);
+            if (!timed) {
+                ctx.put_event(first);
+                ctx.put_event(last);
+            }
+        }
+    } dl{ctx};
     {
         PhaseScope ph(*this, PH_MAT);
         const uint32_t TR = (uint32_t)std::max<int64_t>(64, std::min<int64_t>(ctx.opt.varchar_tile_rows, 8192));
@@ -360,8 +524,9 @@ cj_result *Executor::materialize(const std::vector<ColView> &cols, const std::ve
             for (size_t c = 0; c < nc; ++c) {
                 if (types[c] != CJ_VARCHAR) continue;
                 vtemp[c] = ctx.alloc(varchar_temp_bytes(rows, TR));
+                const ColView cv = view(*cols[c].rel, cols[c].col, cols[c].rid_a);
                 KScope ks(*this, "varchar_plan");
-                ck(launch_varchar_plan(L, cols[c], rows, TR, vtemp[c]->ptr,
+                ck(launch_varchar_plan(L, cv, rows, TR, vtemp[c]->ptr,
                                        totals->as<unsigned long long>() + k),
                    "varchar_plan");
                 ++k;
@@ -373,39 +538,60 @@ cj_result *Executor::materialize(const std::vector<ColView> &cols, const std::ve
             for (size_t c = 0; c < nc; ++c)
                 if (types[c] == CJ_VARCHAR) res->num_pages[c] = host[k++];
         }
+        uint64_t total_pages = 0;
         for (size_t c = 0; c < nc; ++c) {
-            if (!rows) continue;
-            if (types[c] != CJ_VARCHAR) {
+            if (rows && types[c] != CJ_VARCHAR) {
                 const uint32_t R = rows_per_page_fixed(types[c]);
                 res->num_pages[c] = (rows + R - 1) / R;
-                res->dev_pages[c] = ctx.alloc(res->num_pages[c] * kPageSize);
+            }
+            total_pages += res->num_pages[c];
+        }
+        stats.output_rows = rows;
+        stats.output_pages = total_pages;
+        if (to_host && total_pages) {
+            res->host = ctx.alloc_pinned(total_pages * kPageSize);
+            uint8_t *h = static_cast<uint8_t *>(res->host->ptr);
+            for (size_t c = 0; c < nc; ++c) {
+                res->host_cols[c] = h;
+                h += res->num_pages[c] * kPageSize;
+            }
+        }
+        for (size_t c = 0; c < nc; ++c) {
+            if (!rows) continue;
+            /* decoded here, not before the loop: the kernel stream waits for
+             * a column's upload only when its pages are written */
+            const ColView cv = view(*cols[c].rel, cols[c].col, cols[c].rid_a);
+            res->dev_pages[c] = ctx.alloc(res->num_pages[c] * kPageSize);
+            if (types[c] != CJ_VARCHAR) {
                 KScope ks(*this, types[c] == CJ_INT32 ? "write_pages_int32" : "write_pages_8byte");
-                ck(launch_write_fixed_pages(L, cols[c], rows, res->dev_pages[c]->as<uint8_t>()), "write_fixed");
+                ck(launch_write_fixed_pages(L, cv, rows, res->dev_pages[c]->as<uint8_t>()), "write_fixed");
             } else {
-                res->dev_pages[c] = ctx.alloc(res->num_pages[c] * kPageSize);
                 KScope ks(*this, "varchar_write");
-                ck(launch_varchar_write(L, cols[c], rows, TR, vtemp[c]->ptr, res->dev_pages[c]->as<uint8_t>()),
+                ck(launch_varchar_write(L, cv, rows, TR, vtemp[c]->ptr, res->dev_pages[c]->as<uint8_t>()),
                    "varchar_write");
+            }
+            const size_t bytes = res->num_pages[c] * kPageSize;
+            if (to_host && bytes) {
+                cudaEvent_t written = ctx.get_event();
+                ck(cudaEventRecord(written, ctx.stream), "event record");
+                ck(cudaStreamWaitEvent(ctx.d2h_stream, written, 0), "stream wait");
+                ctx.put_event(written);
+                if (!dl.first) {
+                    dl.first = ctx.get_event();
+                    ck(cudaEventRecord(dl.first, ctx.d2h_stream), "event record");
+                }
+                ck(cudaMemcpyAsync(res->host_cols[c], res->dev_pages[c]->ptr, bytes, cudaMemcpyDeviceToHost,
+                                   ctx.d2h_stream),
+                   "download");
+                stats.d2h_bytes += bytes;
             }
         }
     }
-    uint64_t total_pages = 0;
-    for (size_t c = 0; c < nc; ++c) total_pages += res->num_pages[c];
-    stats.output_rows = rows;
-    stats.output_pages = total_pages;
-    res->host_cols.assign(nc, nullptr);
-    if (!(flags & CJ_EXEC_RESULT_ON_DEVICE) && total_pages) {
-        PhaseScope ph(*this, PH_DOWNLOAD);
-        res->host = ctx.alloc_pinned(total_pages * kPageSize);
-        uint8_t *h = static_cast<uint8_t *>(res->host->ptr);
-        for (size_t c = 0; c < nc; ++c) {
-            res->host_cols[c] = h;
-            const size_t bytes = res->num_pages[c] * kPageSize;
-            if (bytes)
-                ck(cudaMemcpyAsync(h, res->dev_pages[c]->ptr, bytes, cudaMemcpyDeviceToHost, ctx.stream), "download");
-            h += bytes;
-        }
-        stats.d2h_bytes += total_pages * kPageSize;
+    if (dl.first) {
+        dl.last = ctx.get_event();
+        ck(cudaEventRecord(dl.last, ctx.d2h_stream), "event record");
+        phase_events.push_back({PH_DOWNLOAD, dl.first, dl.last});
+        dl.timed = true;
     }
     return guard.release();
 }
@@ -414,6 +600,7 @@ cj_result *Executor::run(cj_exec_stats *st) {
     auto t0 = std::chrono::steady_clock::now();
     const uint64_t launches0 = launches_so_far();
     validate();
+    prefetch();
     cj_result *res = nullptr;
     const cj_plan_node &root = plan.nodes[plan.root];
     if (root.node_type == CJ_NODE_SCAN) {
@@ -421,10 +608,10 @@ cj_result *Executor::run(cj_exec_stats *st) {
          * projected table. */
         Relation s = scan_relation(plan, root);
         if (s.rows > 0xFFFFFFFFull) fail(CJ_ERR_LIMIT, "table exceeds 2^32-1 rows");
-        std::vector<ColView> cols;
+        std::vector<OutCol> cols;
         std::vector<int32_t> types;
         for (auto &c : s.cols) {
-            cols.push_back(view(s, c, nullptr));
+            cols.push_back({&s, c, nullptr});
             types.push_back(c.type);
         }
         res = materialize(cols, types, s.rows);

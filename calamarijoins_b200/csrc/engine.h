@@ -44,6 +44,7 @@ struct Options {
     int64_t block_threads = 0;
     int64_t varchar_tile_rows = 2048;
     int64_t ctas_per_sm = 0;
+    int64_t dense_keys = 2; /* max key span / build rows for a direct-mapped table; 0 = off */
 };
 
 struct Context;
@@ -76,7 +77,9 @@ struct KernelProfile {
 struct Context {
     int device = 0;
     int num_sms = 148;
-    cudaStream_t stream = nullptr;
+    cudaStream_t stream = nullptr;     /* kernels, allocation, frees       */
+    cudaStream_t h2d_stream = nullptr; /* input pages ahead of the kernels */
+    cudaStream_t d2h_stream = nullptr; /* result pages behind the kernels  */
     cudaMemPool_t pool = nullptr;
     bool owns_pool = true;            /* false: pool shared with a server   */
     uint16_t *d_bloom = nullptr;      /* 2048 Bloom tags                  */
@@ -129,7 +132,8 @@ struct ColumnPages {
     DevPtr owner; /* null when the memory is adopted from the caller */
 };
 
-void upload_pages(Context &ctx, const cj_column_desc &cd, ColumnPages &out, uint64_t *h2d_bytes);
+void upload_pages(Context &ctx, const cj_column_desc &cd, ColumnPages &out, uint64_t *h2d_bytes,
+                  cudaStream_t stream = nullptr);
 
 /* Creates a context on `device`; with `shared_pool` non-null the context
  * allocates from that pool instead of creating its own. Throws Error. */

@@ -24,6 +24,7 @@ struct Decoded {
     uint64_t rows = 0;
     ColumnPages src;
     DevPtr values, valid, desc;
+    DevPtr has_nulls; /* u32 flag from the page headers; null: not computed */
 };
 
 /* A column of a relation: base column (input, col) reached through row-id
@@ -35,6 +36,20 @@ struct RelCol {
     int vec;
     bool sentinel; /* value left a non-root join: INT32_MIN reads as NULL */
 };
+
+inline bool same_column(const RelCol &a, const RelCol &b) {
+    return a.input == b.input && a.col == b.col && a.vec == b.vec;
+}
+
+/* On every output row of an equi-join the build key equals the probe key.
+ * When both keys have one type, an output of the build key is read through
+ * the probe side instead: its row ids run in probe order, the build side's
+ * are random, and a join whose build side contributes nothing else needs no
+ * build row ids at all. (NULL and, after a non-root join, INT32_MIN never
+ * match, so the two columns agree on every output row, NULL flags too.) */
+inline bool key_from_probe_side(bool from_build, const RelCol &c, const RelCol &bk, const RelCol &pk) {
+    return from_build && same_column(c, bk) && bk.type == pk.type;
+}
 
 /* A scan (rows are base rows) or a join output (late-materialised: one
  * u32 row-id vector per contributing base table). */
@@ -78,6 +93,7 @@ inline ColView make_view(const Decoded &d, const Relation &R, const RelCol &c, c
     v.rid_a = rid_a;
     v.rid_b = c.vec >= 0 ? R.vecs[c.vec]->as<uint32_t>() : nullptr;
     v.null_sentinel = (c.sentinel && c.type == CJ_INT32) ? 1 : 0;
+    v.has_nulls = d.has_nulls ? d.has_nulls->as<uint32_t>() : nullptr;
     return v;
 }
 

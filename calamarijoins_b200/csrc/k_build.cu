@@ -329,6 +329,68 @@ cudaError_t build_impl(const Launch &L, const BuildPlan &bp, const ColView &key,
     return cudaGetLastError();
 }
 
+/* ---- direct-mapped table (unique keys over a dense range) ---- */
+CJ_DEV unsigned long long warp_min_u64(unsigned long long v) {
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) v = min(v, __shfl_xor_sync(0xffffffffu, v, d));
+    return v;
+}
+CJ_DEV unsigned long long warp_max_u64(unsigned long long v) {
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, d));
+    return v;
+}
+
+__global__ void __launch_bounds__(kBuildThreads)
+    k_key_range(ColView key, uint32_t n, unsigned long long *range) {
+    __shared__ unsigned long long s_min[kBuildThreads / 32], s_max[kBuildThreads / 32];
+    __shared__ unsigned int s_cnt[kBuildThreads / 32];
+    unsigned long long mn = ~0ull, mx = 0ull;
+    unsigned int cnt = 0;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        int64_t k;
+        if (load_key(key, (uint32_t)i, &k)) {
+            const unsigned long long b = (unsigned long long)k ^ (1ull << 63);
+            mn = min(mn, b);
+            mx = max(mx, b);
+            ++cnt;
+        }
+    }
+    mn = warp_min_u64(mn);
+    mx = warp_max_u64(mx);
+    cnt = __reduce_add_sync(0xffffffffu, cnt);
+    const uint32_t warp = threadIdx.x >> 5;
+    if (lane_id() == 0) {
+        s_min[warp] = mn;
+        s_max[warp] = mx;
+        s_cnt[warp] = cnt;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < kBuildThreads / 32; ++w) {
+            mn = min(mn, s_min[w]);
+            mx = max(mx, s_max[w]);
+            cnt += s_cnt[w];
+        }
+        if (cnt) {
+            atomicMin(range, mn);
+            atomicMax(range + 1, mx);
+            atomicAdd(range + 2, (unsigned long long)cnt);
+        }
+    }
+}
+
+__global__ void k_array_build(ColView key, uint32_t n, int64_t lo, uint64_t span, uint32_t *__restrict__ slots,
+                              unsigned long long *dup) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        int64_t k;
+        if (!load_key(key, (uint32_t)i, &k)) continue;
+        const uint64_t off = (uint64_t)k - (uint64_t)lo;
+        if (off >= span) continue; /* cannot happen when lo/span come from k_key_range */
+        if (atomicCAS(slots + off, kArrayEmpty, (uint32_t)i) != kArrayEmpty) *dup = 1ull;
+    }
+}
+
 bool g_attrs_set = false;
 void set_smem_attrs() {
     if (g_attrs_set) return;
@@ -393,6 +455,25 @@ cudaError_t launch_build_grouped(const Launch &L, const BuildTask *tasks_dev, ui
 
 size_t build_grouped_temp_bytes(uint64_t total_cells) {
     return align256(total_cells * 4) + align256((total_cells + 1) * 8) + scan_temp_bytes(total_cells) + 256;
+}
+
+cudaError_t launch_key_range(const Launch &L, const ColView &key, uint32_t n, unsigned long long *range) {
+    if (n == 0) return cudaSuccess;
+    uint64_t g = ((uint64_t)n + kBuildThreads * 8 - 1) / (kBuildThreads * 8);
+    g = std::min<uint64_t>(std::max<uint64_t>(g, 1), (uint64_t)L.num_sms * 8);
+    k_key_range<<<(unsigned)g, kBuildThreads, 0, L.stream>>>(key, n, range);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_array_build(const Launch &L, const ColView &key, uint32_t n, int64_t lo, uint64_t span,
+                               uint32_t *slots, unsigned long long *dup) {
+    if (n == 0 || span == 0) return cudaSuccess;
+    uint64_t g = ((uint64_t)n + 255) / 256;
+    g = std::min<uint64_t>(g, (uint64_t)L.num_sms * 8);
+    k_array_build<<<(unsigned)g, 256, 0, L.stream>>>(key, n, lo, span, slots, dup);
+    count_launches(1);
+    return cudaGetLastError();
 }
 
 size_t build_tuple_bytes(int key_bytes) {

@@ -53,11 +53,23 @@ CJ_DEV uint32_t page_rows_of(const uint8_t *pg, int32_t type, unsigned int *err)
     return r;
 }
 
+/* True if a regular page stores fewer values than rows (some row is
+ * NULL); long-string pages hold one non-NULL row or none. */
+CJ_DEV bool page_has_nulls(const uint8_t *pg, int32_t type) {
+    const uint32_t nr = rd16(pg), nv = rd16(pg + 2);
+    if (type == CJ_VARCHAR && nr >= 0xfffe) return false;
+    return nv < nr;
+}
+
 __global__ void k_page_rows(const uint8_t *__restrict__ pages, uint64_t np, int32_t type,
-                            uint32_t *__restrict__ rows, unsigned int *err) {
+                            uint32_t *__restrict__ rows, uint32_t *has_nulls, unsigned int *err) {
+    bool nulls = false;
     for (uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; p < np;
-         p += (uint64_t)gridDim.x * blockDim.x)
+         p += (uint64_t)gridDim.x * blockDim.x) {
         rows[p] = page_rows_of(pages + p * kPageSize, type, err);
+        nulls |= page_has_nulls(pages + p * kPageSize, type);
+    }
+    if (__any_sync(0xffffffffu, nulls) && lane_id() == 0 && has_nulls) *has_nulls = 1u;
 }
 
 /* Loads a sparse page's bitmap into s_bm (bits past n_rows cleared) and the
@@ -158,16 +170,28 @@ CJ_DEV void decode_fixed_page(const uint8_t *__restrict__ pages, uint64_t p, uin
     const T *vals = reinterpret_cast<const T *>(pg + DB);
     const bool dense = nr == nv;
     if (!dense) load_page_bitmap(pg, nr, sm.bm, sm.pre, sm.wbuf);
-    for (uint32_t i = threadIdx.x; i < nr; i += blockDim.x) {
-        T v = T(0);
-        if (dense) {
-            v = __ldcs(vals + i);
-        } else {
-            int idx = value_index(sm.bm, sm.pre, i);
-            if (idx >= (int)nv) atomicOr(err, DEV_ERR_PAGE_HEADER); /* bitmap holds > n_values bits */
-            else if (idx >= 0) v = __ldcs(vals + idx);
+    /* All loads of a chunk are issued before any store: a full page (1984 /
+     * 1007 rows) is one chunk, so it costs one DRAM round trip. Only a
+     * sparse page with more rows than that takes several. */
+    constexpr int kSlabs =
+        (int)(((sizeof(T) == 4 ? kRowsPerPageInt32 : kRowsPerPage8B) + kDecodeThreads - 1) / kDecodeThreads);
+    for (uint32_t base = 0; base < nr; base += kSlabs * kDecodeThreads) {
+        T v[kSlabs];
+#pragma unroll
+        for (int k = 0; k < kSlabs; ++k) {
+            const uint32_t i = base + k * kDecodeThreads + threadIdx.x;
+            v[k] = T(0);
+            if (i < nr) {
+                const int idx = dense ? (int)i : value_index(sm.bm, sm.pre, i);
+                if (idx >= (int)nv) atomicOr(err, DEV_ERR_PAGE_HEADER); /* bitmap holds > n_values bits */
+                else if (idx >= 0) v[k] = __ldcs(vals + idx);
+            }
         }
-        values[rs + i] = v;
+#pragma unroll
+        for (int k = 0; k < kSlabs; ++k) {
+            const uint32_t i = base + k * kDecodeThreads + threadIdx.x;
+            if (i < nr) values[rs + i] = v[k];
+        }
     }
     write_validity(dense, sm.bm, nr, rs, valid);
     __syncthreads();
@@ -230,7 +254,7 @@ CJ_DEV void decode_varchar_page(const uint8_t *__restrict__ pages, uint64_t p, u
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kDecodeThreads)
+__global__ void __launch_bounds__(kDecodeThreads, 8)
     k_decode_fixed(const uint8_t *__restrict__ pages, uint64_t np, const uint64_t *__restrict__ row_start,
                    uint64_t max_rows, T *__restrict__ values, uint32_t *__restrict__ valid, unsigned int *err) {
     __shared__ DecodeSmem sm;
@@ -310,11 +334,11 @@ unsigned grid_for(const Launch &L, uint64_t units, int per_sm) {
 } // namespace
 
 cudaError_t launch_page_rows(const Launch &L, const uint8_t *pages, uint64_t np, int32_t type,
-                             uint32_t *rows) {
+                             uint32_t *rows, uint32_t *has_nulls) {
     if (np == 0) return cudaSuccess;
     unsigned g = (unsigned)((np + 255) / 256);
     if (g > (unsigned)L.num_sms * 8) g = L.num_sms * 8;
-    k_page_rows<<<g, 256, 0, L.stream>>>(pages, np, type, rows, L.dev_errors);
+    k_page_rows<<<g, 256, 0, L.stream>>>(pages, np, type, rows, has_nulls, L.dev_errors);
     count_launches(1);
     return cudaGetLastError();
 }
@@ -323,7 +347,7 @@ cudaError_t launch_decode_fixed(const Launch &L, const uint8_t *pages, uint64_t 
                                 const uint64_t *row_start, uint64_t max_rows, void *values,
                                 uint32_t *valid) {
     if (np == 0) return cudaSuccess;
-    unsigned g = grid_for(L, np, 6);
+    unsigned g = grid_for(L, np, 8); /* 32 registers, 16 KB shared: 8 CTAs per SM */
     if (type == CJ_INT32) {
         k_decode_fixed<int32_t><<<g, kDecodeThreads, 0, L.stream>>>(
             pages, np, row_start, max_rows, reinterpret_cast<int32_t *>(values), valid, L.dev_errors);

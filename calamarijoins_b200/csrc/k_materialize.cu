@@ -12,9 +12,10 @@
  * Fixed-width pages (k_write_fixed): output page p holds rows
  * [p*R, p*R+R) with R = 1984 (INT32) or 1007 (INT64 / FP64), the fill of
  * ColumnInserter<T> (plan.h:241-250), so every page fits whatever the NULL
- * pattern. One CTA builds one page in shared memory: values compacted by a
- * ballot/scan over the validity bits, bitmap at the page end, header
- * (n_rows, n_values), gap zeroed; then 16-byte stores write the page out.
+ * pattern. One CTA builds one page in shared memory: all of the page's
+ * loads issued at once, values compacted by one ballot/scan over the
+ * validity bits, bitmap at the page end, header (n_rows, n_values), gap
+ * zeroed; then 16-byte streaming stores write the page out.
  *
  * VARCHAR pages (k_varchar_plan / k_varchar_write): rows are cut into tiles;
  * within a tile pages are packed greedily in row order like
@@ -56,74 +57,122 @@ CJ_DEV void scan_warp_counts(uint32_t *s_warp) {
     }
 }
 
+constexpr int kMatMinBlocks = 8; /* page writers: 8 x 256 threads per SM */
+
 struct PageSmem {
-    uint4 page[kPageSize / 16];
-    uint32_t warp[kMatThreads / 32 + 1];
+    uint4 page[kPageSize / 16]; /* zero between pages: copy-out clears it */
+    uint32_t cnt[64];           /* non-NULL rows per (slab, warp), then offsets */
+    uint32_t total;
 };
 
 /* Builds output page `pg` (rows [pg*R, pg*R+R)) of a fixed-width column in
- * shared memory and stores it. Block-wide. */
+ * shared memory and stores it. Block-wide; sm.page must be zero on entry and
+ * is zero again on return.
+ *
+ * Thread t takes rows t, t+256, ... of the page (kSlabs of them) and issues
+ * all their loads (row ids, then validity words and values) before using
+ * any, so a page costs one dependent round trip, not one per 256 rows. One
+ * scan over the (slab, warp) counts then places the non-NULL values. */
 template <typename T>
 CJ_DEV void write_fixed_page(const ColView &col, uint64_t rows, uint32_t R, uint64_t pg, uint8_t *__restrict__ out,
                              PageSmem &sm) {
     constexpr uint32_t DB = sizeof(T) == 4 ? 4u : 8u;
+    constexpr int kSlabs = (int)(((sizeof(T) == 4 ? kRowsPerPageInt32 : kRowsPerPage8B) + kMatThreads - 1) / kMatThreads);
+    constexpr int kWarps = kMatThreads / 32;
+    static_assert(kSlabs * kWarps <= 64, "cnt holds 64 (slab, warp) counts");
     uint8_t *sp = reinterpret_cast<uint8_t *>(sm.page);
     const uint32_t warp = threadIdx.x >> 5, lane = lane_id();
-    for (uint32_t k = threadIdx.x; k < kPageSize / 16; k += blockDim.x) sm.page[k] = make_uint4(0, 0, 0, 0);
-    __syncthreads();
     const uint64_t r0 = pg * R;
     const uint32_t nr = (uint32_t)min((uint64_t)R, rows - r0);
+
+    uint32_t br[kSlabs];
+#pragma unroll
+    for (int k = 0; k < kSlabs; ++k) {
+        const uint32_t r = k * kMatThreads + threadIdx.x;
+        br[k] = 0xffffffffu;
+        if (r < nr) br[k] = col.rid_a ? __ldcs(col.rid_a + r0 + r) : (uint32_t)(r0 + r);
+    }
+    if (col.rid_b) {
+#pragma unroll
+        for (int k = 0; k < kSlabs; ++k)
+            if (br[k] != 0xffffffffu) br[k] = __ldg(col.rid_b + br[k]);
+    }
+    T val[kSlabs];
+    uint32_t vm = 0; /* bit k: row of slab k is non-NULL */
+    /* a column without NULLs needs no validity loads (one random load per
+     * row instead of two when the row ids are random) */
+    const bool all_valid = col.has_nulls && __ldg(col.has_nulls) == 0u;
+#pragma unroll
+    for (int k = 0; k < kSlabs; ++k) {
+        val[k] = T(0);
+        if (br[k] != 0xffffffffu) {
+            const bool v = all_valid || valid_bit(col.valid, br[k]);
+            val[k] = __ldg(reinterpret_cast<const T *>(col.values) + br[k]);
+            if (v && !(sizeof(T) == 4 && col.null_sentinel && (int32_t)val[k] == INT32_MIN)) vm |= 1u << k;
+        }
+    }
+
     const uint32_t bm_bytes = (nr + 7) / 8;
     uint8_t *bm = sp + kPageSize - bm_bytes;
-    T *vals = reinterpret_cast<T *>(sp + DB);
-    uint32_t running = 0;
-    for (uint32_t slab = 0; slab * kMatThreads < nr; ++slab) {
-        const uint32_t r = slab * kMatThreads + threadIdx.x;
-        bool v = false;
-        T val = T(0);
-        if (r < nr) {
-            uint32_t br = base_row(col, (uint32_t)(r0 + r));
-            v = valid_bit(col.valid, br);
-            if (v) {
-                val = __ldg(reinterpret_cast<const T *>(col.values) + br);
-                if (sizeof(T) == 4 && col.null_sentinel && (int32_t)val == INT32_MIN) v = false;
-            }
-        }
-        uint32_t ball = __ballot_sync(0xffffffffu, v);
-        if (lane == 0) sm.warp[warp] = __popc(ball);
-        __syncthreads();
-        scan_warp_counts(sm.warp);
-        __syncthreads();
-        if (v) vals[running + sm.warp[warp] + __popc(ball & lanemask_lt())] = val;
+#pragma unroll
+    for (int k = 0; k < kSlabs; ++k) {
+        const uint32_t ball = __ballot_sync(0xffffffffu, (vm >> k) & 1u);
+        if (lane == 0) sm.cnt[k * kWarps + warp] = __popc(ball);
         if (lane < 4) {
-            uint32_t byte = (slab * kMatThreads + warp * 32) / 8 + lane;
+            const uint32_t byte = (k * kMatThreads + warp * 32) / 8 + lane;
             if (byte < bm_bytes) bm[byte] = (uint8_t)(ball >> (8 * lane));
         }
-        running += sm.warp[kMatThreads / 32];
-        __syncthreads();
+    }
+    __syncthreads();
+    if (warp == 0) {
+        const uint32_t i0 = 2 * lane, i1 = 2 * lane + 1, n = kSlabs * kWarps;
+        const uint32_t a = i0 < n ? sm.cnt[i0] : 0u, b = i1 < n ? sm.cnt[i1] : 0u;
+        const uint32_t incl = warp_inclusive_scan(a + b);
+        if (i0 < n) sm.cnt[i0] = incl - a - b;
+        if (i1 < n) sm.cnt[i1] = incl - b;
+        if (lane == 31) sm.total = incl;
+    }
+    __syncthreads();
+    T *vals = reinterpret_cast<T *>(sp + DB);
+    const uint32_t lt = lanemask_lt();
+#pragma unroll
+    for (int k = 0; k < kSlabs; ++k) {
+        const uint32_t ball = __ballot_sync(0xffffffffu, (vm >> k) & 1u);
+        if ((vm >> k) & 1u) vals[sm.cnt[k * kWarps + warp] + __popc(ball & lt)] = val[k];
     }
     if (threadIdx.x == 0) {
         reinterpret_cast<uint16_t *>(sp)[0] = (uint16_t)nr;
-        reinterpret_cast<uint16_t *>(sp)[1] = (uint16_t)running;
+        reinterpret_cast<uint16_t *>(sp)[1] = (uint16_t)sm.total;
     }
     __syncthreads();
     uint4 *dst = reinterpret_cast<uint4 *>(out + pg * kPageSize);
-    for (uint32_t k = threadIdx.x; k < kPageSize / 16; k += blockDim.x) dst[k] = sm.page[k];
+    const uint4 zero = make_uint4(0, 0, 0, 0);
+    for (uint32_t k = threadIdx.x; k < kPageSize / 16; k += blockDim.x) {
+        __stcs(dst + k, sm.page[k]);
+        sm.page[k] = zero;
+    }
+    __syncthreads();
+}
+
+CJ_DEV void zero_page(PageSmem &sm) {
+    for (uint32_t k = threadIdx.x; k < kPageSize / 16; k += blockDim.x) sm.page[k] = make_uint4(0, 0, 0, 0);
     __syncthreads();
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kMatThreads)
+__global__ void __launch_bounds__(kMatThreads, kMatMinBlocks)
     k_write_fixed(ColView col, uint64_t rows, uint32_t R, uint64_t num_pages, uint8_t *__restrict__ out) {
     __shared__ PageSmem sm;
+    zero_page(sm);
     for (uint64_t pg = blockIdx.x; pg < num_pages; pg += gridDim.x) write_fixed_page<T>(col, rows, R, pg, out, sm);
 }
 
 /* Grouped page writer: every fixed-width output column of a batch. */
-__global__ void __launch_bounds__(kMatThreads)
+__global__ void __launch_bounds__(kMatThreads, kMatMinBlocks)
     k_write_fixed_grouped(const PageTask *__restrict__ tasks, uint32_t ntasks, uint64_t total_pages) {
     __shared__ PageSmem sm;
     __shared__ uint32_t s_task;
+    zero_page(sm);
     for (uint64_t gp = blockIdx.x; gp < total_pages; gp += gridDim.x) {
         if (threadIdx.x == 0) {
             uint32_t lo = 0, hi = ntasks;
@@ -193,9 +242,10 @@ CJ_DEV VarSmem carve(uint8_t *base, uint32_t TR) {
  * segment count; the page count is in s.segpg[nseg]. Block-wide. */
 CJ_DEV uint32_t plan_tile(const ColView &col, uint64_t r0, uint32_t nt, uint32_t TR,
                           const VarSmem &s, uint32_t *wbuf, uint32_t *s_nseg) {
+    const bool all_valid = col.has_nulls && __ldg(col.has_nulls) == 0u;
     for (uint32_t r = threadIdx.x; r < nt; r += blockDim.x) {
         uint32_t br = base_row(col, (uint32_t)(r0 + r));
-        s.desc[r] = valid_bit(col.valid, br) ? __ldg(col.str_desc + br) : 0ull;
+        s.desc[r] = (all_valid || valid_bit(col.valid, br)) ? __ldg(col.str_desc + br) : 0ull;
     }
     __syncthreads();
     const uint32_t per = (TR + blockDim.x - 1) / blockDim.x;
@@ -396,7 +446,7 @@ cudaError_t launch_gather_u32(const Launch &L, const uint32_t *src, const uint32
 cudaError_t launch_write_fixed_grouped(const Launch &L, const PageTask *tasks_dev, uint32_t ntasks,
                                       uint64_t total_pages) {
     if (!total_pages) return cudaSuccess;
-    uint64_t g = std::min<uint64_t>(total_pages, (uint64_t)L.num_sms * 6);
+    uint64_t g = std::min<uint64_t>(total_pages, (uint64_t)L.num_sms * kMatMinBlocks);
     k_write_fixed_grouped<<<(unsigned)g, kMatThreads, 0, L.stream>>>(tasks_dev, ntasks, total_pages);
     count_launches(1);
     return cudaGetLastError();
@@ -420,7 +470,7 @@ cudaError_t launch_write_fixed_pages(const Launch &L, const ColView &col, uint64
     if (rows == 0) return cudaSuccess;
     const uint32_t R = rows_per_page_fixed(col.type);
     const uint64_t np = (rows + R - 1) / R;
-    uint64_t g = np, cap = (uint64_t)L.num_sms * 6;
+    uint64_t g = np, cap = (uint64_t)L.num_sms * kMatMinBlocks;
     if (g > cap) g = cap;
     if (col.type == CJ_INT32) {
         k_write_fixed<int32_t><<<(unsigned)g, kMatThreads, 0, L.stream>>>(col, rows, R, np, out);

@@ -57,6 +57,7 @@ template <typename KB> struct HashMatcher {
     struct Shared {
         uint16_t bloom[2048];
     };
+    CJ_DEV bool skip() const { return false; }
     CJ_DEV void init(Shared &sh) const { load_bloom(sh.bloom, g_bloom); }
     CJ_DEV void range(const Shared &sh, int64_t key, uint32_t &s, uint32_t &n) const {
         const uint64_t h = hash_key(key);
@@ -97,6 +98,38 @@ template <typename KB> struct HashMatcher {
     }
 };
 
+/* Direct-mapped table: slots[key - lo] holds the build row of `key`, or
+ * kArrayEmpty. Unique build keys only: a duplicate found while building
+ * sets *dup, and a probe launched over such a table does nothing (the
+ * caller then builds the hash table instead). */
+struct ArrayMatcher {
+    const uint32_t *slots;
+    int64_t lo;
+    uint64_t span;
+    const unsigned long long *dup;
+    struct Shared {
+        uint32_t unused;
+    };
+    CJ_DEV bool skip() const { return *dup != 0ull; }
+    CJ_DEV void init(Shared &) const {}
+    CJ_DEV uint32_t count(const Shared &, int64_t key, uint32_t &first) const {
+        const uint64_t off = (uint64_t)key - (uint64_t)lo; /* keys below lo wrap past span */
+        if (off >= span) return 0;
+        const uint32_t r = __ldg(slots + off);
+        if (r == kArrayEmpty) return 0;
+        first = r;
+        return 1;
+    }
+    CJ_DEV void write_all(const Shared &sh, int64_t key, unsigned long long pos, uint32_t prow,
+                          const MatchOut &out) const {
+        uint32_t r;
+        if (count(sh, key, r) && pos < out.capacity) {
+            if (out.build_rids) out.build_rids[pos] = r;
+            if (out.probe_rids) out.probe_rids[pos] = prow;
+        }
+    }
+};
+
 struct LoopMatcher {
     const int64_t *g_keys;
     const uint32_t *g_rids;
@@ -106,6 +139,7 @@ struct LoopMatcher {
         uint32_t rids[kNestedLoopMax];
         uint32_t n;
     };
+    CJ_DEV bool skip() const { return false; }
     CJ_DEV void init(Shared &sh) const {
         const uint32_t n = *g_count;
         if (threadIdx.x == 0) sh.n = n;
@@ -206,6 +240,7 @@ __global__ void __launch_bounds__(kProbeThreads, kProbeMinBlocks)
     k_probe_tiles(ColView pkey, uint32_t n, M m, MatchOut out, TileSched ts) {
     __shared__ typename M::Shared sh;
     __shared__ ProbeSmem ps;
+    if (m.skip()) return;
     m.init(sh);
     __syncthreads();
     for (;;) {
@@ -350,6 +385,13 @@ cudaError_t launch_probe_tiles_hash(const Launch &L, const ColView &pkey, uint32
         return run_tiles(L, pkey, n_probe, m, out, sched_mem);
     }
     HashMatcher<int64_t> m{{dir, reinterpret_cast<const Tuple<int64_t> *>(tuples), log2_slots}, bloom};
+    return run_tiles(L, pkey, n_probe, m, out, sched_mem);
+}
+
+cudaError_t launch_probe_tiles_array(const Launch &L, const ColView &pkey, uint32_t n_probe, const uint32_t *slots,
+                                     int64_t lo, uint64_t span, const unsigned long long *dup, const MatchOut &out,
+                                     void *sched_mem) {
+    ArrayMatcher m{slots, lo, span, dup};
     return run_tiles(L, pkey, n_probe, m, out, sched_mem);
 }
 

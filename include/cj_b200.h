@@ -163,6 +163,8 @@ typedef struct cj_exec_stats {
     uint64_t output_rows;
     uint64_t output_pages;
     uint64_t kernel_launches;
+    uint64_t num_direct_joins; /* hash joins served by a direct-mapped table
+                                  (CJ_OPT_DENSE_KEYS); within num_hash_joins */
 } cj_exec_stats;
 
 /* ------------------------------------------------------------------------ */
@@ -190,8 +192,14 @@ typedef enum cj_option {
     CJ_OPT_BLOCK_THREADS = 3,         /* threads per CTA of streaming kernels;
                                          0 = auto                           */
     CJ_OPT_VARCHAR_TILE_ROWS = 4,     /* rows per VARCHAR page-packing tile  */
-    CJ_OPT_CTAS_PER_SM = 5            /* resident CTAs per SM for persistent
+    CJ_OPT_CTAS_PER_SM = 5,           /* resident CTAs per SM for persistent
                                          grids; 0 = auto                    */
+    CJ_OPT_DENSE_KEYS = 6             /* a build side whose non-NULL keys are
+                                         unique and span at most this many
+                                         times its row count uses a direct-
+                                         mapped table (slot = key - min)
+                                         instead of the hash table; same
+                                         results; 0 = off; default 2        */
 } cj_option;
 int cj_context_set_option(cj_context *ctx, int32_t option, int64_t value);
 int cj_context_get_option(const cj_context *ctx, int32_t option, int64_t *value);

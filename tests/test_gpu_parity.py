@@ -158,6 +158,121 @@ def test_int32_min_through_intermediate(gpu_ctx):
     assert_same(r2, run_oracle(plan))  # at the root it is still a value
 
 
+def test_build_key_output_read_from_probe_side(gpu_ctx):
+    """An output of the build key is read through the probe side's row ids
+    (the two keys are equal on every output row): at the root and below it,
+    with NULL and INT32_MIN keys, with an intermediate probe side, and with a
+    build side that contributes nothing but its key (no build row ids)."""
+    imin = -(2 ** 31)
+    rng = np.random.default_rng(11)
+    nb, npr = 3000, 40000
+    bk = rng.integers(-50, 2000, nb).astype(np.int32)
+    bk[:7] = imin
+    pk = rng.integers(-60, 2100, npr).astype(np.int32)
+    pk[::97] = imin
+    bv = (rng.random(nb) > 0.1).astype(np.uint8)
+    pv = (rng.random(npr) > 0.1).astype(np.uint8)
+    pay = rng.integers(0, 1 << 40, npr).astype(np.int64)
+    plan = Plan()
+    plan.inputs.append(ColumnarTable(nb, [encode_column(I, bk, bv), encode_column(F, rng.random(nb))]))
+    plan.inputs.append(ColumnarTable(npr, [encode_column(I, pk, pv), encode_column(L, pay)]))
+    plan.inputs.append(ColumnarTable(500, [encode_column(I, rng.integers(-60, 2100, 500).astype(np.int32))]))
+    s0 = plan.new_scan_node(0, [(0, I), (1, F)])
+    s1 = plan.new_scan_node(1, [(0, I), (1, L)])
+    s2 = plan.new_scan_node(2, [(0, I)])
+    # root projects only the build key and probe payload: no build row ids
+    plan.new_join_node(True, s0, s1, 0, 0, [(0, I), (3, L)])
+    plan.root = 3
+    r, _ = run_product(plan, gpu_ctx)
+    assert_same(r, run_oracle(plan), "key only")
+    # both keys and a build payload at the root
+    plan.nodes[3].output_attrs = [(0, I), (1, F), (2, I), (3, L)]
+    r, _ = run_product(plan, gpu_ctx)
+    assert_same(r, run_oracle(plan), "keys and payloads")
+    # below the root: the projected build key feeds the next join's key and
+    # the root's output; the next join's probe side is that intermediate
+    j = plan.new_join_node(True, s0, s1, 0, 0, [(0, I), (3, L)])
+    plan.new_join_node(True, s2, j, 0, 0, [(0, I), (1, I), (2, L)])
+    plan.root = 5
+    r, _ = run_product(plan, gpu_ctx)
+    assert_same(r, run_oracle(plan), "through an intermediate")
+
+
+def _direct_case(kind, rng):
+    """Build keys for the direct-mapped table cases."""
+    if kind == "dense_i32":
+        return rng.permutation(50_000).astype(np.int64) - 20_000, I
+    if kind == "dense_i64":
+        return rng.permutation(50_000).astype(np.int64) + (1 << 40), L
+    if kind == "dense_dups":  # dense range, one key repeated: falls back to the hash table
+        k = rng.permutation(50_000).astype(np.int64)
+        k[123] = k[4567]
+        return k, I
+    if kind == "sparse":  # span far above 2 x rows: hash table
+        return rng.choice(1 << 30, 50_000, replace=False).astype(np.int64), I
+    if kind == "extremes":  # INT32_MIN and INT32_MAX as keys: span 2^32
+        k = rng.permutation(50_000).astype(np.int64)
+        k[0], k[1] = -(2 ** 31), 2 ** 31 - 1
+        return k, I
+    raise ValueError(kind)
+
+
+@pytest.mark.parametrize("kind,direct", [("dense_i32", 1), ("dense_i64", 1), ("dense_dups", 0), ("sparse", 0),
+                                         ("extremes", 0)])
+def test_direct_mapped_build(gpu_ctx, kind, direct):
+    """Unique build keys spread over at most twice the build rows take a
+    direct-mapped table; duplicates, wide spans and the option turned off
+    take the hash table. Every path gives the oracle's result."""
+    rng = np.random.default_rng(5)
+    bkeys, kt = _direct_case(kind, rng)
+    nb, npr = len(bkeys), 300_000
+    pick = rng.integers(0, nb, npr)
+    pkeys = bkeys[pick].copy()
+    miss = rng.random(npr) < 0.3
+    pkeys[miss] = rng.integers(bkeys.min() - 1000, bkeys.max() + 1000, int(miss.sum()))
+    bv = (rng.random(nb) > 0.05).astype(np.uint8)
+    bv[[0, 1, 123, 4567]] = 1  # the repeated and the extreme keys are not NULL
+    pv = (rng.random(npr) > 0.02).astype(np.uint8)
+    plan = Plan()
+    npt = np.int32 if kt == I else np.int64
+    if kt == I:
+        pkeys = np.clip(pkeys, -(2 ** 31), 2 ** 31 - 1)
+    plan.inputs.append(ColumnarTable(nb, [encode_column(kt, bkeys.astype(npt), bv),
+                                          encode_column(L, rng.integers(0, 1 << 50, nb))]))
+    plan.inputs.append(ColumnarTable(npr, [encode_column(kt, pkeys.astype(npt), pv),
+                                           encode_column(F, rng.random(npr))]))
+    plan.new_scan_node(0, [(0, kt), (1, L)])
+    plan.new_scan_node(1, [(0, kt), (1, F)])
+    plan.new_join_node(True, 0, 1, 0, 0, [(0, kt), (1, L), (2, kt), (3, F)])
+    plan.root = 2
+    want = run_oracle(plan)
+    try:
+        for opt, expect in ((2, direct), (0, 0)):
+            gpu_ctx.set_option(_lib.CJ_OPT_DENSE_KEYS, opt)
+            r, st = run_product(plan, gpu_ctx)
+            assert_same(r, want, f"{kind} dense_keys={opt}")
+            assert st.exec["num_direct_joins"] == expect
+            assert st.exec["num_hash_joins"] == 1
+    finally:
+        gpu_ctx.set_option(_lib.CJ_OPT_DENSE_KEYS, 2)
+
+
+def test_direct_mapped_all_null_build(gpu_ctx):
+    rng = np.random.default_rng(6)
+    nb, npr = 1000, 20_000
+    plan = Plan()
+    plan.inputs.append(ColumnarTable(nb, [encode_column(I, np.arange(nb, dtype=np.int32), np.zeros(nb, np.uint8))]))
+    plan.inputs.append(ColumnarTable(npr, [encode_column(I, rng.integers(0, nb, npr).astype(np.int32))]))
+    plan.new_scan_node(0, [(0, I)])
+    plan.new_scan_node(1, [(0, I)])
+    plan.new_join_node(True, 0, 1, 0, 0, [(0, I), (1, I)])
+    plan.root = 2
+    r, st = run_product(plan, gpu_ctx)
+    assert r.num_rows == 0
+    assert_same(r, run_oracle(plan))
+    assert st.exec["num_direct_joins"] == 1
+
+
 def test_scan_root(gpu_ctx):
     plan = join2(1000, 10, seed=3, build_payload=(V, F))
     plan.root = 0
