@@ -94,9 +94,34 @@ CJ_DEV bool valid_bit(const uint32_t *valid, uint32_t r) {
     return (__ldg(valid + (r >> 5)) >> (r & 31)) & 1u;
 }
 
+/* A fixed-width column read in place from its pages (no NULL, full
+ * pages; COL_* flags word 0). */
+CJ_DEV bool col_direct(const ColView &c) { return c.col_flags && __ldg(c.col_flags) == 0u; }
+/* A column without NULLs: validity need not be read. */
+CJ_DEV bool col_all_valid(const ColView &c) { return c.col_flags && (__ldg(c.col_flags) & COL_HAS_NULLS) == 0u; }
+
+/* Base row r of a direct column: value r % R of page r / R (R constant per
+ * width, so the division is a multiply). */
+template <typename T> CJ_DEV T page_value(const uint8_t *pages, uint32_t r) {
+    constexpr uint32_t R = sizeof(T) == 4 ? kRowsPerPageInt32 : kRowsPerPage8B;
+    constexpr uint32_t DB = sizeof(T) == 4 ? 4u : 8u;
+    const uint32_t p = r / R, k = r - p * R;
+    return __ldg(reinterpret_cast<const T *>(pages + (uint64_t)p * kPageSize + DB) + k);
+}
+
 /* Join key of relation row i as a 64-bit integer; false if NULL. */
 CJ_DEV bool load_key(const ColView &c, uint32_t i, int64_t *key) {
     uint32_t r = base_row(c, i);
+    if (col_direct(c)) {
+        if (c.type == CJ_INT32) {
+            const int32_t v = page_value<int32_t>(c.pages, r);
+            if (c.null_sentinel && v == INT32_MIN) return false;
+            *key = v;
+        } else {
+            *key = page_value<long long>(c.pages, r);
+        }
+        return true;
+    }
     if (!valid_bit(c.valid, r)) return false;
     if (c.type == CJ_INT32) {
         int32_t v = __ldg(reinterpret_cast<const int32_t *>(c.values) + r);
@@ -111,7 +136,7 @@ CJ_DEV bool load_key(const ColView &c, uint32_t i, int64_t *key) {
 /* Streaming variant for a dense key column read once in row order: the
  * loads are marked evict-first so the hash table stays in L2. */
 CJ_DEV bool load_key_stream(const ColView &c, uint32_t i, int64_t *key) {
-    if (c.rid_a || c.rid_b) return load_key(c, i, key);
+    if (c.rid_a || c.rid_b || col_direct(c)) return load_key(c, i, key);
     if (!((__ldcs(c.valid + (i >> 5)) >> (i & 31)) & 1u)) return false;
     if (c.type == CJ_INT32) {
         int32_t v = __ldcs(reinterpret_cast<const int32_t *>(c.values) + i);

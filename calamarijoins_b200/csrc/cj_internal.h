@@ -80,8 +80,19 @@ struct ColView {
     const uint32_t *rid_b;
     int32_t type;
     int32_t null_sentinel; /* INT32: INT32_MIN reads as NULL (value_t) */
-    const uint32_t *has_nulls; /* device flag, 0: no row is NULL (validity
-                                  need not be read); null: unknown        */
+    const uint32_t *col_flags; /* device word of COL_* bits from the page
+                                  headers; null: unknown (read the decoded
+                                  values and validity)                   */
+};
+
+/* Column flags, set by the page-row pass. A fixed-width column whose word
+ * is 0 has no NULL and every page but the last holds exactly
+ * kRowsPerPageInt32 / kRowsPerPage8B rows (the fill of the reference's
+ * ColumnInserter): row r is value r % R of page r / R, so it is read from
+ * the pages and not decoded at all. */
+enum ColFlag : uint32_t {
+    COL_HAS_NULLS = 1u,  /* some page stores fewer values than rows      */
+    COL_NOT_DIRECT = 2u, /* VARCHAR, or pages not filled as above        */
 };
 
 template <typename K> struct Tuple;
@@ -103,10 +114,13 @@ template <typename K> struct HashTableView {
 
 /* Output of a probe / nested-loop launch. */
 struct MatchOut {
-    uint32_t *build_rids; /* null: not collected (RIGHT_ONLY)           */
-    uint32_t *probe_rids; /* null: not collected (LEFT_ONLY)            */
-    unsigned long long capacity;
-    unsigned long long *counter;
+    uint32_t *build_rids = nullptr; /* null: not collected (RIGHT_ONLY)  */
+    uint32_t *probe_rids = nullptr; /* null: not collected (LEFT_ONLY)   */
+    void *keys = nullptr;           /* null, or the join key of every match
+                                       (key_bytes wide), beside the row ids */
+    int32_t key_bytes = 4;
+    unsigned long long capacity = 0;
+    unsigned long long *counter = nullptr;
 };
 
 /* Kernels launched by this process (every launcher adds its launches). */
@@ -130,17 +144,18 @@ cudaError_t scan_u32_to_u64(const Launch &L, const uint32_t *in, uint64_t *out,
                             size_t n, void *temp);
 
 /* Decode */
-/* Rows per page; *has_nulls (zeroed by the caller, may be null) becomes 1
- * if any page holds a NULL (n_values < n_rows). */
+/* Rows per page, and the column's COL_* flags ORed into *col_flags
+ * (zeroed by the caller; may be null). */
 cudaError_t launch_page_rows(const Launch &L, const uint8_t *pages,
                              uint64_t num_pages, int32_t type,
-                             uint32_t *rows_per_page, uint32_t *has_nulls);
+                             uint32_t *rows_per_page, uint32_t *col_flags);
 /* Rows past max_rows are never written; a page that would write them
- * raises DEV_ERR_ROW_COUNT instead. */
+ * raises DEV_ERR_ROW_COUNT instead. Does nothing when *col_flags is 0
+ * (readers then take the values from the pages). */
 cudaError_t launch_decode_fixed(const Launch &L, const uint8_t *pages,
                                 uint64_t num_pages, int32_t type,
                                 const uint64_t *row_start, uint64_t max_rows,
-                                void *values, uint32_t *valid);
+                                void *values, uint32_t *valid, const uint32_t *col_flags);
 cudaError_t launch_decode_varchar(const Launch &L, const uint8_t *pages,
                                   uint64_t num_pages,
                                   const uint64_t *row_start, uint64_t max_rows,
@@ -164,7 +179,8 @@ cudaError_t launch_decode_grouped(const Launch &L, const DecodeTask *tasks_dev, 
                                   uint64_t total_pages, uint32_t *rows_pp, uint64_t *row_start,
                                   void *scan_temp);
 /* Raises DEV_ERR_ROW_COUNT unless *total == expected. */
-cudaError_t launch_check_rows(const Launch &L, const uint64_t *total, uint64_t expected);
+cudaError_t launch_check_rows(const Launch &L, const uint64_t *total, uint64_t expected,
+                              uint32_t *col_flags = nullptr);
 
 /* Build */
 struct BuildPlan {

@@ -125,10 +125,12 @@ class Executor {
     /* An output column of the root: its relation column and the match row
      * ids that select its rows (null for a scan root). Decoded on use. */
     struct OutCol {
-        const Relation *rel;
+        const Relation *rel; /* null: `fixed` is the column (dense, no NULL) */
         RelCol col;
         const uint32_t *rid_a;
+        ColView fixed;
     };
+    ColView out_view(const OutCol &oc) { return oc.rel ? view(*oc.rel, oc.col, oc.rid_a) : oc.fixed; }
     cj_result *materialize(const std::vector<OutCol> &cols, const std::vector<int32_t> &types,
                            uint64_t rows);
     void ck(cudaError_t e, const char *what) { check_cuda(e, what); }
@@ -211,18 +213,18 @@ Decoded &Executor::decode(uint64_t t, uint64_t c) {
     DevPtr rows_pp = ctx.alloc(std::max<uint64_t>(np, 1) * 4);
     DevPtr row_start = ctx.alloc((np + 1) * 8);
     DevPtr scan_tmp = ctx.alloc(scan_temp_bytes(np));
-    d.has_nulls = ctx.alloc(4);
-    ck(cudaMemsetAsync(d.has_nulls->ptr, 0, 4, ctx.stream), "memset");
+    d.col_flags = ctx.alloc(4);
+    ck(cudaMemsetAsync(d.col_flags->ptr, 0, 4, ctx.stream), "memset");
     {
         KScope k(*this, "page_rows");
-        ck(launch_page_rows(L, d.src.dev, np, d.type, rows_pp->as<uint32_t>(), d.has_nulls->as<uint32_t>()),
+        ck(launch_page_rows(L, d.src.dev, np, d.type, rows_pp->as<uint32_t>(), d.col_flags->as<uint32_t>()),
            "page_rows");
     }
     {
         KScope k(*this, "scan");
         ck(scan_u32_to_u64(L, rows_pp->as<uint32_t>(), row_start->as<uint64_t>(), np, scan_tmp->ptr), "scan");
     }
-    ck(launch_check_rows(L, row_start->as<uint64_t>() + np, d.rows), "check_rows");
+    ck(launch_check_rows(L, row_start->as<uint64_t>() + np, d.rows, d.col_flags->as<uint32_t>()), "check_rows");
     const uint64_t words = (d.rows + 31) / 32;
     d.valid = ctx.alloc(std::max<uint64_t>(words, 1) * 4);
     ck(cudaMemsetAsync(d.valid->ptr, 0, std::max<uint64_t>(words, 1) * 4, ctx.stream), "memset");
@@ -237,7 +239,7 @@ Decoded &Executor::decode(uint64_t t, uint64_t c) {
         d.values = ctx.alloc(d.rows * w);
         KScope k(*this, d.type == CJ_INT32 ? "decode_int32" : "decode_8byte");
         ck(launch_decode_fixed(L, d.src.dev, np, d.type, row_start->as<uint64_t>(), d.rows, d.values->ptr,
-                               d.valid->as<uint32_t>()),
+                               d.valid->as<uint32_t>(), d.col_flags->as<uint32_t>()),
            "decode_fixed");
     }
     return decoded.emplace(key, std::move(d)).first->second;
@@ -278,6 +280,7 @@ Relation Executor::exec_join(uint64_t node_idx, int depth, bool is_root, cj_resu
         bool from_build;
         const Relation *rel;
         RelCol col;
+        bool from_keys = false; /* root: read from the keys the probe writes */
     };
     std::vector<OutRef> outs;
     bool need_b = false, need_p = false;
@@ -302,7 +305,25 @@ Relation Executor::exec_join(uint64_t node_idx, int depth, bool is_root, cj_resu
     stats.num_joins++;
     stats.probe_rows += P.rows;
     uint64_t M = 0;
-    DevPtr mb, mp;
+    /* At the root, outputs of the probe key (and of the build key, which is
+     * read through the probe side) come from the key the probe writes beside
+     * every match: the page writer copies them in order instead of gathering
+     * them through row ids. Matched keys are never NULL. */
+    bool emit_keys = false;
+    if (is_root) {
+        need_p = false;
+        for (auto &o : outs) {
+            if (!o.from_build && o.rel == &P && same_column(o.col, pk)) {
+                o.from_keys = true;
+                emit_keys = true;
+            } else if (!o.from_build) {
+                need_p = true;
+            }
+        }
+    }
+    const bool collect = need_b || need_p || emit_keys;
+    const int32_t key_bytes = pk.type == CJ_INT32 ? 4 : 8;
+    DevPtr mb, mp, mk;
     if (B.rows && P.rows) {
         const ColView bv = view(B, bk, nullptr);
         const ColView pv = view(P, pk, nullptr);
@@ -383,10 +404,13 @@ Relation Executor::exec_join(uint64_t node_idx, int depth, bool is_root, cj_resu
         for (;;) {
             mb = need_b ? ctx.alloc(cap * 4) : nullptr;
             mp = need_p ? ctx.alloc(cap * 4) : nullptr;
+            mk = emit_keys ? ctx.alloc(cap * key_bytes) : nullptr;
             MatchOut mo;
             mo.build_rids = mb ? mb->as<uint32_t>() : nullptr;
             mo.probe_rids = mp ? mp->as<uint32_t>() : nullptr;
-            mo.capacity = (need_b || need_p) ? cap : 0;
+            mo.keys = mk ? mk->ptr : nullptr;
+            mo.key_bytes = key_bytes;
+            mo.capacity = collect ? cap : 0;
             mo.counter = &ctx.d_status->counter;
             DevPtr sched = ctx.alloc(probe_sched_bytes((uint32_t)P.rows));
             {
@@ -419,7 +443,7 @@ Relation Executor::exec_join(uint64_t node_idx, int depth, bool is_root, cj_resu
                 continue;
             }
             M = ctx.h_status->counter;
-            if (M <= cap || !(need_b || need_p)) break;
+            if (M <= cap || !collect) break;
             if (M > 0xFFFFFFFFull) fail(CJ_ERR_LIMIT, "join result exceeds 2^32-1 rows");
             stats.probe_reruns++;
             cap = M;
@@ -433,8 +457,15 @@ Relation Executor::exec_join(uint64_t node_idx, int depth, bool is_root, cj_resu
         std::vector<OutCol> cols;
         std::vector<int32_t> types;
         for (auto &o : outs) {
-            const uint32_t *ra = o.from_build ? (mb ? mb->as<uint32_t>() : nullptr) : (mp ? mp->as<uint32_t>() : nullptr);
-            cols.push_back({o.rel, o.col, ra});
+            OutCol oc{o.rel, o.col, nullptr, ColView{}};
+            if (o.from_keys) {
+                oc.rel = nullptr;
+                oc.fixed.values = mk ? mk->ptr : nullptr;
+                oc.fixed.type = o.col.type; /* == the probe key's type */
+            } else {
+                oc.rid_a = o.from_build ? (mb ? mb->as<uint32_t>() : nullptr) : (mp ? mp->as<uint32_t>() : nullptr);
+            }
+            cols.push_back(oc);
             types.push_back(o.col.type);
         }
         *out = materialize(cols, types, M);
@@ -524,7 +555,7 @@ cj_result *Executor::materialize(const std::vector<OutCol> &cols, const std::vec
             for (size_t c = 0; c < nc; ++c) {
                 if (types[c] != CJ_VARCHAR) continue;
                 vtemp[c] = ctx.alloc(varchar_temp_bytes(rows, TR));
-                const ColView cv = view(*cols[c].rel, cols[c].col, cols[c].rid_a);
+                const ColView cv = out_view(cols[c]);
                 KScope ks(*this, "varchar_plan");
                 ck(launch_varchar_plan(L, cv, rows, TR, vtemp[c]->ptr,
                                        totals->as<unsigned long long>() + k),
@@ -560,7 +591,7 @@ cj_result *Executor::materialize(const std::vector<OutCol> &cols, const std::vec
             if (!rows) continue;
             /* decoded here, not before the loop: the kernel stream waits for
              * a column's upload only when its pages are written */
-            const ColView cv = view(*cols[c].rel, cols[c].col, cols[c].rid_a);
+            const ColView cv = out_view(cols[c]);
             res->dev_pages[c] = ctx.alloc(res->num_pages[c] * kPageSize);
             if (types[c] != CJ_VARCHAR) {
                 KScope ks(*this, types[c] == CJ_INT32 ? "write_pages_int32" : "write_pages_8byte");
@@ -611,7 +642,7 @@ cj_result *Executor::run(cj_exec_stats *st) {
         std::vector<OutCol> cols;
         std::vector<int32_t> types;
         for (auto &c : s.cols) {
-            cols.push_back({&s, c, nullptr});
+            cols.push_back({&s, c, nullptr, ColView{}});
             types.push_back(c.type);
         }
         res = materialize(cols, types, s.rows);

@@ -24,7 +24,7 @@ struct Decoded {
     uint64_t rows = 0;
     ColumnPages src;
     DevPtr values, valid, desc;
-    DevPtr has_nulls; /* u32 flag from the page headers; null: not computed */
+    DevPtr col_flags; /* u32 COL_* flags from the page headers; null: not computed */
 };
 
 /* A column of a relation: base column (input, col) reached through row-id
@@ -93,7 +93,7 @@ inline ColView make_view(const Decoded &d, const Relation &R, const RelCol &c, c
     v.rid_a = rid_a;
     v.rid_b = c.vec >= 0 ? R.vecs[c.vec]->as<uint32_t>() : nullptr;
     v.null_sentinel = (c.sentinel && c.type == CJ_INT32) ? 1 : 0;
-    v.has_nulls = d.has_nulls ? d.has_nulls->as<uint32_t>() : nullptr;
+    v.col_flags = d.col_flags ? d.col_flags->as<uint32_t>() : nullptr;
     return v;
 }
 

@@ -53,23 +53,29 @@ CJ_DEV uint32_t page_rows_of(const uint8_t *pg, int32_t type, unsigned int *err)
     return r;
 }
 
-/* True if a regular page stores fewer values than rows (some row is
- * NULL); long-string pages hold one non-NULL row or none. */
-CJ_DEV bool page_has_nulls(const uint8_t *pg, int32_t type) {
+/* COL_* flags of page p of np: COL_HAS_NULLS if a regular page stores
+ * fewer values than rows (long-string pages hold one non-NULL row or none);
+ * COL_NOT_DIRECT for VARCHAR, or unless every page but the last holds
+ * exactly R rows and the last 1..R. */
+CJ_DEV uint32_t page_flags(const uint8_t *pg, uint64_t p, uint64_t np, int32_t type) {
     const uint32_t nr = rd16(pg), nv = rd16(pg + 2);
-    if (type == CJ_VARCHAR && nr >= 0xfffe) return false;
-    return nv < nr;
+    if (type == CJ_VARCHAR) return COL_NOT_DIRECT | ((nr < 0xfffe && nv < nr) ? COL_HAS_NULLS : 0u);
+    const uint32_t R = type == CJ_INT32 ? kRowsPerPageInt32 : kRowsPerPage8B;
+    uint32_t f = nv < nr ? COL_HAS_NULLS : 0u;
+    if (p + 1 < np ? nr != R : (nr == 0 || nr > R)) f |= COL_NOT_DIRECT;
+    return f;
 }
 
 __global__ void k_page_rows(const uint8_t *__restrict__ pages, uint64_t np, int32_t type,
-                            uint32_t *__restrict__ rows, uint32_t *has_nulls, unsigned int *err) {
-    bool nulls = false;
+                            uint32_t *__restrict__ rows, uint32_t *col_flags, unsigned int *err) {
+    uint32_t f = 0;
     for (uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; p < np;
          p += (uint64_t)gridDim.x * blockDim.x) {
         rows[p] = page_rows_of(pages + p * kPageSize, type, err);
-        nulls |= page_has_nulls(pages + p * kPageSize, type);
+        f |= page_flags(pages + p * kPageSize, p, np, type);
     }
-    if (__any_sync(0xffffffffu, nulls) && lane_id() == 0 && has_nulls) *has_nulls = 1u;
+    f = __reduce_or_sync(0xffffffffu, f);
+    if (f && lane_id() == 0 && col_flags) atomicOr(col_flags, f);
 }
 
 /* Loads a sparse page's bitmap into s_bm (bits past n_rows cleared) and the
@@ -256,8 +262,10 @@ CJ_DEV void decode_varchar_page(const uint8_t *__restrict__ pages, uint64_t p, u
 template <typename T>
 __global__ void __launch_bounds__(kDecodeThreads, 8)
     k_decode_fixed(const uint8_t *__restrict__ pages, uint64_t np, const uint64_t *__restrict__ row_start,
-                   uint64_t max_rows, T *__restrict__ values, uint32_t *__restrict__ valid, unsigned int *err) {
+                   uint64_t max_rows, T *__restrict__ values, uint32_t *__restrict__ valid, unsigned int *err,
+                   const uint32_t *__restrict__ col_flags) {
     __shared__ DecodeSmem sm;
+    if (col_flags && *col_flags == 0u) return; /* read in place from the pages */
     for (uint64_t p = blockIdx.x; p < np; p += gridDim.x)
         decode_fixed_page<T>(pages, p, row_start[p], max_rows, values, valid, err, sm);
 }
@@ -321,8 +329,11 @@ __global__ void __launch_bounds__(kDecodeThreads)
     }
 }
 
-__global__ void k_check_rows(const uint64_t *total, uint64_t expected, unsigned int *err) {
-    if (*total != expected) atomicOr(err, DEV_ERR_ROW_COUNT);
+__global__ void k_check_rows(const uint64_t *total, uint64_t expected, unsigned int *err, uint32_t *col_flags) {
+    if (*total != expected) {
+        atomicOr(err, DEV_ERR_ROW_COUNT);
+        if (col_flags) atomicOr(col_flags, COL_NOT_DIRECT); /* readers stay inside the decoded arrays */
+    }
 }
 
 unsigned grid_for(const Launch &L, uint64_t units, int per_sm) {
@@ -334,27 +345,28 @@ unsigned grid_for(const Launch &L, uint64_t units, int per_sm) {
 } // namespace
 
 cudaError_t launch_page_rows(const Launch &L, const uint8_t *pages, uint64_t np, int32_t type,
-                             uint32_t *rows, uint32_t *has_nulls) {
+                             uint32_t *rows, uint32_t *col_flags) {
     if (np == 0) return cudaSuccess;
     unsigned g = (unsigned)((np + 255) / 256);
     if (g > (unsigned)L.num_sms * 8) g = L.num_sms * 8;
-    k_page_rows<<<g, 256, 0, L.stream>>>(pages, np, type, rows, has_nulls, L.dev_errors);
+    k_page_rows<<<g, 256, 0, L.stream>>>(pages, np, type, rows, col_flags, L.dev_errors);
     count_launches(1);
     return cudaGetLastError();
 }
 
 cudaError_t launch_decode_fixed(const Launch &L, const uint8_t *pages, uint64_t np, int32_t type,
                                 const uint64_t *row_start, uint64_t max_rows, void *values,
-                                uint32_t *valid) {
+                                uint32_t *valid, const uint32_t *col_flags) {
     if (np == 0) return cudaSuccess;
     unsigned g = grid_for(L, np, 8); /* 32 registers, 16 KB shared: 8 CTAs per SM */
     if (type == CJ_INT32) {
         k_decode_fixed<int32_t><<<g, kDecodeThreads, 0, L.stream>>>(
-            pages, np, row_start, max_rows, reinterpret_cast<int32_t *>(values), valid, L.dev_errors);
+            pages, np, row_start, max_rows, reinterpret_cast<int32_t *>(values), valid, L.dev_errors, col_flags);
         count_launches(1);
     } else {
         k_decode_fixed<long long><<<g, kDecodeThreads, 0, L.stream>>>(
-            pages, np, row_start, max_rows, reinterpret_cast<long long *>(values), valid, L.dev_errors);
+            pages, np, row_start, max_rows, reinterpret_cast<long long *>(values), valid, L.dev_errors,
+            col_flags);
         count_launches(1);
     }
     return cudaGetLastError();
@@ -391,8 +403,8 @@ cudaError_t launch_decode_grouped(const Launch &L, const DecodeTask *tasks_dev, 
     return cudaGetLastError();
 }
 
-cudaError_t launch_check_rows(const Launch &L, const uint64_t *total, uint64_t expected) {
-    k_check_rows<<<1, 1, 0, L.stream>>>(total, expected, L.dev_errors);
+cudaError_t launch_check_rows(const Launch &L, const uint64_t *total, uint64_t expected, uint32_t *col_flags) {
+    k_check_rows<<<1, 1, 0, L.stream>>>(total, expected, L.dev_errors, col_flags);
     count_launches(1);
     return cudaGetLastError();
 }

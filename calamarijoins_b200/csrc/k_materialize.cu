@@ -12,10 +12,12 @@
  * Fixed-width pages (k_write_fixed): output page p holds rows
  * [p*R, p*R+R) with R = 1984 (INT32) or 1007 (INT64 / FP64), the fill of
  * ColumnInserter<T> (plan.h:241-250), so every page fits whatever the NULL
- * pattern. One CTA builds one page in shared memory: all of the page's
- * loads issued at once, values compacted by one ballot/scan over the
- * validity bits, bitmap at the page end, header (n_rows, n_values), gap
- * zeroed; then 16-byte streaming stores write the page out.
+ * pattern. One CTA writes one page: all of the page's loads issued at
+ * once; a page without NULLs is stored straight from registers (values in
+ * row order, header, zero gap, all-ones bitmap); a page with NULLs is built
+ * in shared memory (values compacted by one ballot/scan over the validity
+ * bits, bitmap at the page end, gap zeroed) and written with 16-byte
+ * streaming stores.
  *
  * VARCHAR pages (k_varchar_plan / k_varchar_write): rows are cut into tiles;
  * within a tile pages are packed greedily in row order like
@@ -100,19 +102,55 @@ CJ_DEV void write_fixed_page(const ColView &col, uint64_t rows, uint32_t R, uint
     T val[kSlabs];
     uint32_t vm = 0; /* bit k: row of slab k is non-NULL */
     /* a column without NULLs needs no validity loads (one random load per
-     * row instead of two when the row ids are random) */
-    const bool all_valid = col.has_nulls && __ldg(col.has_nulls) == 0u;
+     * row instead of two when the row ids are random); a direct column is
+     * read from its pages */
+    const bool all_valid = !col.valid || col_all_valid(col); /* no validity array: no NULL */
+    const bool direct = col_direct(col);
 #pragma unroll
     for (int k = 0; k < kSlabs; ++k) {
         val[k] = T(0);
         if (br[k] != 0xffffffffu) {
             const bool v = all_valid || valid_bit(col.valid, br[k]);
-            val[k] = __ldg(reinterpret_cast<const T *>(col.values) + br[k]);
+            val[k] = direct ? page_value<T>(col.pages, br[k]) : __ldg(reinterpret_cast<const T *>(col.values) + br[k]);
             if (v && !(sizeof(T) == 4 && col.null_sentinel && (int32_t)val[k] == INT32_MIN)) vm |= 1u << k;
         }
     }
 
     const uint32_t bm_bytes = (nr + 7) / 8;
+
+    /* No NULL on this page (always, for a column without NULLs): a value's
+     * place is its row, so the page is stored straight from registers, with
+     * no compaction, no shared memory and no barrier. Same bytes as below:
+     * header, values, zero gap, bitmap of nr ones. */
+    uint32_t live = 0;
+#pragma unroll
+    for (int k = 0; k < kSlabs; ++k)
+        if (k * kMatThreads + threadIdx.x < nr) live |= 1u << k;
+    const bool null_free_col = all_valid && !(sizeof(T) == 4 && col.null_sentinel);
+    if (null_free_col || !__syncthreads_or(vm != live)) {
+        uint8_t *dst = out + pg * kPageSize;
+        T *dv = reinterpret_cast<T *>(dst + DB);
+#pragma unroll
+        for (int k = 0; k < kSlabs; ++k) {
+            const uint32_t r = k * kMatThreads + threadIdx.x;
+            if (r < nr) __stcs(dv + r, val[k]);
+        }
+        if (threadIdx.x == 0) {
+            if (DB == 8) __stcs(reinterpret_cast<unsigned long long *>(dst), (unsigned long long)nr * 0x10001ull);
+            else __stcs(reinterpret_cast<unsigned int *>(dst), nr * 0x10001u);
+        }
+        const uint32_t bm0 = kPageSize - bm_bytes;
+        for (uint32_t b = DB + nr * (uint32_t)sizeof(T) + threadIdx.x; b < kPageSize; b += blockDim.x) {
+            uint8_t v = 0;
+            if (b >= bm0) {
+                const uint32_t i = b - bm0;
+                v = (i + 1) * 8 <= nr ? 0xFFu : (uint8_t)((1u << (nr - i * 8)) - 1u);
+            }
+            dst[b] = v;
+        }
+        return;
+    }
+
     uint8_t *bm = sp + kPageSize - bm_bytes;
 #pragma unroll
     for (int k = 0; k < kSlabs; ++k) {
@@ -242,7 +280,7 @@ CJ_DEV VarSmem carve(uint8_t *base, uint32_t TR) {
  * segment count; the page count is in s.segpg[nseg]. Block-wide. */
 CJ_DEV uint32_t plan_tile(const ColView &col, uint64_t r0, uint32_t nt, uint32_t TR,
                           const VarSmem &s, uint32_t *wbuf, uint32_t *s_nseg) {
-    const bool all_valid = col.has_nulls && __ldg(col.has_nulls) == 0u;
+    const bool all_valid = col_all_valid(col);
     for (uint32_t r = threadIdx.x; r < nt; r += blockDim.x) {
         uint32_t br = base_row(col, (uint32_t)(r0 + r));
         s.desc[r] = (all_valid || valid_bit(col.valid, br)) ? __ldg(col.str_desc + br) : 0ull;

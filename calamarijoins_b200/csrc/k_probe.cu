@@ -48,6 +48,13 @@ struct TileSched {
 
 /* ---------------- matchers ---------------- */
 
+/* The join key of match `pos`, when the caller asked for it. */
+CJ_DEV void put_key(const MatchOut &out, unsigned long long pos, int64_t key) {
+    if (!out.keys) return;
+    if (out.key_bytes == 4) reinterpret_cast<int32_t *>(out.keys)[pos] = (int32_t)key;
+    else reinterpret_cast<long long *>(out.keys)[pos] = key;
+}
+
 /* Directory entry: start of the slot's tuples (bits 63..32), their count
  * (31..16, saturated at 0xFFFF: then the next entry's start bounds them) and
  * the OR of their Bloom tags (15..0). */
@@ -92,6 +99,7 @@ template <typename KB> struct HashMatcher {
             if (pos < out.capacity) {
                 if (out.build_rids) out.build_rids[pos] = t.rid;
                 if (out.probe_rids) out.probe_rids[pos] = prow;
+                put_key(out, pos, key);
             }
             ++pos;
         }
@@ -126,6 +134,7 @@ struct ArrayMatcher {
         if (count(sh, key, r) && pos < out.capacity) {
             if (out.build_rids) out.build_rids[pos] = r;
             if (out.probe_rids) out.probe_rids[pos] = prow;
+            put_key(out, pos, key);
         }
     }
 };
@@ -164,6 +173,7 @@ struct LoopMatcher {
             if (pos < out.capacity) {
                 if (out.build_rids) out.build_rids[pos] = sh.rids[b];
                 if (out.probe_rids) out.probe_rids[pos] = prow;
+                put_key(out, pos, key);
             }
             ++pos;
         }
@@ -174,6 +184,7 @@ struct LoopMatcher {
  * memory, not registers, so the kernel fits 32 registers (8 CTAs per SM). */
 struct ProbeSmem {
     uint32_t first[kTileRows]; /* first matching build row (one-match rows) */
+    int64_t key[kTileRows];    /* the row's key, when the matches carry it   */
     uint32_t pre[kTileRows];   /* row's match offset within its warp        */
     uint32_t warp[kProbeThreads / 32 + 1];
     uint32_t tile;
@@ -199,6 +210,7 @@ CJ_DEV void probe_tile(const ColView &pkey, uint32_t n, const M &m, const typena
         kinds |= (c == 0 ? 0u : (c == 1 ? 1u : 2u)) << (2 * it);
         const uint32_t incl = warp_inclusive_scan(c);
         ps.first[si] = first;
+        if (out.keys && c == 1) ps.key[si] = key;
         ps.pre[si] = wrun + incl - c;
         wrun += __shfl_sync(0xffffffffu, incl, 31);
     }
@@ -225,6 +237,7 @@ CJ_DEV void probe_tile(const ColView &pkey, uint32_t n, const M &m, const typena
             if (pos < out.capacity) {
                 if (out.build_rids) out.build_rids[pos] = ps.first[si];
                 if (out.probe_rids) out.probe_rids[pos] = prow;
+                if (out.keys) put_key(out, pos, ps.key[si]);
             }
         } else {
             int64_t key;

@@ -5,7 +5,7 @@ oracle's, and every output page must be well formed."""
 import numpy as np
 import pytest
 
-from calamarijoins_b200 import (CJError, ColumnarTable, DataType, Plan, PlanDescriptor, ResidentTable, Table,
+from calamarijoins_b200 import (CJError, Column, ColumnarTable, DataType, Plan, PlanDescriptor, ResidentTable, Table,
                                 encode_column, execute_raw)
 from calamarijoins_b200 import _lib
 from calamarijoins_b200.datagen import chain_plan, config_c1, config_c3, join2
@@ -273,6 +273,41 @@ def test_direct_mapped_all_null_build(gpu_ctx):
     assert st.exec["num_direct_joins"] == 1
 
 
+def test_scan_root_pages_byte_identical(gpu_ctx):
+    """A scan root writes its rows in order. For NULL-free columns (pages
+    stored straight from registers) its pages are the input pages byte for
+    byte: both hold 1984 / 1007 rows per page, ColumnInserter's fill. With
+    NULLs the writer keeps that fixed fill (compacting each page's values in
+    shared memory), where ColumnInserter packs more rows into a page; those
+    columns must hold the same rows, in ceil(n / R) well-formed pages,
+    including a column that mixes NULL-free pages with pages holding NULLs."""
+    rng = np.random.default_rng(12)
+    n = 50_000
+    mixed = np.ones(n, np.uint8)
+    mixed[20_000:21_000] = rng.random(1000) > 0.5  # NULLs on a few pages only
+    cols = [
+        encode_column(I, rng.integers(-(2 ** 31), 2 ** 31, n).astype(np.int32)),
+        encode_column(L, rng.integers(-(1 << 62), 1 << 62, n)),
+        encode_column(F, rng.standard_normal(n)),
+        encode_column(I, rng.integers(0, 100, n).astype(np.int32), (rng.random(n) > 0.1).astype(np.uint8)),
+        encode_column(F, rng.standard_normal(n), (rng.random(n) > 0.3).astype(np.uint8)),
+        encode_column(L, rng.integers(0, 1 << 40, n), mixed),
+    ]
+    types = [I, L, F, I, F, L]
+    plan = Plan()
+    plan.inputs.append(ColumnarTable(n, cols))
+    plan.new_scan_node(0, [(i, t) for i, t in enumerate(types)])
+    plan.root = 0
+    r, _ = run_product(plan, gpu_ctx)
+    assert_same(r, run_oracle(plan))
+    for c, col in enumerate(cols[:3]):
+        assert r.pages[c].shape == col.pages.shape, c
+        assert np.array_equal(r.pages[c], col.pages), f"column {c}: pages differ"
+    for c in range(3, 6):
+        R = 1984 if types[c] == I else 1007
+        assert r.pages[c].shape[0] == (n + R - 1) // R
+
+
 def test_scan_root(gpu_ctx):
     plan = join2(1000, 10, seed=3, build_payload=(V, F))
     plan.root = 0
@@ -319,11 +354,47 @@ def test_malformed_pages_rejected(gpu_ctx):
 
 
 def test_row_count_mismatch_rejected(gpu_ctx):
-    plan = join2(3000, 3000, seed=7)
-    plan.inputs[1].num_rows = 2999
-    with pytest.raises(CJError) as e:
-        run_product(plan, gpu_ctx)
-    assert e.value.status == 3
+    # fewer and more rows declared than the pages hold, on the probe side and
+    # on the (NULL-free, full-page) build side, whose columns would otherwise
+    # be read in place from their pages
+    for side, delta in ((1, -1), (1, 1), (0, 1), (0, 1000)):
+        plan = join2(3000, 5000, seed=7, build_payload=(L,), probe_payload=(F,))
+        plan.inputs[side].num_rows += delta
+        with pytest.raises(CJError) as e:
+            run_product(plan, gpu_ctx)
+        assert e.value.status == 3
+    r, _ = run_product(join2(300, 500, seed=8), gpu_ctx)  # the context still works
+    assert r.num_rows > 0
+
+
+def _chunked(dtype, values, chunk):
+    """A column written by a producer that starts a new page every `chunk`
+    rows: every page but the last partial, unlike ColumnInserter's fill."""
+    parts = [encode_column(dtype, values[i:i + chunk]) for i in range(0, len(values), chunk)]
+    return Column(dtype, np.ascontiguousarray(np.concatenate([c.pages for c in parts])))
+
+
+def test_partial_pages_are_decoded(gpu_ctx):
+    """NULL-free fixed-width columns are read in place from their pages only
+    when every page but the last holds the full 1984 / 1007 rows; columns of
+    partial pages take the decode path. Both agree with the oracle."""
+    rng = np.random.default_rng(9)
+    nb, npr = 20_000, 200_000
+    bk = rng.permutation(nb).astype(np.int32)
+    pk = rng.integers(0, nb + 5000, npr).astype(np.int32)
+    bp = rng.integers(-(1 << 60), 1 << 60, nb)
+    pp = rng.random(npr)
+    for chunk in (None, 1000, 1983):
+        enc = (lambda t, v: encode_column(t, v)) if chunk is None else (lambda t, v, c=chunk: _chunked(t, v, c))
+        plan = Plan()
+        plan.inputs.append(ColumnarTable(nb, [enc(I, bk), enc(L, bp)]))
+        plan.inputs.append(ColumnarTable(npr, [enc(I, pk), enc(F, pp)]))
+        plan.new_scan_node(0, [(0, I), (1, L)])
+        plan.new_scan_node(1, [(0, I), (1, F)])
+        plan.new_join_node(True, 0, 1, 0, 0, [(0, I), (1, L), (2, I), (3, F)])
+        plan.root = 2
+        r, _ = run_product(plan, gpu_ctx)
+        assert_same(r, run_oracle(plan), f"chunk={chunk}")
 
 
 def test_invalid_plans(gpu_ctx):
