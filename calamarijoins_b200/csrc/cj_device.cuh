@@ -133,6 +133,15 @@ CJ_DEV bool load_key(const ColView &c, uint32_t i, int64_t *key) {
     return true;
 }
 
+/* A copy of `c` whose col_flags pointer is kept only when the column is
+ * read in place (col_direct): with it, per-row loaders test a kernel
+ * argument instead of loading the flag word for every row. */
+CJ_DEV ColView resolve_view(const ColView &c) {
+    ColView v = c;
+    if (!col_direct(c)) v.col_flags = nullptr;
+    return v;
+}
+
 /* Streaming variant for a dense key column read once in row order: the
  * loads are marked evict-first so the hash table stays in L2. */
 CJ_DEV bool load_key_stream(const ColView &c, uint32_t i, int64_t *key) {

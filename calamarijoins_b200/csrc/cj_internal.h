@@ -227,18 +227,19 @@ cudaError_t launch_build_grouped(const Launch &L, const BuildTask *tasks_dev, ui
                                  const uint16_t *bloom, void *temp);
 
 /* Direct-mapped build for unique keys spread densely over [lo, lo + span):
- * slots[key - lo] = build row. `range` (3 u64, set by the caller to
- * {~0, 0, 0}) receives the min and max non-NULL key, each XOR 2^63 so that
- * unsigned order is signed order, and the non-NULL count. The build sets
- * *dup to 1 if two rows share a key; slots start as kArrayEmpty. */
+ * slots[key - lo] = build row, decided on the device. `params` (6 u64, set
+ * by the caller to {~0, 0, 0, 0, 0, 0}) receives [0] min and [1] max of the
+ * non-NULL keys (XOR 2^63: unsigned order is signed order), [2] their count,
+ * [3] 1 when the table cannot be used (span above max_span, or a repeated
+ * key), [4] lo, [5] span. `slots` holds max_span entries. Four launches, no
+ * host round trip. */
 constexpr uint32_t kArrayEmpty = 0xFFFFFFFFu;
-cudaError_t launch_key_range(const Launch &L, const ColView &key, uint32_t n, unsigned long long *range);
-cudaError_t launch_array_build(const Launch &L, const ColView &key, uint32_t n, int64_t lo, uint64_t span,
-                               uint32_t *slots, unsigned long long *dup);
-/* Probe of a direct-mapped table; does nothing when *dup is set. */
+constexpr int kDirectParams = 6;
+cudaError_t launch_direct_build(const Launch &L, const ColView &key, uint32_t n, uint64_t max_span, uint32_t *slots,
+                                unsigned long long *params);
+/* Probe of a direct-mapped table; does nothing when params[3] is set. */
 cudaError_t launch_probe_tiles_array(const Launch &L, const ColView &pkey, uint32_t n_probe, const uint32_t *slots,
-                                     int64_t lo, uint64_t span, const unsigned long long *dup, const MatchOut &out,
-                                     void *sched);
+                                     const unsigned long long *params, const MatchOut &out, void *sched);
 
 /* Probe and nested loop share one tiled kernel; `sched` is scratch of
  * probe_sched_bytes(n_probe) bytes (the tile ticket). */

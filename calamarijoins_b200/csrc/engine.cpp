@@ -331,10 +331,8 @@ Relation Executor::exec_join(uint64_t node_idx, int depth, bool is_root, cj_resu
         const bool nl = B.rows <= nl_max;
         DevPtr dir, tuples, nlk, nlr, nlc, slots;
         int log2_slots = 0;
-        bool direct = false; /* direct-mapped table instead of the hash table */
-        int64_t lo = 0;
-        uint64_t span = 0;
-        unsigned long long *d_dup = &ctx.d_status->aux[3];
+        bool direct = false; /* direct-mapped table tried (the device decides) */
+        unsigned long long *d_params = &ctx.d_status->aux[0];
         auto build_hash = [&]() {
             BuildPlan bp;
             bp.num_rows = (uint32_t)B.rows;
@@ -367,36 +365,21 @@ Relation Executor::exec_join(uint64_t node_idx, int depth, bool is_root, cj_resu
             stats.num_hash_joins++;
             PhaseScope ph(*this, PH_BUILD);
             if (ctx.opt.dense_keys > 0) {
-                /* Key range of the build side (one host round trip). Unique
-                 * keys spread over at most dense_keys x rows values get a
-                 * direct-mapped table: one random access per probe row
-                 * instead of a directory entry and a tuple. */
-                ck(cudaMemsetAsync(&ctx.d_status->aux[0], 0xFF, 8, ctx.stream), "memset");
-                ck(cudaMemsetAsync(&ctx.d_status->aux[1], 0, 24, ctx.stream), "memset");
-                {
-                    KScope k(*this, "key_range");
-                    ck(launch_key_range(L, bv, (uint32_t)B.rows, &ctx.d_status->aux[0]), "key_range");
-                }
-                ctx.sync_status();
-                const uint64_t cnt = ctx.h_status->aux[2];
-                if (cnt == 0) {
-                    direct = true; /* no non-NULL build key: nothing can match */
-                } else {
-                    lo = (int64_t)(ctx.h_status->aux[0] ^ (1ull << 63));
-                    const int64_t hi = (int64_t)(ctx.h_status->aux[1] ^ (1ull << 63));
-                    const uint64_t width = (uint64_t)hi - (uint64_t)lo; /* span - 1, no overflow */
-                    if (width < 0xFFFFFFFFull && width + 1 <= (uint64_t)ctx.opt.dense_keys * B.rows) {
-                        direct = true;
-                        span = width + 1;
-                    }
-                }
-                if (direct && span) {
-                    slots = ctx.alloc(span * 4);
-                    ck(cudaMemsetAsync(slots->ptr, 0xFF, span * 4, ctx.stream), "memset");
-                    KScope k(*this, "array_build");
-                    ck(launch_array_build(L, bv, (uint32_t)B.rows, lo, span, slots->as<uint32_t>(), d_dup),
-                       "array_build");
-                }
+                /* Unique keys spread over at most dense_keys x rows values get
+                 * a direct-mapped table: one random access per probe row
+                 * instead of a directory entry and a tuple. The device works
+                 * out the key range and whether the table is usable; the
+                 * host learns it at the probe's own synchronisation and then,
+                 * if it was not, builds the hash table. */
+                const uint64_t max_span =
+                    std::min<uint64_t>((uint64_t)ctx.opt.dense_keys * B.rows, 0xFFFFFFFFull);
+                ck(cudaMemsetAsync(d_params, 0xFF, 8, ctx.stream), "memset");
+                ck(cudaMemsetAsync(d_params + 1, 0, (kDirectParams - 1) * 8, ctx.stream), "memset");
+                slots = ctx.alloc(max_span * 4);
+                KScope k(*this, "direct_build");
+                ck(launch_direct_build(L, bv, (uint32_t)B.rows, max_span, slots->as<uint32_t>(), d_params),
+                   "direct_build");
+                direct = true;
             }
             if (!direct) build_hash();
         }
@@ -422,8 +405,8 @@ Relation Executor::exec_join(uint64_t node_idx, int depth, bool is_root, cj_resu
                        "nl_probe");
                 } else if (direct) {
                     KScope k(*this, "probe_array");
-                    ck(launch_probe_tiles_array(L, pv, (uint32_t)P.rows, slots ? slots->as<uint32_t>() : nullptr,
-                                                lo, span, d_dup, mo, sched->ptr),
+                    ck(launch_probe_tiles_array(L, pv, (uint32_t)P.rows, slots->as<uint32_t>(), d_params, mo,
+                                                sched->ptr),
                        "probe_array");
                 } else {
                     KScope k(*this, "probe_hash");
@@ -434,8 +417,8 @@ Relation Executor::exec_join(uint64_t node_idx, int depth, bool is_root, cj_resu
             }
             ctx.sync_status();
             if (direct && ctx.h_status->aux[3]) {
-                /* a key repeats: the direct-mapped table cannot hold the
-                 * build side (the probe did nothing); use the hash table */
+                /* keys too spread out, or a key repeats: the direct-mapped
+                 * table is unusable (the probe did nothing); hash table */
                 direct = false;
                 slots.reset();
                 PhaseScope ph(*this, PH_BUILD);

@@ -380,14 +380,34 @@ __global__ void __launch_bounds__(kBuildThreads)
     }
 }
 
-__global__ void k_array_build(ColView key, uint32_t n, int64_t lo, uint64_t span, uint32_t *__restrict__ slots,
-                              unsigned long long *dup) {
+/* params: [0] min ^ 2^63, [1] max ^ 2^63, [2] count (from k_key_range),
+ * [3] unusable, [4] lo, [5] span. */
+__global__ void k_array_prep(unsigned long long *p, uint64_t max_span) {
+    if (p[2] == 0) return; /* no non-NULL key: span 0, nothing matches */
+    const unsigned long long width = p[1] - p[0]; /* max - min: the bias cancels */
+    if (width >= max_span) {
+        p[3] = 1ull;
+        return;
+    }
+    p[4] = p[0] ^ (1ull << 63);
+    p[5] = width + 1;
+}
+
+__global__ void k_array_fill(uint32_t *__restrict__ slots, const unsigned long long *p) {
+    const uint64_t span = p[5];
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < span; i += (uint64_t)gridDim.x * blockDim.x)
+        slots[i] = kArrayEmpty;
+}
+
+__global__ void k_array_build(ColView key, uint32_t n, uint32_t *__restrict__ slots, unsigned long long *p) {
+    if (p[3]) return;
+    const uint64_t lo = p[4], span = p[5];
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
         int64_t k;
         if (!load_key(key, (uint32_t)i, &k)) continue;
-        const uint64_t off = (uint64_t)k - (uint64_t)lo;
-        if (off >= span) continue; /* cannot happen when lo/span come from k_key_range */
-        if (atomicCAS(slots + off, kArrayEmpty, (uint32_t)i) != kArrayEmpty) *dup = 1ull;
+        const uint64_t off = (uint64_t)k - lo;
+        if (off >= span) continue; /* cannot happen: lo and span come from these keys */
+        if (atomicCAS(slots + off, kArrayEmpty, (uint32_t)i) != kArrayEmpty) p[3] = 1ull;
     }
 }
 
@@ -457,22 +477,18 @@ size_t build_grouped_temp_bytes(uint64_t total_cells) {
     return align256(total_cells * 4) + align256((total_cells + 1) * 8) + scan_temp_bytes(total_cells) + 256;
 }
 
-cudaError_t launch_key_range(const Launch &L, const ColView &key, uint32_t n, unsigned long long *range) {
+cudaError_t launch_direct_build(const Launch &L, const ColView &key, uint32_t n, uint64_t max_span, uint32_t *slots,
+                                unsigned long long *params) {
     if (n == 0) return cudaSuccess;
     uint64_t g = ((uint64_t)n + kBuildThreads * 8 - 1) / (kBuildThreads * 8);
     g = std::min<uint64_t>(std::max<uint64_t>(g, 1), (uint64_t)L.num_sms * 8);
-    k_key_range<<<(unsigned)g, kBuildThreads, 0, L.stream>>>(key, n, range);
-    count_launches(1);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_array_build(const Launch &L, const ColView &key, uint32_t n, int64_t lo, uint64_t span,
-                               uint32_t *slots, unsigned long long *dup) {
-    if (n == 0 || span == 0) return cudaSuccess;
-    uint64_t g = ((uint64_t)n + 255) / 256;
-    g = std::min<uint64_t>(g, (uint64_t)L.num_sms * 8);
-    k_array_build<<<(unsigned)g, 256, 0, L.stream>>>(key, n, lo, span, slots, dup);
-    count_launches(1);
+    k_key_range<<<(unsigned)g, kBuildThreads, 0, L.stream>>>(key, n, params);
+    k_array_prep<<<1, 1, 0, L.stream>>>(params, max_span);
+    g = std::min<uint64_t>(std::max<uint64_t>((max_span + 255) / 256, 1), (uint64_t)L.num_sms * 8);
+    k_array_fill<<<(unsigned)g, 256, 0, L.stream>>>(slots, params);
+    g = std::min<uint64_t>(((uint64_t)n + 255) / 256, (uint64_t)L.num_sms * 8);
+    k_array_build<<<(unsigned)g, 256, 0, L.stream>>>(key, n, slots, params);
+    count_launches(4);
     return cudaGetLastError();
 }
 

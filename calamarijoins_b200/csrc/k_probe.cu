@@ -1,9 +1,9 @@
 /*
  * k_probe.cu — hash probe and nested-loop join on sm_100a.
  *
- * Both are one persistent kernel over probe tiles of kTileRows rows:
+ * Both are one persistent kernel over probe tiles of 256 x kItems rows:
  *   - a CTA takes tiles from an atomic ticket;
- *   - each lane handles kProbeItems rows, one dependent chain each (key ->
+ *   - each lane handles kItems rows, one dependent chain each (key ->
  *     directory entry -> candidate tuples), kept short and register-light so
  *     that eight CTAs share an SM and their loads overlap;
  *   - for every match count it remembers the first matching build row, so
@@ -37,8 +37,8 @@ namespace {
 #define CJ_PROBE_MIN_BLOCKS 8
 #endif
 constexpr int kProbeThreads = 256;
-constexpr int kProbeItems = CJ_PROBE_ITEMS; /* rows per thread and tile pass            */
-constexpr uint32_t kTileRows = kProbeThreads * kProbeItems;
+constexpr int kProbeItems = CJ_PROBE_ITEMS; /* rows per thread (hash, nested loop)      */
+constexpr uint32_t kTileRows = kProbeThreads * kProbeItems; /* grouped kernel's tile */
 constexpr int kProbeMinBlocks = CJ_PROBE_MIN_BLOCKS; /* 8 x 256 threads = 64 warps/SM */
 
 struct TileSched {
@@ -59,6 +59,9 @@ CJ_DEV void put_key(const MatchOut &out, unsigned long long pos, int64_t key) {
  * (31..16, saturated at 0xFFFF: then the next entry's start bounds them) and
  * the OR of their Bloom tags (15..0). */
 template <typename KB> struct HashMatcher {
+    static constexpr bool kAtMostOne = false;
+    static constexpr int kItems = kProbeItems;
+    CJ_DEV HashMatcher resolved() const { return *this; }
     HashTableView<KB> ht;
     const uint16_t *g_bloom;
     struct Shared {
@@ -111,17 +114,26 @@ template <typename KB> struct HashMatcher {
  * sets *dup, and a probe launched over such a table does nothing (the
  * caller then builds the hash table instead). */
 struct ArrayMatcher {
+    static constexpr bool kAtMostOne = true; /* unique keys: 0 or 1 match per row */
+    static constexpr int kItems = 4;         /* one light chain per row: 4 rows per thread
+                                                fit 32 registers (387 us vs 434 us for 2
+                                                on 64M probe rows) */
     const uint32_t *slots;
-    int64_t lo;
-    uint64_t span;
-    const unsigned long long *dup;
+    const unsigned long long *params; /* [3] unusable, [4] lo, [5] span */
+    uint64_t lo = 0, span = 0;        /* read from params by resolved() */
     struct Shared {
         uint32_t unused;
     };
-    CJ_DEV bool skip() const { return *dup != 0ull; }
+    CJ_DEV bool skip() const { return params[3] != 0ull; }
+    CJ_DEV ArrayMatcher resolved() const {
+        ArrayMatcher m = *this;
+        m.lo = params[4];
+        m.span = params[5];
+        return m;
+    }
     CJ_DEV void init(Shared &) const {}
     CJ_DEV uint32_t count(const Shared &, int64_t key, uint32_t &first) const {
-        const uint64_t off = (uint64_t)key - (uint64_t)lo; /* keys below lo wrap past span */
+        const uint64_t off = (uint64_t)key - lo; /* keys below lo wrap past span */
         if (off >= span) return 0;
         const uint32_t r = __ldg(slots + off);
         if (r == kArrayEmpty) return 0;
@@ -140,6 +152,9 @@ struct ArrayMatcher {
 };
 
 struct LoopMatcher {
+    static constexpr bool kAtMostOne = false;
+    static constexpr int kItems = kProbeItems;
+    CJ_DEV LoopMatcher resolved() const { return *this; }
     const int64_t *g_keys;
     const uint32_t *g_rids;
     const uint32_t *g_count;
@@ -182,10 +197,11 @@ struct LoopMatcher {
 
 /* Per-row state between the counting and the writing pass lives in shared
  * memory, not registers, so the kernel fits 32 registers (8 CTAs per SM). */
-struct ProbeSmem {
-    uint32_t first[kTileRows]; /* first matching build row (one-match rows) */
-    int64_t key[kTileRows];    /* the row's key, when the matches carry it   */
-    uint32_t pre[kTileRows];   /* row's match offset within its warp        */
+template <int kItemsT> struct ProbeSmemT {
+    static constexpr uint32_t kRows = kProbeThreads * kItemsT;
+    uint32_t first[kRows]; /* first matching build row (one-match rows) */
+    int64_t key[kRows];    /* the row's key, when the matches carry it   */
+    uint32_t pre[kRows];   /* row's match offset within its warp        */
     uint32_t warp[kProbeThreads / 32 + 1];
     uint32_t tile;
     uint32_t task;
@@ -195,24 +211,32 @@ struct ProbeSmem {
 /* One probe tile. Block-wide. */
 template <class M>
 CJ_DEV void probe_tile(const ColView &pkey, uint32_t n, const M &m, const typename M::Shared &sh,
-                       const MatchOut &out, uint32_t tile, ProbeSmem &ps) {
+                       const MatchOut &out, uint32_t tile, ProbeSmemT<M::kItems> &ps) {
+    constexpr int kItems = M::kItems;
+    constexpr uint32_t kRows = ProbeSmemT<M::kItems>::kRows;
     const uint32_t warp = threadIdx.x >> 5, lane = lane_id();
-    const uint64_t row0 = (uint64_t)tile * kTileRows + (uint64_t)warp * 32 * kProbeItems;
+    const uint64_t row0 = (uint64_t)tile * kRows + (uint64_t)warp * 32 * kItems;
     uint32_t kinds = 0; /* 2 bits per item: 0 none, 1 one match, 2 more */
     uint32_t wrun = 0;
 #pragma unroll
-    for (int it = 0; it < kProbeItems; ++it) {
+    for (int it = 0; it < kItems; ++it) {
         const uint64_t i = row0 + (uint64_t)it * 32 + lane;
-        const uint32_t si = warp * 32 * kProbeItems + it * 32 + lane;
+        const uint32_t si = warp * 32 * kItems + it * 32 + lane;
         int64_t key;
         uint32_t c = 0, first = 0;
         if (i < n && load_key_stream(pkey, (uint32_t)i, &key)) c = m.count(sh, key, first);
         kinds |= (c == 0 ? 0u : (c == 1 ? 1u : 2u)) << (2 * it);
-        const uint32_t incl = warp_inclusive_scan(c);
         ps.first[si] = first;
         if (out.keys && c == 1) ps.key[si] = key;
-        ps.pre[si] = wrun + incl - c;
-        wrun += __shfl_sync(0xffffffffu, incl, 31);
+        if (M::kAtMostOne) {
+            const uint32_t ball = __ballot_sync(0xffffffffu, c != 0);
+            ps.pre[si] = wrun + __popc(ball & lanemask_lt());
+            wrun += __popc(ball);
+        } else {
+            const uint32_t incl = warp_inclusive_scan(c);
+            ps.pre[si] = wrun + incl - c;
+            wrun += __shfl_sync(0xffffffffu, incl, 31);
+        }
     }
     if (lane == 0) ps.warp[warp] = wrun;
     __syncthreads();
@@ -227,11 +251,11 @@ CJ_DEV void probe_tile(const ColView &pkey, uint32_t n, const M &m, const typena
     __syncthreads();
     const unsigned long long base = ps.base + ps.warp[warp];
 #pragma unroll
-    for (int it = 0; it < kProbeItems; ++it) {
+    for (int it = 0; it < kItems; ++it) {
         const uint32_t k = (kinds >> (2 * it)) & 3u;
         if (!k) continue;
         const uint32_t prow = (uint32_t)(row0 + (uint64_t)it * 32 + lane);
-        const uint32_t si = warp * 32 * kProbeItems + it * 32 + lane;
+        const uint32_t si = warp * 32 * kItems + it * 32 + lane;
         const unsigned long long pos = base + ps.pre[si];
         if (k == 1) {
             if (pos < out.capacity) {
@@ -250,10 +274,12 @@ CJ_DEV void probe_tile(const ColView &pkey, uint32_t n, const M &m, const typena
 
 template <class M>
 __global__ void __launch_bounds__(kProbeThreads, kProbeMinBlocks)
-    k_probe_tiles(ColView pkey, uint32_t n, M m, MatchOut out, TileSched ts) {
+    k_probe_tiles(ColView pkey_arg, uint32_t n, M m_arg, MatchOut out, TileSched ts) {
     __shared__ typename M::Shared sh;
-    __shared__ ProbeSmem ps;
-    if (m.skip()) return;
+    __shared__ ProbeSmemT<M::kItems> ps;
+    if (m_arg.skip()) return;
+    const M m = m_arg.resolved();
+    const ColView pkey = resolve_view(pkey_arg);
     m.init(sh);
     __syncthreads();
     for (;;) {
@@ -278,7 +304,9 @@ __global__ void __launch_bounds__(kProbeThreads, kProbeMinBlocks)
     k_probe_grouped(const ProbeTask *__restrict__ tasks, uint32_t ntasks, uint32_t total_tiles,
                     unsigned int *ticket, const uint16_t *__restrict__ g_bloom) {
     __shared__ GroupedShared sh;
-    __shared__ ProbeSmem ps;
+    __shared__ ProbeSmemT<kProbeItems> ps;
+    static_assert(HashMatcher<int32_t>::kItems == kProbeItems && LoopMatcher::kItems == kProbeItems,
+                  "the grouped kernel's tiles have kTileRows rows");
     __shared__ uint32_t loaded_task;
     if (threadIdx.x == 0) loaded_task = 0xffffffffu;
     load_bloom(sh.h.bloom, g_bloom);
@@ -367,7 +395,7 @@ template <class M>
 cudaError_t run_tiles(const Launch &L, const ColView &pkey, uint32_t n, const M &m, const MatchOut &out,
                       void *sched_mem) {
     TileSched ts;
-    ts.num_tiles = (n + kTileRows - 1) / kTileRows;
+    ts.num_tiles = (n + ProbeSmemT<M::kItems>::kRows - 1) / ProbeSmemT<M::kItems>::kRows;
     ts.ticket = reinterpret_cast<unsigned int *>(sched_mem);
     cudaError_t e = cudaMemsetAsync(sched_mem, 0, sizeof(unsigned int), L.stream);
     if (e != cudaSuccess) return e;
@@ -402,9 +430,8 @@ cudaError_t launch_probe_tiles_hash(const Launch &L, const ColView &pkey, uint32
 }
 
 cudaError_t launch_probe_tiles_array(const Launch &L, const ColView &pkey, uint32_t n_probe, const uint32_t *slots,
-                                     int64_t lo, uint64_t span, const unsigned long long *dup, const MatchOut &out,
-                                     void *sched_mem) {
-    ArrayMatcher m{slots, lo, span, dup};
+                                     const unsigned long long *params, const MatchOut &out, void *sched_mem) {
+    ArrayMatcher m{slots, params};
     return run_tiles(L, pkey, n_probe, m, out, sched_mem);
 }
 
