@@ -70,6 +70,13 @@ int cj_context_set_option(cj_context *ctx, int32_t option, int64_t value) {
         if (value < 0 || value > 64) return set_error(CJ_ERR_INVALID_ARGUMENT, "dense key factor in [0, 64]");
         ctx->opt.dense_keys = value;
         break;
+    case CJ_OPT_BUFFER_CACHE_BYTES:
+        if (value < 0) return set_error(CJ_ERR_INVALID_ARGUMENT, "cache bytes must be >= 0");
+        if (ctx->pool && !ctx->owns_pool && value) return set_error(CJ_ERR_INVALID_ARGUMENT, "server workers keep no cache");
+        ctx->opt.buffer_cache_bytes = value;
+        set_device(ctx);
+        ctx->trim_buffers();
+        break;
     default: return set_error(CJ_ERR_INVALID_ARGUMENT, "unknown option");
     }
     return CJ_OK;
@@ -85,6 +92,7 @@ int cj_context_get_option(const cj_context *ctx, int32_t option, int64_t *value)
     case CJ_OPT_VARCHAR_TILE_ROWS: *value = ctx->opt.varchar_tile_rows; break;
     case CJ_OPT_CTAS_PER_SM: *value = ctx->opt.ctas_per_sm; break;
     case CJ_OPT_DENSE_KEYS: *value = ctx->opt.dense_keys; break;
+    case CJ_OPT_BUFFER_CACHE_BYTES: *value = ctx->opt.buffer_cache_bytes; break;
     default: return set_error(CJ_ERR_INVALID_ARGUMENT, "unknown option");
     }
     return CJ_OK;

@@ -35,7 +35,35 @@ void check_cuda(cudaError_t e, const char *what) {
 }
 
 DevBuf::~DevBuf() {
-    if (ptr && ctx) cudaFreeAsync(ptr, ctx->stream);
+    if (ptr && ctx) ctx->release(ptr, cls);
+}
+
+/* Four size classes per power of two (at most 25 % above the request),
+ * 256 bytes at least. */
+static size_t device_class(size_t bytes) {
+    if (bytes <= 256) return 256;
+    int l = 63 - __builtin_clzll((unsigned long long)bytes - 1); /* 2^l < bytes <= 2^(l+1) */
+    const size_t quarter = (size_t)1 << (l > 2 ? l - 2 : 0);
+    return (bytes + quarter - 1) / quarter * quarter;
+}
+
+void Context::release(void *p, size_t c) {
+    {
+        std::lock_guard<std::mutex> g(dev_mu);
+        if (opt.buffer_cache_bytes > 0 && dev_cached + c <= (size_t)opt.buffer_cache_bytes) {
+            dev_free.emplace(c, p);
+            dev_cached += c;
+            return;
+        }
+    }
+    cudaFreeAsync(p, stream);
+}
+
+void Context::trim_buffers() {
+    std::lock_guard<std::mutex> g(dev_mu);
+    for (auto &kv : dev_free) cudaFreeAsync(kv.second, stream);
+    dev_free.clear();
+    dev_cached = 0;
 }
 
 PinnedBlock::~PinnedBlock() {
@@ -49,8 +77,26 @@ DevPtr Context::alloc(size_t bytes) {
     b->ctx = this;
     b->bytes = bytes;
     if (bytes == 0) return b;
-    size_t req = (bytes + 255) & ~size_t(255);
-    cudaError_t e = cudaMallocFromPoolAsync(&b->ptr, req, pool, stream);
+    const size_t cls = device_class(bytes);
+    b->cls = cls;
+    {
+        std::lock_guard<std::mutex> g(dev_mu);
+        auto it = dev_free.find(cls);
+        if (it != dev_free.end()) {
+            b->ptr = it->second;
+            dev_free.erase(it);
+            dev_cached -= cls;
+            return b;
+        }
+    }
+    cudaError_t e = cudaMallocFromPoolAsync(&b->ptr, cls, pool, stream);
+    if (e != cudaSuccess) {
+        /* cached buffers of other sizes go back to the pool, then retry */
+        cudaGetLastError();
+        trim_buffers();
+        cudaStreamSynchronize(stream);
+        e = cudaMallocFromPoolAsync(&b->ptr, cls, pool, stream);
+    }
     if (e != cudaSuccess) {
         b->ptr = nullptr;
         cudaGetLastError();
@@ -140,6 +186,7 @@ void Context::resolve_profile() {
 }
 
 Context::~Context() {
+    trim_buffers();
     if (h2d_stream) cudaStreamSynchronize(h2d_stream);
     if (d2h_stream) cudaStreamSynchronize(d2h_stream);
     if (stream) cudaStreamSynchronize(stream);
@@ -230,6 +277,8 @@ Context *create_context(int device, cudaMemPool_t shared_pool) {
     c->opt.varchar_tile_rows = env_opt("CJ_VARCHAR_TILE_ROWS", c->opt.varchar_tile_rows);
     c->opt.ctas_per_sm = env_opt("CJ_CTAS_PER_SM", c->opt.ctas_per_sm);
     c->opt.dense_keys = std::max<int64_t>(0, std::min<int64_t>(64, env_opt("CJ_DENSE_KEYS", c->opt.dense_keys)));
+    c->opt.buffer_cache_bytes = std::max<int64_t>(0, env_opt("CJ_BUFFER_CACHE_BYTES", c->opt.buffer_cache_bytes));
+    if (shared_pool) c->opt.buffer_cache_bytes = 0; /* contexts sharing a pool share through it */
     return c.release();
 }
 

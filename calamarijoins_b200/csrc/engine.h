@@ -45,15 +45,17 @@ struct Options {
     int64_t varchar_tile_rows = 2048;
     int64_t ctas_per_sm = 0;
     int64_t dense_keys = 2; /* max key span / build rows for a direct-mapped table; 0 = off */
+    int64_t buffer_cache_bytes = 16ll << 30; /* freed device buffers kept for reuse */
 };
 
 struct Context;
 
-/* A stream-ordered device allocation from the context's pool. */
+/* A device allocation of the context, ordered on its kernel stream. */
 struct DevBuf {
     Context *ctx = nullptr;
     void *ptr = nullptr;
     size_t bytes = 0;
+    size_t cls = 0; /* bytes actually held (size class) */
     ~DevBuf();
     template <typename T> T *as() const { return reinterpret_cast<T *>(ptr); }
 };
@@ -93,6 +95,16 @@ struct Context {
     /* pinned pool: size class -> free blocks */
     std::multimap<size_t, void *> pinned_free;
     std::mutex pinned_mu;
+
+    /* Freed device buffers by size class. Every use of a context buffer is
+     * ordered on the kernel stream (copy streams wait on it and it waits on
+     * them), so a buffer freed at some point of that order can serve a
+     * later allocation at once: no driver call in the steady state. */
+    std::multimap<size_t, void *> dev_free;
+    size_t dev_cached = 0;
+    std::mutex dev_mu;
+    void release(void *ptr, size_t cls);
+    void trim_buffers(); /* returns every cached buffer to the pool */
 
     /* profiler */
     std::vector<KernelProfile> profile;

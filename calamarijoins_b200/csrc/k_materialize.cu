@@ -87,6 +87,38 @@ CJ_DEV void write_fixed_page(const ColView &col, uint64_t rows, uint32_t R, uint
     const uint64_t r0 = pg * R;
     const uint32_t nr = (uint32_t)min((uint64_t)R, rows - r0);
 
+    if (sizeof(T) == 4 && !col.rid_a && !col.rid_b && !col.valid && !col.col_flags) {
+        /* A dense NULL-free INT32 array (the join keys the probe emitted):
+         * a plain copy. A page starts at row pg x 1984, a multiple of 4, so
+         * each thread moves 4 values with one 16-byte load. */
+        uint8_t *dst = out + pg * kPageSize;
+        const int32_t *src = reinterpret_cast<const int32_t *>(col.values) + r0;
+        int32_t *dv = reinterpret_cast<int32_t *>(dst + DB);
+        for (uint32_t q = threadIdx.x; q * 4 < nr; q += blockDim.x) {
+            const uint32_t r = q * 4;
+            if (r + 4 <= nr) {
+                const int4 v = __ldcs(reinterpret_cast<const int4 *>(src) + q);
+                __stcs(dv + r, v.x);
+                __stcs(dv + r + 1, v.y);
+                __stcs(dv + r + 2, v.z);
+                __stcs(dv + r + 3, v.w);
+            } else {
+                for (uint32_t k = r; k < nr; ++k) __stcs(dv + k, __ldcs(src + k));
+            }
+        }
+        if (threadIdx.x == 0) __stcs(reinterpret_cast<unsigned int *>(dst), nr * 0x10001u);
+        const uint32_t bm_bytes = (nr + 7) / 8, bm0 = kPageSize - bm_bytes;
+        for (uint32_t b = DB + nr * 4u + threadIdx.x; b < kPageSize; b += blockDim.x) {
+            uint8_t v = 0;
+            if (b >= bm0) {
+                const uint32_t i = b - bm0;
+                v = (i + 1) * 8 <= nr ? 0xFFu : (uint8_t)((1u << (nr - i * 8)) - 1u);
+            }
+            dst[b] = v;
+        }
+        return;
+    }
+
     uint32_t br[kSlabs];
 #pragma unroll
     for (int k = 0; k < kSlabs; ++k) {

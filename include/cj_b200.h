@@ -194,12 +194,16 @@ typedef enum cj_option {
     CJ_OPT_VARCHAR_TILE_ROWS = 4,     /* rows per VARCHAR page-packing tile  */
     CJ_OPT_CTAS_PER_SM = 5,           /* resident CTAs per SM for persistent
                                          grids; 0 = auto                    */
-    CJ_OPT_DENSE_KEYS = 6             /* a build side whose non-NULL keys are
+    CJ_OPT_DENSE_KEYS = 6,            /* a build side whose non-NULL keys are
                                          unique and span at most this many
                                          times its row count uses a direct-
                                          mapped table (slot = key - min)
                                          instead of the hash table; same
                                          results; 0 = off; default 2        */
+    CJ_OPT_BUFFER_CACHE_BYTES = 7     /* device buffers freed by a plan are
+                                         kept for the next one up to this
+                                         many bytes (default 16 GiB; 0 = off;
+                                         always 0 for server workers)       */
 } cj_option;
 int cj_context_set_option(cj_context *ctx, int32_t option, int64_t value);
 int cj_context_get_option(const cj_context *ctx, int32_t option, int64_t *value);

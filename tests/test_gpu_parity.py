@@ -410,6 +410,33 @@ def test_invalid_plans(gpu_ctx):
     assert e.value.status == 6
 
 
+def test_buffer_cache_reuse_and_trim(gpu_ctx):
+    """Buffers freed by one plan serve the next (no growth over repeated
+    plans, same results); turning the cache off hands them back to the
+    pool."""
+    plan = join2(50_000, 400_000, seed=13, build_payload=(L, V), probe_payload=(F,))
+    want = run_oracle(plan)
+    r, _ = run_product(plan, gpu_ctx)
+    assert_same(r, want)
+    used1, _ = gpu_ctx.memory()
+    for _ in range(3):
+        r, _ = run_product(plan, gpu_ctx)
+        assert_same(r, want)
+    used2, _ = gpu_ctx.memory()
+    assert used2 == used1
+    default = gpu_ctx.get_option(_lib.CJ_OPT_BUFFER_CACHE_BYTES)
+    try:
+        gpu_ctx.set_option(_lib.CJ_OPT_BUFFER_CACHE_BYTES, 0)
+        used3, _ = gpu_ctx.memory()
+        assert used3 < used2
+        r, _ = run_product(plan, gpu_ctx)
+        assert_same(r, want)
+        used4, _ = gpu_ctx.memory()
+        assert used4 <= used3
+    finally:
+        gpu_ctx.set_option(_lib.CJ_OPT_BUFFER_CACHE_BYTES, default)
+
+
 def test_memory_returns_to_pool(gpu_ctx):
     plan = join2(10000, 100000, seed=12, build_payload=(V,))
     run_product(plan, gpu_ctx)
