@@ -190,8 +190,9 @@ def algorithmic_bytes(kernel: str, st: dict, plan_info: dict):
     if kernel == "probe_array":
         # probe keys (4 B + validity bit), the direct-mapped table (4 B per
         # slot; the C2 build keys are a permutation of [0, rows), so slots =
-        # build rows) once, 2 x 4 B row ids per match
-        return npr * (4 + 1 / 8) + nb * 4 + m * 8
+        # build rows) once; per match 2 x 4 B row ids and the 4 B key the
+        # probe emits for the root's key columns
+        return npr * (4 + 1 / 8) + nb * 4 + m * 12
     if kernel == "write_pages_int32":
         # per output row: 4 B match row id + 4 B value + validity bit read; page bytes written
         pages = (m + 1983) // 1984
