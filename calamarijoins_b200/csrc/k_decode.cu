@@ -175,10 +175,47 @@ CJ_DEV void decode_fixed_page(const uint8_t *__restrict__ pages, uint64_t p, uin
     }
     const T *vals = reinterpret_cast<const T *>(pg + DB);
     const bool dense = nr == nv;
-    if (!dense) load_page_bitmap(pg, nr, sm.bm, sm.pre, sm.wbuf);
+    if (!dense) {
+        load_page_bitmap(pg, nr, sm.bm, sm.pre, sm.wbuf);
+        /* Sparse page: a thread takes 4 consecutive rows, whose non-NULL
+         * values are consecutive in the page (one bitmap word and its
+         * prefix give the first index), and stores the 4 rows at once when
+         * the page starts on a multiple of 4 rows. */
+        const bool vec = sizeof(T) == 4 && (rs & 3u) == 0;
+        for (uint32_t g = threadIdx.x; g * 4 < nr; g += blockDim.x) {
+            const uint32_t r = g * 4, w = r >> 5, sh = r & 31u;
+            const uint32_t word = sm.bm[w]; /* bits past n_rows are clear */
+            uint32_t idx = sm.pre[w] + __popc(word & ((1u << sh) - 1u));
+            const uint32_t nib = (word >> sh) & 0xFu;
+            T v[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                v[k] = T(0);
+                if ((nib >> k) & 1u) {
+                    if (idx >= nv) atomicOr(err, DEV_ERR_PAGE_HEADER); /* bitmap holds > n_values bits */
+                    else v[k] = __ldcs(vals + idx);
+                    ++idx;
+                }
+            }
+            bool done = false;
+            if constexpr (sizeof(T) == 4) {
+                if (vec && r + 4 <= nr) {
+                    *reinterpret_cast<int4 *>(values + rs + r) = make_int4(v[0], v[1], v[2], v[3]);
+                    done = true;
+                }
+            }
+            if (!done) {
+#pragma unroll
+                for (int k = 0; k < 4; ++k)
+                    if (r + k < nr) values[rs + r + k] = v[k];
+            }
+        }
+        write_validity(false, sm.bm, nr, rs, valid);
+        __syncthreads();
+        return;
+    }
     /* All loads of a chunk are issued before any store: a full page (1984 /
-     * 1007 rows) is one chunk, so it costs one DRAM round trip. Only a
-     * sparse page with more rows than that takes several. */
+     * 1007 rows) is one chunk, so it costs one DRAM round trip. */
     constexpr int kSlabs =
         (int)(((sizeof(T) == 4 ? kRowsPerPageInt32 : kRowsPerPage8B) + kDecodeThreads - 1) / kDecodeThreads);
     for (uint32_t base = 0; base < nr; base += kSlabs * kDecodeThreads) {
