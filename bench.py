@@ -27,6 +27,23 @@ cpu_baseline the reference's own execute() (oracle/_ref, all host threads)
 --impl reference runs only that CPU reference (rank 0; other ranks exit).
 Multi-GPU (torchrun): independent replicas, one per GPU, no collective on
 the data path ("scaling": "weak").
+
+Other workloads (not the default line; --workload):
+  c1  100K x 1M join (INT32 build payload, INT64 probe payload), same
+      measurements as the default line.
+  c3  6-way left-deep join: a 36M-row fact table with 5 foreign keys into
+      dimensions of 2.5K-4.2M rows (pre-filtered to 10-40 %), VARCHAR
+      outputs (lengths log-normal, mean 20 B, 0.01 % long strings);
+      metric fact rows/s.
+  c4  256 seeded 2-4-way INT32 plans (builds log-uniform 10-1e6, probes
+      1e3-1e7): plans/s through cj_execute_batch, beside a loop of
+      cj_execute over the same plans and the reference's execute() on
+      the host cores; host pages in, host pages out.
+  c5  the server (cj_server_*, 4 worker streams, 150 GB admission budget)
+      under Poisson arrivals at several rates over a pool of 32 2-16-way
+      plans (probes 1e4-3e6 rows) with INT32 / INT64 keys and 10 % VARCHAR
+      outputs; a client thread takes and frees each result as it
+      completes: p50 / p99 latency and plans/s per rate.
 """
 from __future__ import annotations
 
@@ -48,6 +65,23 @@ UNIT = "rows/s"
 WORKLOAD = ("C2: build 4,000,000 unique shuffled INT32 keys + INT64 payload; probe 64,000,000 rows, "
             "INT32 FK Zipf(0.8) over build keys, 30% outside the build domain, 2% NULL, + FP64 payload; "
             "output build key, build INT64, probe key, probe FP64 (2 INT32 + INT64 + FP64)")
+WORKLOADS = {
+    "c2": {"metric": METRIC, "unit": UNIT, "desc": WORKLOAD, "units": "probe rows"},
+    "c1": {"metric": "probe rows/s, 100K x 1M INT32 equi-join (plain execute)", "unit": UNIT,
+           "desc": ("C1: build 100,000 unique shuffled INT32 keys + INT32 payload; probe 1,000,000 rows, INT32 FK "
+                    "Zipf(1.0), 5% NULL, + INT64 payload; output build key, build payload, probe payload"),
+           "units": "probe rows"},
+    "c3": {"metric": "fact rows/s, 6-way join of a 36M-row fact table (plain execute)", "unit": UNIT,
+           "desc": ("C3: fact 36,000,000 rows x 5 INT32 FKs (Zipf 0.5-1.2) into dimensions of 2,500 / 130,000 / "
+                    "1,200,000 / 2,500,000 / 4,200,000 rows kept at 40/40/30/20/10 %; outputs the fact's first FK, "
+                    "a fact VARCHAR and every dimension's VARCHAR (log-normal lengths, 0.01 % long strings)"),
+           "units": "fact rows"},
+}
+C4_PLANS, C4_SEED = 256, 404
+C5_RATES = (50, 200, 1000, 2000)
+for _k, _v in WORKLOADS.items():
+    _v["name"] = _k
+WL = WORKLOADS["c2"]
 
 
 def rank_info():
@@ -207,9 +241,18 @@ def algorithmic_bytes(kernel: str, st: dict, plan_info: dict):
     return None
 
 
-def gen_workload(pinned: bool, scale: float, int32_standin: bool = False):
-    from calamarijoins_b200.datagen import config_c2, join2
+def gen_workload(pinned: bool, scale: float, int32_standin: bool = False, workload: str = None):
+    from calamarijoins_b200.datagen import config_c1, config_c2, config_c3, join2
     from calamarijoins_b200 import DataType
+    workload = workload or WL["name"]
+    if workload == "c1":
+        if int32_standin:
+            return join2(max(int(100_000 * scale), 16), max(int(1_000_000 * scale), 16), seed=101, zipf=1.0,
+                         probe_null=0.05, build_payload=(DataType.INT32,), probe_payload=(DataType.INT32,),
+                         output=[0, 1, 3], pinned=pinned)
+        return config_c1(scale=scale, pinned=pinned)
+    if workload == "c3":  # INT32 keys, VARCHAR without NULLs: the reference runs it as it is
+        return config_c3(scale=scale, pinned=pinned)
     if int32_standin:
         return join2(max(int(4_000_000 * scale), 16), max(int(64_000_000 * scale), 16), seed=202, zipf=0.8,
                      outside=0.30, probe_null=0.02, build_payload=(DataType.INT32,),
@@ -217,10 +260,16 @@ def gen_workload(pinned: bool, scale: float, int32_standin: bool = False):
     return config_c2(seed=202, scale=scale, pinned=pinned)
 
 
+def work_units(plan) -> int:
+    """Rows the metric counts: the probe side of the 2-table workloads, the
+    fact table of C3."""
+    return plan.inputs[0].num_rows if WL["name"] == "c3" else plan.inputs[1].num_rows
+
+
 def plan_info(plan):
     import math
     nb = plan.inputs[0].num_rows
-    npr = plan.inputs[1].num_rows
+    npr = work_units(plan)
     i32 = [c for t in plan.inputs for c in t.columns if int(c.type) == 0]
     return {"build_rows": nb, "probe_rows": npr, "slots": 1 << max(11, math.ceil(math.log2(max(nb, 1)))),
             "int32_pages": sum(c.num_pages for c in i32), "int32_cols": max(len(i32), 1)}
@@ -246,15 +295,28 @@ def ref_worker(threads: int, scale: float, warmup: int, steps: int) -> None:
     every variant carries its own worker-pool singleton)."""
     from calamarijoins_b200 import PlanDescriptor
     from oracle import oracle_api as oa
+    if WL["name"] == "c4":  # one pass = every plan of the batch, one after another
+        from calamarijoins_b200.datagen import batch_plans
+        descs = [PlanDescriptor(p) for p in batch_plans(C4_PLANS, seed=C4_SEED, scale=scale)]
+        ms = []
+        for i in range(max(warmup, 1) + steps):
+            t0 = time.perf_counter()
+            for d in descs:
+                oa.ref_execute(d, threads)
+            if i >= max(warmup, 1):
+                ms.append((time.perf_counter() - t0) * 1e3)
+        print(json.dumps({"threads": threads, "ms": statistics.median(ms), "probe_rows": len(descs), "build_rows": 0}))
+        return
     plan = gen_workload(False, scale, int32_standin=True)
     d = PlanDescriptor(plan)
+    units = work_units(plan)
     for _ in range(max(warmup, 1)):
         oa.ref_execute(d, threads)
     ms = []
     for _ in range(steps):
         _, w, _ = oa.ref_execute(d, threads)
         ms.append(w)
-    print(json.dumps({"threads": threads, "ms": statistics.median(ms), "probe_rows": plan.inputs[1].num_rows,
+    print(json.dumps({"threads": threads, "ms": statistics.median(ms), "probe_rows": units,
                       "build_rows": plan.inputs[0].num_rows}))
 
 
@@ -269,8 +331,8 @@ def time_reference(scale: float, warmup: int, steps: int, timeout_s: float = 900
     for t in cands:
         log(f"reference: {t} threads, scale {scale}")
         res = subprocess.run([sys.executable, os.path.abspath(__file__), "--ref-worker", str(t), "--scale", str(scale),
-                              "--warmup", str(warmup), "--steps", str(steps)], capture_output=True, text=True,
-                             timeout=timeout_s)
+                              "--warmup", str(warmup), "--steps", str(steps), "--workload", WL["name"]],
+                             capture_output=True, text=True, timeout=timeout_s)
         if res.returncode != 0:
             log(f"reference variant {t} failed: {res.stderr[-500:]}")
             continue
@@ -295,13 +357,13 @@ def run_reference(args):
         return 0
     npr = r["probe_rows"]
     val = npr / (r["ms"] / 1000.0)
-    sample = (f"C2 shape at scale {scale}: {r['build_rows']} x {npr} rows, INT32 stand-ins for the "
-              f"INT64/FP64 payloads (the reference cannot emit them); median of {args.steps} runs after "
+    sample = (f"{WL['name'].upper()} shape at scale {scale}: {r['build_rows']} x {npr} rows, INT32 stand-ins for "
+              f"any INT64/FP64 payloads (the reference cannot emit them); median of {args.steps} runs after "
               f"{max(args.warmup, 1)} warm-up; best of thread counts {sorted(r['all_ms'])} on {os.cpu_count()} CPUs")
-    line = {"impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": 0, "steps": args.steps,
+    line = {"impl": "reference", "metric": WL["metric"], "value": val, "unit": UNIT, "n_gpus": 0, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": r["ms"], "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "int32", "data": "synthetic",
-            "config": {"workload": WORKLOAD + " [reference: INT32 stand-in payloads]", "parallelism": "cpu threads"},
+            "config": {"workload": WL["desc"] + " [reference: INT32 stand-in payloads]", "parallelism": "cpu threads"},
             "cpu_baseline": {"value": val, "unit": UNIT, "cores": r["threads"], "kind": "reference",
                              "sample": sample},
             "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -436,16 +498,17 @@ def run_ours(args):
         if r is not None:
             snp = r["probe_rows"]
             cpu = {"value": snp / (r["ms"] / 1000.0), "unit": UNIT, "cores": r["threads"], "kind": "reference",
-                   "sample": (f"reference execute() (oracle/_ref) on the C2 shape at scale {args.cpu_scale} "
+                   "sample": (f"reference execute() (oracle/_ref) on the {WL['name'].upper()} shape at scale "
+                              f"{args.cpu_scale} "
                               f"({r['build_rows']} x {snp} rows) with INT32 stand-ins for the INT64/FP64 payloads; "
                               f"median of 3 runs after 1 warm-up; {r['threads']} threads (of {sorted(r['all_ms'])} "
                               f"tried) on {os.cpu_count()} host CPUs")}
     if rank == 0:
-        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        line = {"metric": WL["metric"], "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "int32", "data": "synthetic",
                 "step_ms": {"min": min(step_ms), "median": statistics.median(step_ms), "max": max(step_ms)},
-                "config": {"workload": WORKLOAD, "scale": args.scale,
+                "config": {"workload": WL["desc"], "scale": args.scale,
                            "inputs": "paged columns resident in HBM (device-resident cj_table)",
                            "l2": "inputs larger than L2 (1.1 GB of pages); no flush",
                            "parallelism": f"replicas x{world}",
@@ -464,6 +527,144 @@ def run_ours(args):
     return 0
 
 
+def run_batch(args):
+    """c4: plans/s of 256 plans, batched (cj_execute_batch) and looped
+    (cj_execute), host pages in and out; the reference's execute() over
+    the same plans on the host cores."""
+    import calamarijoins_b200 as cj
+    from calamarijoins_b200.datagen import batch_plans
+    ctx = cj.Context(0)
+    log("generating 256 plans")
+    plans = batch_plans(C4_PLANS, seed=C4_SEED, scale=args.scale, pinned=True)
+    descs = [cj.PlanDescriptor(p) for p in plans]
+    rows = sum(p.inputs[0].num_rows for p in plans)
+
+    def batched():
+        results, statuses, st = cj.execute_batch(plans, ctx, descs=descs)
+        assert all(x == 0 for x in statuses), statuses
+        for r in results:
+            r.free()
+        return st
+
+    def looped():
+        for p, d in zip(plans, descs):
+            r, _ = cj.execute_raw(p, ctx, 0, d)
+            r.free()
+
+    out = {}
+    for name, fn in (("batched", batched), ("looped", looped)):
+        log(f"{name}: warm-up")
+        for _ in range(args.warmup):
+            fn()
+        walls = []
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            fn()
+            walls.append(time.perf_counter() - t0)
+        out[name] = {"plans_per_s": C4_PLANS / statistics.mean(walls), "ms_per_pass": statistics.mean(walls) * 1e3,
+                     "pass_ms": {"min": min(walls) * 1e3, "median": statistics.median(walls) * 1e3,
+                                 "max": max(walls) * 1e3}}
+    st = batched()
+    ref = None
+    if not args.no_cpu_baseline:
+        r = time_reference(args.scale, 1, 3)
+        if r is not None:
+            ref = {"value": C4_PLANS / (r["ms"] / 1000.0), "unit": "plans/s", "cores": r["threads"],
+                   "kind": "reference", "sample": (f"the reference's execute() over the same {C4_PLANS} plans one "
+                                                   f"after another, median of 3 passes after 1 warm-up; best of "
+                                                   f"thread counts {sorted(r['all_ms'])} on {os.cpu_count()} CPUs")}
+    line = {"metric": "plans/s, 256 batched 2-4-way INT32 plans", "value": out["batched"]["plans_per_s"],
+            "unit": "plans/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": out["batched"]["ms_per_pass"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+            "config": {"workload": ("C4: 256 seeded 2-4-way INT32 chain plans, builds log-uniform 10-1e6 rows, "
+                                    "probes 1e3-1e7 rows; host pages in, host pages out"), "scale": args.scale,
+                       "fact_rows_total": rows},
+            "batched": out["batched"], "looped": out["looped"],
+            "batch_stats": {k: st[k] for k in ("num_levels", "num_joins", "kernel_launches", "syncs")},
+            "cpu_baseline": ref}
+    print(json.dumps(line))
+    ctx.close()
+    return 0
+
+
+def run_serve(args):
+    """c5: the server under Poisson arrivals over a pool of plans: p50 / p99
+    latency (submit to completion) and plans/s per arrival rate. A client
+    thread takes and frees each result as it completes."""
+    import queue
+    import numpy as np
+    import calamarijoins_b200 as cj
+    from calamarijoins_b200 import DataType
+    from calamarijoins_b200.datagen import chain_plan
+    rng = np.random.default_rng(505)
+    log("generating the plan pool")
+    pool = []
+    for i in range(32):
+        ways = int(rng.integers(2, 17))
+        nprobe = int(10 ** rng.uniform(4, 4 + 2.5 * max(args.scale, 0.01) ** 0.25))
+        pool.append(chain_plan(ways, nprobe, rng, max_build=max(int(1_000_000 * args.scale), 1000),
+                               key_types=[DataType.INT32 if rng.random() < 0.7 else DataType.INT64
+                                          for _ in range(ways - 1)],
+                               varchar_frac=0.1, pinned=True))
+    descs = [cj.PlanDescriptor(p) for p in pool]
+    srv = cj.Server(device=0, slots=4, memory_budget=150 << 30)
+    try:
+        log("warm-up")
+        for d in descs:
+            r, _ = srv.wait(srv.submit(d))
+            r.free()
+        srv.stats(reset=True)
+        per_rate = []
+        for lam in C5_RATES:
+            n = int(min(max(lam * 4, 100), 2000))
+            gaps = rng.exponential(1.0 / lam, n)
+            order = rng.integers(0, len(descs), n)
+            log(f"rate {lam}/s: {n} plans")
+            q = queue.Queue()
+
+            def consume():
+                while True:
+                    t = q.get()
+                    if t is None:
+                        return
+                    r, _ = srv.wait(t)
+                    r.free()
+            th = threading.Thread(target=consume)
+            th.start()
+            t0 = time.perf_counter()
+            at = 0.0
+            for g, k in zip(gaps, order):
+                at += g
+                d = at - (time.perf_counter() - t0)
+                if d > 0:
+                    time.sleep(d)
+                q.put(srv.submit(descs[k]))
+            q.put(None)
+            th.join()
+            st = srv.stats(reset=True)
+            per_rate.append({"rate": lam, "plans": n, "p50_ms": st["p50_us"] / 1e3, "p99_ms": st["p99_us"] / 1e3,
+                             "mean_ms": st["mean_us"] / 1e3, "max_ms": st["max_us"] / 1e3,
+                             "plans_per_s": st["plans_per_s"], "failed": st["failed"], "rejected": st["rejected"],
+                             "peak_admitted_gb": st["peak_admitted_bytes"] / 1e9})
+    finally:
+        srv.close()
+    best = max(per_rate, key=lambda x: x["plans_per_s"])
+    line = {"metric": "served plans/s (Poisson arrivals), p50 / p99 latency", "value": best["plans_per_s"],
+            "unit": "plans/s", "n_gpus": 1, "steps": len(C5_RATES), "warmup": 1, "ms_per_step": None,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32/int64",
+            "data": "synthetic",
+            "config": {"workload": ("C5: pool of 32 seeded 2-16-way chain plans, 70 % INT32 / 30 % INT64 keys, "
+                                    "10 % VARCHAR outputs, probes log-uniform 1e4-3e6 rows, dimensions 10-1e6 rows, "
+                                    "4 worker streams, 150 GB admission budget; Poisson arrivals, each plan drawn "
+                                    "from the pool"), "scale": args.scale},
+            "rates": per_rate,
+            "cpu_baseline": {"unavailable": "the reference joins INT32 keys only (30 % of the pool has INT64 keys) "
+                                            "and has no serving front end"}}
+    print(json.dumps(line))
+    return 0
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -474,7 +675,11 @@ def main(argv=None):
     ap.add_argument("--cpu-scale", type=float, default=0.25, help="scale of the CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-worker", type=int, default=0, help=argparse.SUPPRESS)
+    ap.add_argument("--workload", choices=["c2", "c1", "c3", "c4", "c5"], default="c2",
+                    help="c2 (default): the headline line; the others: see the module docstring")
     args = ap.parse_args(argv)
+    global WL
+    WL = WORKLOADS.get(args.workload, {"name": args.workload})
     if args.ref_worker:
         ref_worker(args.ref_worker, args.scale, args.warmup, args.steps)
         return 0
@@ -483,7 +688,15 @@ def main(argv=None):
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
     if args.impl == "reference":
+        if args.workload in ("c4", "c5"):
+            print(json.dumps({"impl": "reference", "unavailable": "use --workload c2 (c4 and c5 report the "
+                                                                   "reference inside their own line)"}))
+            return 0
         return run_reference(args)
+    if args.workload == "c4":
+        return run_batch(args)
+    if args.workload == "c5":
+        return run_serve(args)
     return run_ours(args)
 
 

@@ -371,8 +371,10 @@ Relation Executor::exec_join(uint64_t node_idx, int depth, bool is_root, cj_resu
                  * out the key range and whether the table is usable; the
                  * host learns it at the probe's own synchronisation and then,
                  * if it was not, builds the hash table. */
-                const uint64_t max_span =
-                    std::min<uint64_t>((uint64_t)ctx.opt.dense_keys * B.rows, 0xFFFFFFFFull);
+                /* 4 bytes per slot: at 8 x rows, 32 B per build row, against
+                 * about 16-24 B for the hash table, for one random access
+                 * per probe row instead of two; at most 2^28 slots (1 GiB) */
+                const uint64_t max_span = std::min<uint64_t>((uint64_t)ctx.opt.dense_keys * B.rows, 1ull << 28);
                 ck(cudaMemsetAsync(d_params, 0xFF, 8, ctx.stream), "memset");
                 ck(cudaMemsetAsync(d_params + 1, 0, (kDirectParams - 1) * 8, ctx.stream), "memset");
                 slots = ctx.alloc(max_span * 4);

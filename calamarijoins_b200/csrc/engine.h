@@ -44,7 +44,7 @@ struct Options {
     int64_t block_threads = 0;
     int64_t varchar_tile_rows = 2048;
     int64_t ctas_per_sm = 0;
-    int64_t dense_keys = 2; /* max key span / build rows for a direct-mapped table; 0 = off */
+    int64_t dense_keys = 8; /* max key span / build rows for a direct-mapped table; 0 = off */
     int64_t buffer_cache_bytes = 16ll << 30; /* freed device buffers kept for reuse */
 };
 

@@ -196,10 +196,11 @@ typedef enum cj_option {
                                          grids; 0 = auto                    */
     CJ_OPT_DENSE_KEYS = 6,            /* a build side whose non-NULL keys are
                                          unique and span at most this many
-                                         times its row count uses a direct-
-                                         mapped table (slot = key - min)
-                                         instead of the hash table; same
-                                         results; 0 = off; default 2        */
+                                         times its row count (and 2^28
+                                         values) uses a direct-mapped table
+                                         (slot = key - min) instead of the
+                                         hash table; same results; 0 = off;
+                                         default 8                          */
     CJ_OPT_BUFFER_CACHE_BYTES = 7     /* device buffers freed by a plan are
                                          kept for the next one up to this
                                          many bytes (default 16 GiB; 0 = off;

@@ -208,7 +208,9 @@ def _direct_case(kind, rng):
         k = rng.permutation(50_000).astype(np.int64)
         k[123] = k[4567]
         return k, I
-    if kind == "sparse":  # span far above 2 x rows: hash table
+    if kind == "spread5":  # span about 5 x rows: direct at factor 8, hash at 2
+        return rng.choice(250_000, 50_000, replace=False).astype(np.int64), I
+    if kind == "sparse":  # span far above 8 x rows: hash table
         return rng.choice(1 << 30, 50_000, replace=False).astype(np.int64), I
     if kind == "extremes":  # INT32_MIN and INT32_MAX as keys: span 2^32
         k = rng.permutation(50_000).astype(np.int64)
@@ -217,12 +219,13 @@ def _direct_case(kind, rng):
     raise ValueError(kind)
 
 
-@pytest.mark.parametrize("kind,direct", [("dense_i32", 1), ("dense_i64", 1), ("dense_dups", 0), ("sparse", 0),
-                                         ("extremes", 0)])
-def test_direct_mapped_build(gpu_ctx, kind, direct):
-    """Unique build keys spread over at most twice the build rows take a
-    direct-mapped table; duplicates, wide spans and the option turned off
-    take the hash table. Every path gives the oracle's result."""
+@pytest.mark.parametrize("kind,direct2,direct8", [("dense_i32", 1, 1), ("dense_i64", 1, 1), ("dense_dups", 0, 0),
+                                                  ("spread5", 0, 1), ("sparse", 0, 0), ("extremes", 0, 0)])
+def test_direct_mapped_build(gpu_ctx, kind, direct2, direct8):
+    """Unique build keys spread over at most CJ_OPT_DENSE_KEYS times the
+    build rows take a direct-mapped table; duplicates, wider spans and the
+    option turned off take the hash table. Every path gives the oracle's
+    result."""
     rng = np.random.default_rng(5)
     bkeys, kt = _direct_case(kind, rng)
     nb, npr = len(bkeys), 300_000
@@ -246,15 +249,17 @@ def test_direct_mapped_build(gpu_ctx, kind, direct):
     plan.new_join_node(True, 0, 1, 0, 0, [(0, kt), (1, L), (2, kt), (3, F)])
     plan.root = 2
     want = run_oracle(plan)
+    default = gpu_ctx.get_option(_lib.CJ_OPT_DENSE_KEYS)
+    assert default == 8
     try:
-        for opt, expect in ((2, direct), (0, 0)):
+        for opt, expect in ((2, direct2), (8, direct8), (0, 0)):
             gpu_ctx.set_option(_lib.CJ_OPT_DENSE_KEYS, opt)
             r, st = run_product(plan, gpu_ctx)
             assert_same(r, want, f"{kind} dense_keys={opt}")
             assert st.exec["num_direct_joins"] == expect
             assert st.exec["num_hash_joins"] == 1
     finally:
-        gpu_ctx.set_option(_lib.CJ_OPT_DENSE_KEYS, 2)
+        gpu_ctx.set_option(_lib.CJ_OPT_DENSE_KEYS, default)
 
 
 def test_direct_mapped_all_null_build(gpu_ctx):
