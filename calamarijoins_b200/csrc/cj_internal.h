@@ -116,8 +116,11 @@ template <typename K> struct HashTableView {
 struct MatchOut {
     uint32_t *build_rids = nullptr; /* null: not collected (RIGHT_ONLY)  */
     uint32_t *probe_rids = nullptr; /* null: not collected (LEFT_ONLY)   */
-    void *keys = nullptr;           /* null, or the join key of every match
-                                       (key_bytes wide), beside the row ids */
+    uint8_t *key_pages = nullptr;   /* null, or the join key written straight
+                                       into 8 KiB result pages: value pos % R
+                                       of page pos / R (R = 1984 or 1007 by
+                                       key_bytes); launch_finish_dense_pages
+                                       adds headers and bitmaps */
     int32_t key_bytes = 4;
     unsigned long long capacity = 0;
     unsigned long long *counter = nullptr;
@@ -285,6 +288,11 @@ struct NlCollectTask {
     uint32_t *count;
 };
 cudaError_t launch_nl_collect_grouped(const Launch &L, const NlCollectTask *tasks_dev, uint32_t ntasks);
+
+/* Headers (n_rows = n_values), zero gaps and all-ones bitmaps of the
+ * ceil(rows / R) pages of a NULL-free fixed-width column whose values are
+ * already in place (R by type, as rows_per_page_fixed). */
+cudaError_t launch_finish_dense_pages(const Launch &L, uint8_t *pages, uint64_t rows, int32_t type);
 
 /* Intermediates: out[i] = src[idx[i]] */
 cudaError_t launch_gather_u32(const Launch &L, const uint32_t *src,

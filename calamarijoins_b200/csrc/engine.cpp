@@ -125,12 +125,12 @@ class Executor {
     /* An output column of the root: its relation column and the match row
      * ids that select its rows (null for a scan root). Decoded on use. */
     struct OutCol {
-        const Relation *rel; /* null: `fixed` is the column (dense, no NULL) */
+        const Relation *rel; /* null: the values are already in `pages` */
         RelCol col;
         const uint32_t *rid_a;
-        ColView fixed;
+        DevPtr pages; /* result pages written by the probe (no NULL) */
     };
-    ColView out_view(const OutCol &oc) { return oc.rel ? view(*oc.rel, oc.col, oc.rid_a) : oc.fixed; }
+    ColView out_view(const OutCol &oc) { return view(*oc.rel, oc.col, oc.rid_a); }
     cj_result *materialize(const std::vector<OutCol> &cols, const std::vector<int32_t> &types,
                            uint64_t rows);
     void ck(cudaError_t e, const char *what) { check_cuda(e, what); }
@@ -306,9 +306,9 @@ Relation Executor::exec_join(uint64_t node_idx, int depth, bool is_root, cj_resu
     stats.probe_rows += P.rows;
     uint64_t M = 0;
     /* At the root, outputs of the probe key (and of the build key, which is
-     * read through the probe side) come from the key the probe writes beside
-     * every match: the page writer copies them in order instead of gathering
-     * them through row ids. Matched keys are never NULL. */
+     * read through the probe side) are written by the probe itself, straight
+     * into their places in the result pages (matched keys are never NULL):
+     * no gather, no copy; every such column shares those pages. */
     bool emit_keys = false;
     if (is_root) {
         need_p = false;
@@ -389,11 +389,13 @@ Relation Executor::exec_join(uint64_t node_idx, int depth, bool is_root, cj_resu
         for (;;) {
             mb = need_b ? ctx.alloc(cap * 4) : nullptr;
             mp = need_p ? ctx.alloc(cap * 4) : nullptr;
-            mk = emit_keys ? ctx.alloc(cap * key_bytes) : nullptr;
+            /* the key columns' result pages, sized for the capacity */
+            const uint32_t key_rpp = rows_per_page_fixed(pk.type);
+            mk = emit_keys ? ctx.alloc((cap + key_rpp - 1) / key_rpp * kPageSize) : nullptr;
             MatchOut mo;
             mo.build_rids = mb ? mb->as<uint32_t>() : nullptr;
             mo.probe_rids = mp ? mp->as<uint32_t>() : nullptr;
-            mo.keys = mk ? mk->ptr : nullptr;
+            mo.key_pages = mk ? mk->as<uint8_t>() : nullptr;
             mo.key_bytes = key_bytes;
             mo.capacity = collect ? cap : 0;
             mo.counter = &ctx.d_status->counter;
@@ -442,11 +444,10 @@ Relation Executor::exec_join(uint64_t node_idx, int depth, bool is_root, cj_resu
         std::vector<OutCol> cols;
         std::vector<int32_t> types;
         for (auto &o : outs) {
-            OutCol oc{o.rel, o.col, nullptr, ColView{}};
+            OutCol oc{o.rel, o.col, nullptr, nullptr};
             if (o.from_keys) {
                 oc.rel = nullptr;
-                oc.fixed.values = mk ? mk->ptr : nullptr;
-                oc.fixed.type = o.col.type; /* == the probe key's type */
+                oc.pages = mk; /* o.col.type == the probe key's type */
             } else {
                 oc.rid_a = o.from_build ? (mb ? mb->as<uint32_t>() : nullptr) : (mp ? mp->as<uint32_t>() : nullptr);
             }
@@ -574,17 +575,30 @@ cj_result *Executor::materialize(const std::vector<OutCol> &cols, const std::vec
         }
         for (size_t c = 0; c < nc; ++c) {
             if (!rows) continue;
-            /* decoded here, not before the loop: the kernel stream waits for
-             * a column's upload only when its pages are written */
-            const ColView cv = out_view(cols[c]);
-            res->dev_pages[c] = ctx.alloc(res->num_pages[c] * kPageSize);
-            if (types[c] != CJ_VARCHAR) {
-                KScope ks(*this, types[c] == CJ_INT32 ? "write_pages_int32" : "write_pages_8byte");
-                ck(launch_write_fixed_pages(L, cv, rows, res->dev_pages[c]->as<uint8_t>()), "write_fixed");
+            if (cols[c].pages) {
+                /* values already in place: headers and bitmaps, once per
+                 * shared page array */
+                res->dev_pages[c] = cols[c].pages;
+                bool first = true;
+                for (size_t k = 0; k < c; ++k)
+                    if (cols[k].pages == cols[c].pages) first = false;
+                if (first) {
+                    KScope ks(*this, "finish_pages");
+                    ck(launch_finish_dense_pages(L, cols[c].pages->as<uint8_t>(), rows, types[c]), "finish_pages");
+                }
             } else {
-                KScope ks(*this, "varchar_write");
-                ck(launch_varchar_write(L, cv, rows, TR, vtemp[c]->ptr, res->dev_pages[c]->as<uint8_t>()),
-                   "varchar_write");
+                /* decoded here, not before the loop: the kernel stream waits
+                 * for a column's upload only when its pages are written */
+                const ColView cv = out_view(cols[c]);
+                res->dev_pages[c] = ctx.alloc(res->num_pages[c] * kPageSize);
+                if (types[c] != CJ_VARCHAR) {
+                    KScope ks(*this, types[c] == CJ_INT32 ? "write_pages_int32" : "write_pages_8byte");
+                    ck(launch_write_fixed_pages(L, cv, rows, res->dev_pages[c]->as<uint8_t>()), "write_fixed");
+                } else {
+                    KScope ks(*this, "varchar_write");
+                    ck(launch_varchar_write(L, cv, rows, TR, vtemp[c]->ptr, res->dev_pages[c]->as<uint8_t>()),
+                       "varchar_write");
+                }
             }
             const size_t bytes = res->num_pages[c] * kPageSize;
             if (to_host && bytes) {
@@ -627,7 +641,7 @@ cj_result *Executor::run(cj_exec_stats *st) {
         std::vector<OutCol> cols;
         std::vector<int32_t> types;
         for (auto &c : s.cols) {
-            cols.push_back({&s, c, nullptr, ColView{}});
+            cols.push_back({&s, c, nullptr, nullptr});
             types.push_back(c.type);
         }
         res = materialize(cols, types, s.rows);

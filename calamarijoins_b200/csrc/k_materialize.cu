@@ -87,37 +87,6 @@ CJ_DEV void write_fixed_page(const ColView &col, uint64_t rows, uint32_t R, uint
     const uint64_t r0 = pg * R;
     const uint32_t nr = (uint32_t)min((uint64_t)R, rows - r0);
 
-    if (sizeof(T) == 4 && !col.rid_a && !col.rid_b && !col.valid && !col.col_flags) {
-        /* A dense NULL-free INT32 array (the join keys the probe emitted):
-         * a plain copy. A page starts at row pg x 1984, a multiple of 4, so
-         * each thread moves 4 values with one 16-byte load. */
-        uint8_t *dst = out + pg * kPageSize;
-        const int32_t *src = reinterpret_cast<const int32_t *>(col.values) + r0;
-        int32_t *dv = reinterpret_cast<int32_t *>(dst + DB);
-        for (uint32_t q = threadIdx.x; q * 4 < nr; q += blockDim.x) {
-            const uint32_t r = q * 4;
-            if (r + 4 <= nr) {
-                const int4 v = __ldcs(reinterpret_cast<const int4 *>(src) + q);
-                __stcs(dv + r, v.x);
-                __stcs(dv + r + 1, v.y);
-                __stcs(dv + r + 2, v.z);
-                __stcs(dv + r + 3, v.w);
-            } else {
-                for (uint32_t k = r; k < nr; ++k) __stcs(dv + k, __ldcs(src + k));
-            }
-        }
-        if (threadIdx.x == 0) __stcs(reinterpret_cast<unsigned int *>(dst), nr * 0x10001u);
-        const uint32_t bm_bytes = (nr + 7) / 8, bm0 = kPageSize - bm_bytes;
-        for (uint32_t b = DB + nr * 4u + threadIdx.x; b < kPageSize; b += blockDim.x) {
-            uint8_t v = 0;
-            if (b >= bm0) {
-                const uint32_t i = b - bm0;
-                v = (i + 1) * 8 <= nr ? 0xFFu : (uint8_t)((1u << (nr - i * 8)) - 1u);
-            }
-            dst[b] = v;
-        }
-        return;
-    }
 
     uint32_t br[kSlabs];
 #pragma unroll
@@ -136,7 +105,7 @@ CJ_DEV void write_fixed_page(const ColView &col, uint64_t rows, uint32_t R, uint
     /* a column without NULLs needs no validity loads (one random load per
      * row instead of two when the row ids are random); a direct column is
      * read from its pages */
-    const bool all_valid = !col.valid || col_all_valid(col); /* no validity array: no NULL */
+    const bool all_valid = col_all_valid(col);
     const bool direct = col_direct(col);
 #pragma unroll
     for (int k = 0; k < kSlabs; ++k) {
@@ -235,6 +204,31 @@ __global__ void __launch_bounds__(kMatThreads, kMatMinBlocks)
     __shared__ PageSmem sm;
     zero_page(sm);
     for (uint64_t pg = blockIdx.x; pg < num_pages; pg += gridDim.x) write_fixed_page<T>(col, rows, R, pg, out, sm);
+}
+
+/* Finishes pages whose values are in place (a NULL-free column written by
+ * the probe): header, zero gap after the values, bitmap of nr ones. */
+template <typename T>
+__global__ void k_finish_dense_pages(uint8_t *__restrict__ pages, uint64_t rows, uint64_t num_pages) {
+    constexpr uint32_t R = sizeof(T) == 4 ? kRowsPerPageInt32 : kRowsPerPage8B;
+    constexpr uint32_t DB = sizeof(T) == 4 ? 4u : 8u;
+    for (uint64_t pg = blockIdx.x; pg < num_pages; pg += gridDim.x) {
+        uint8_t *dst = pages + pg * kPageSize;
+        const uint32_t nr = (uint32_t)min((uint64_t)R, rows - pg * R);
+        if (threadIdx.x == 0) {
+            if (DB == 8) __stcs(reinterpret_cast<unsigned long long *>(dst), (unsigned long long)nr * 0x10001ull);
+            else __stcs(reinterpret_cast<unsigned int *>(dst), nr * 0x10001u);
+        }
+        const uint32_t bm_bytes = (nr + 7) / 8, bm0 = kPageSize - bm_bytes;
+        for (uint32_t b = DB + nr * (uint32_t)sizeof(T) + threadIdx.x; b < kPageSize; b += blockDim.x) {
+            uint8_t v = 0;
+            if (b >= bm0) {
+                const uint32_t i = b - bm0;
+                v = (i + 1) * 8 <= nr ? 0xFFu : (uint8_t)((1u << (nr - i * 8)) - 1u);
+            }
+            dst[b] = v;
+        }
+    }
 }
 
 /* Grouped page writer: every fixed-width output column of a batch. */
@@ -549,6 +543,17 @@ cudaError_t launch_write_fixed_pages(const Launch &L, const ColView &col, uint64
         k_write_fixed<long long><<<(unsigned)g, kMatThreads, 0, L.stream>>>(col, rows, R, np, out);
         count_launches(1);
     }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_finish_dense_pages(const Launch &L, uint8_t *pages, uint64_t rows, int32_t type) {
+    if (rows == 0) return cudaSuccess;
+    const uint32_t R = rows_per_page_fixed(type);
+    const uint64_t np = (rows + R - 1) / R;
+    const unsigned g = (unsigned)std::min<uint64_t>(np, (uint64_t)L.num_sms * 8);
+    if (type == CJ_INT32) k_finish_dense_pages<int32_t><<<g, 128, 0, L.stream>>>(pages, rows, np);
+    else k_finish_dense_pages<long long><<<g, 128, 0, L.stream>>>(pages, rows, np);
+    count_launches(1);
     return cudaGetLastError();
 }
 

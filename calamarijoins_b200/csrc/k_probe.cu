@@ -48,11 +48,19 @@ struct TileSched {
 
 /* ---------------- matchers ---------------- */
 
-/* The join key of match `pos`, when the caller asked for it. */
+CJ_DEV bool wants_key(const MatchOut &out) { return out.key_pages != nullptr; }
+
+/* The join key of match `pos`, when the caller asked for it, straight into
+ * its place in the key columns' result pages: value q sits at byte
+ * 4 + 4q + 256 (q / 1984) (INT32: a page is 7936 value bytes and 256
+ * others) or 8 + 8q + 136 (q / 1007) (8-byte keys). */
 CJ_DEV void put_key(const MatchOut &out, unsigned long long pos, int64_t key) {
-    if (!out.keys) return;
-    if (out.key_bytes == 4) reinterpret_cast<int32_t *>(out.keys)[pos] = (int32_t)key;
-    else reinterpret_cast<long long *>(out.keys)[pos] = key;
+    if (!out.key_pages) return;
+    const uint64_t q = (uint32_t)pos; /* pos < capacity < 2^32 */
+    if (out.key_bytes == 4)
+        __stcs(reinterpret_cast<int32_t *>(out.key_pages + 4 + 4 * q + 256 * (q / kRowsPerPageInt32)), (int32_t)key);
+    else
+        __stcs(reinterpret_cast<long long *>(out.key_pages + 8 + 8 * q + 136 * (q / kRowsPerPage8B)), (long long)key);
 }
 
 /* Directory entry: start of the slot's tuples (bits 63..32), their count
@@ -227,7 +235,7 @@ CJ_DEV void probe_tile(const ColView &pkey, uint32_t n, const M &m, const typena
         if (i < n && load_key_stream(pkey, (uint32_t)i, &key)) c = m.count(sh, key, first);
         kinds |= (c == 0 ? 0u : (c == 1 ? 1u : 2u)) << (2 * it);
         ps.first[si] = first;
-        if (out.keys && c == 1) ps.key[si] = key;
+        if (wants_key(out) && c == 1) ps.key[si] = key;
         if (M::kAtMostOne) {
             const uint32_t ball = __ballot_sync(0xffffffffu, c != 0);
             ps.pre[si] = wrun + __popc(ball & lanemask_lt());
@@ -261,7 +269,7 @@ CJ_DEV void probe_tile(const ColView &pkey, uint32_t n, const M &m, const typena
             if (pos < out.capacity) {
                 if (out.build_rids) out.build_rids[pos] = ps.first[si];
                 if (out.probe_rids) out.probe_rids[pos] = prow;
-                if (out.keys) put_key(out, pos, ps.key[si]);
+                if (wants_key(out)) put_key(out, pos, ps.key[si]);
             }
         } else {
             int64_t key;
