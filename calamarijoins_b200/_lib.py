@@ -79,6 +79,11 @@ class ExecStatsC(C.Structure):
             "kernel_launches", "num_direct_joins")])
 
 
+class CacheMetaC(C.Structure):
+    _fields_ = [("num_rows", C.c_uint64), ("num_columns", C.c_uint64), ("types", C.c_int32 * 16),
+                ("num_pages", C.c_uint64 * 16)]
+
+
 class BatchStatsC(C.Structure):
     _fields_ = ([(n, C.c_uint64) for n in (
         "num_plans", "num_levels", "num_joins", "num_hash_joins", "num_nested_loop_joins", "probe_rows",
@@ -116,6 +121,16 @@ _SIGS = {
                                        C.POINTER(C.c_uint64), C.POINTER(_P), C.POINTER(_P)]),
     "cj_table_column_pages": (C.c_int, [_P, C.c_uint64, C.POINTER(_P), C.POINTER(C.c_uint64)]),
     "cj_table_free": (None, [_P]),
+    "cj_cache_read_meta": (C.c_int, [C.c_char_p, C.POINTER(CacheMetaC)]),
+    "cj_table_write_cache": (C.c_int, [C.POINTER(TableDesc), C.c_char_p]),
+    "cj_table_load_cache": (C.c_int, [_P, C.c_char_p, C.POINTER(_P)]),
+    "cj_catalog_create": (C.c_int, [_P, C.POINTER(_P)]),
+    "cj_catalog_destroy": (None, [_P]),
+    "cj_catalog_add": (C.c_int, [_P, C.c_char_p, _P]),
+    "cj_catalog_load": (C.c_int, [_P, C.c_char_p, C.c_char_p]),
+    "cj_catalog_get": (C.c_int, [_P, C.c_char_p, C.POINTER(_P)]),
+    "cj_catalog_size": (C.c_int, [_P, C.POINTER(C.c_uint64)]),
+    "cj_catalog_name": (C.c_int, [_P, C.c_uint64, C.POINTER(C.c_char_p)]),
     "cj_execute": (C.c_int, [_P, C.POINTER(PlanDesc), C.c_uint32, C.POINTER(_P),
                              C.POINTER(TimingStatsC), C.POINTER(ExecStatsC)]),
     "cj_execute_batch": (C.c_int, [_P, C.POINTER(PlanDesc), C.c_uint64, C.c_uint32, C.POINTER(_P),

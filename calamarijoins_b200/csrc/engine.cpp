@@ -565,10 +565,23 @@ cj_result *Executor::materialize(const std::vector<OutCol> &cols, const std::vec
         }
         stats.output_rows = rows;
         stats.output_pages = total_pages;
-        if (to_host && total_pages) {
-            res->host = ctx.alloc_pinned(total_pages * kPageSize);
+        /* Columns that share device pages (the join keys written by the
+         * probe) share one host copy too: downloaded once. */
+        std::vector<int64_t> alias(nc, -1);
+        for (size_t c = 0; c < nc; ++c)
+            for (size_t k = 0; k < c && alias[c] < 0; ++k)
+                if (cols[c].pages && cols[k].pages == cols[c].pages) alias[c] = (int64_t)k;
+        uint64_t host_pages = 0;
+        for (size_t c = 0; c < nc; ++c)
+            if (alias[c] < 0) host_pages += res->num_pages[c];
+        if (to_host && host_pages) {
+            res->host = ctx.alloc_pinned(host_pages * kPageSize);
             uint8_t *h = static_cast<uint8_t *>(res->host->ptr);
             for (size_t c = 0; c < nc; ++c) {
+                if (alias[c] >= 0) {
+                    res->host_cols[c] = res->host_cols[alias[c]];
+                    continue;
+                }
                 res->host_cols[c] = h;
                 h += res->num_pages[c] * kPageSize;
             }
@@ -579,10 +592,7 @@ cj_result *Executor::materialize(const std::vector<OutCol> &cols, const std::vec
                 /* values already in place: headers and bitmaps, once per
                  * shared page array */
                 res->dev_pages[c] = cols[c].pages;
-                bool first = true;
-                for (size_t k = 0; k < c; ++k)
-                    if (cols[k].pages == cols[c].pages) first = false;
-                if (first) {
+                if (alias[c] < 0) {
                     KScope ks(*this, "finish_pages");
                     ck(launch_finish_dense_pages(L, cols[c].pages->as<uint8_t>(), rows, types[c]), "finish_pages");
                 }
@@ -601,7 +611,7 @@ cj_result *Executor::materialize(const std::vector<OutCol> &cols, const std::vec
                 }
             }
             const size_t bytes = res->num_pages[c] * kPageSize;
-            if (to_host && bytes) {
+            if (to_host && bytes && alias[c] < 0) {
                 cudaEvent_t written = ctx.get_event();
                 ck(cudaEventRecord(written, ctx.stream), "event record");
                 ck(cudaStreamWaitEvent(ctx.d2h_stream, written, 0), "stream wait");

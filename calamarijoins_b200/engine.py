@@ -11,6 +11,7 @@ throws std::bad_alloc / std::runtime_error).
 from __future__ import annotations
 
 import ctypes as C
+import os
 from dataclasses import dataclass, field
 from typing import Optional
 
@@ -96,14 +97,108 @@ class ResidentTable:
         h = C.c_void_p()
         check(lib().cj_table_upload(ctx.handle, C.byref(td), C.byref(h)))
         self.handle = h.value
+        self._owned = True
+
+    @classmethod
+    def from_handle(cls, ctx: Context, handle: int, num_rows: int, types, owned: bool = True) -> "ResidentTable":
+        """Wraps a cj_table made elsewhere (a cache file, a catalog entry);
+        `owned` False leaves freeing it to its owner."""
+        t = cls.__new__(cls)
+        t.ctx, t.handle, t.num_rows, t.types, t._owned = ctx, handle, num_rows, [DataType(x) for x in types], owned
+        return t
+
+    @classmethod
+    def from_cache(cls, ctx: Context, path: str) -> "ResidentTable":
+        """Loads one of the reference's `.tbl` cache files into HBM
+        (cj_table_load_cache; Table::from_cache, src/build_table.cpp:140-197)."""
+        meta = read_cache_meta(path)
+        h = C.c_void_p()
+        check(lib().cj_table_load_cache(ctx.handle, os.fsencode(path), C.byref(h)))
+        return cls.from_handle(ctx, h.value, meta["num_rows"], meta["types"])
 
     def free(self):
         if getattr(self, "handle", None):
-            lib().cj_table_free(self.handle)
+            if getattr(self, "_owned", True):
+                lib().cj_table_free(self.handle)
             self.handle = None
 
     def __del__(self):
         self.free()
+
+
+def read_cache_meta(path: str) -> dict:
+    """Header of a `.tbl` cache file (TableMeta, include/data_access/
+    table.h:30-35), checked against the file size."""
+    m = _lib.CacheMetaC()
+    check(lib().cj_cache_read_meta(os.fsencode(path), C.byref(m)))
+    n = m.num_columns
+    return {"num_rows": m.num_rows, "types": [DataType(m.types[i]) for i in range(n)],
+            "num_pages": [m.num_pages[i] for i in range(n)]}
+
+
+def write_cache(table: ColumnarTable, path: str) -> None:
+    """Writes host pages as a `.tbl` cache file (DumpTable::dump,
+    include/data_access/table.h:210-220)."""
+    keep = []
+    cols = (_lib.ColumnDesc * max(len(table.columns), 1))()
+    for c, col in enumerate(table.columns):
+        ptrs = col.page_pointers()
+        keep.append(ptrs)
+        cols[c].type = int(col.type)
+        cols[c].num_pages = col.num_pages
+        cols[c].pages = C.cast(ptrs, C.POINTER(C.c_void_p))
+    td = _lib.TableDesc(table.num_rows, len(table.columns), cols)
+    check(lib().cj_table_write_cache(C.byref(td), os.fsencode(path)))
+
+
+class Catalog:
+    """Resident tables by name (cj_catalog). load() reads a `.tbl` cache
+    file into HBM once; catalog[name] is a ResidentTable for Plan.inputs."""
+
+    def __init__(self, ctx: Context):
+        self.ctx = ctx
+        h = C.c_void_p()
+        check(lib().cj_catalog_create(ctx.handle, C.byref(h)))
+        self.handle = h.value
+        self._meta = {}
+
+    def load(self, name: str, path: str) -> None:
+        meta = read_cache_meta(path)
+        check(lib().cj_catalog_load(self.handle, name.encode(), os.fsencode(path)))
+        self._meta[name] = meta
+
+    def load_dir(self, directory: str) -> list:
+        """Every `<name>.tbl` file of a directory, under its name."""
+        names = []
+        for f in sorted(os.listdir(directory)):
+            if f.endswith(".tbl"):
+                self.load(f[:-4], os.path.join(directory, f))
+                names.append(f[:-4])
+        return names
+
+    def names(self) -> list:
+        n = C.c_uint64()
+        check(lib().cj_catalog_size(self.handle, C.byref(n)))
+        out = []
+        for i in range(n.value):
+            p = C.c_char_p()
+            check(lib().cj_catalog_name(self.handle, i, C.byref(p)))
+            out.append(p.value.decode())
+        return out
+
+    def __getitem__(self, name: str) -> ResidentTable:
+        h = C.c_void_p()
+        check(lib().cj_catalog_get(self.handle, name.encode(), C.byref(h)))
+        m = self._meta[name]
+        return ResidentTable.from_handle(self.ctx, h.value, m["num_rows"], m["types"], owned=False)
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib().cj_catalog_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        self.close()
 
 
 class Result:

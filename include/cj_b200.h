@@ -247,6 +247,41 @@ int cj_table_column_pages(const cj_table *table, uint64_t column,
 
 void cj_table_free(cj_table *table);
 
+/* The reference's `.tbl` table cache (written by DumpTable::dump,
+ * include/data_access/table.h:136-221; read by Table::from_cache,
+ * src/build_table.cpp:140-197): an 8 KiB header page with TableMeta
+ * (table.h:30-35) and zeros, then every column's pages in column order; at
+ * most 16 columns. `cj_cache_meta` mirrors TableMeta. */
+typedef struct cj_cache_meta {
+    uint64_t num_rows;
+    uint64_t num_columns;
+    int32_t types[16];
+    uint64_t num_pages[16];
+} cj_cache_meta;
+
+/* Reads and checks a cache file's header (no GPU needed); a header that
+ * disagrees with the file size is CJ_ERR_MALFORMED_PAGE. */
+int cj_cache_read_meta(const char *path, cj_cache_meta *meta);
+
+/* Writes host pages as a cache file (the DumpTable format). */
+int cj_table_write_cache(const cj_table_desc *table, const char *path);
+
+/* Loads a cache file into a resident table: its pages cross to HBM once.
+ * Replaces Table::from_cache for callers that keep tables on the GPU. */
+int cj_table_load_cache(cj_context *ctx, const char *path, cj_table **out);
+
+/* Catalog: resident tables by name (no reference counterpart; the
+ * reference's driver maps one cache file per table and query). The catalog
+ * owns its tables and frees them in cj_catalog_destroy. */
+typedef struct cj_catalog cj_catalog;
+int cj_catalog_create(cj_context *ctx, cj_catalog **out);
+void cj_catalog_destroy(cj_catalog *cat);
+int cj_catalog_add(cj_catalog *cat, const char *name, cj_table *table);  /* takes ownership */
+int cj_catalog_load(cj_catalog *cat, const char *name, const char *path); /* a cache file   */
+int cj_catalog_get(const cj_catalog *cat, const char *name, cj_table **table);
+int cj_catalog_size(const cj_catalog *cat, uint64_t *count);
+int cj_catalog_name(const cj_catalog *cat, uint64_t index, const char **name);
+
 /* ------------------------------------------------------------------------ */
 /* Execution                                                                 */
 /* ------------------------------------------------------------------------ */
