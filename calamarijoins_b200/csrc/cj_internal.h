@@ -65,7 +65,7 @@ struct StatusBlock {
     unsigned int errors;          /* DevError bits                          */
     unsigned int pad;
     unsigned long long counter;   /* match counter of the last probe        */
-    unsigned long long aux[6];    /* scratch totals (pages, rows)           */
+    unsigned long long aux[6];    /* direct-mapped table parameters        */
 };
 
 /* How a kernel reads one column of a relation: row i of the relation is
@@ -147,11 +147,16 @@ cudaError_t scan_u32_to_u64(const Launch &L, const uint32_t *in, uint64_t *out,
                             size_t n, void *temp);
 
 /* Decode */
-/* Rows per page, and the column's COL_* flags ORed into *col_flags
- * (zeroed by the caller; may be null). */
-cudaError_t launch_page_rows(const Launch &L, const uint8_t *pages,
-                             uint64_t num_pages, int32_t type,
-                             uint32_t *rows_per_page, uint32_t *col_flags);
+/* Page index of one column: rows_pp[p] = rows of page p, row_start[p] =
+ * rows before page p (row_start[num_pages] = total; only the total when
+ * the column is read in place), state[0] |= the column's COL_* flags;
+ * a total other than `rows` raises DEV_ERR_ROW_COUNT and sets
+ * COL_NOT_DIRECT. state (2 words) must be zero; partials holds
+ * page_index_blocks(num_pages) entries. Two launches. */
+uint64_t page_index_blocks(const Launch &L, uint64_t num_pages);
+cudaError_t launch_page_index(const Launch &L, const uint8_t *pages, uint64_t num_pages, int32_t type,
+                              uint64_t rows, uint32_t *rows_pp, uint64_t *partials, uint64_t *row_start,
+                              uint32_t *state);
 /* Rows past max_rows are never written; a page that would write them
  * raises DEV_ERR_ROW_COUNT instead. Does nothing when *col_flags is 0
  * (readers then take the values from the pages). */
@@ -181,9 +186,6 @@ struct DecodeTask {
 cudaError_t launch_decode_grouped(const Launch &L, const DecodeTask *tasks_dev, uint32_t ntasks,
                                   uint64_t total_pages, uint32_t *rows_pp, uint64_t *row_start,
                                   void *scan_temp);
-/* Raises DEV_ERR_ROW_COUNT unless *total == expected. */
-cudaError_t launch_check_rows(const Launch &L, const uint64_t *total, uint64_t expected,
-                              uint32_t *col_flags = nullptr);
 
 /* Build */
 struct BuildPlan {

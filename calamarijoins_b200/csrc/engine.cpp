@@ -212,19 +212,15 @@ Decoded &Executor::decode(uint64_t t, uint64_t c) {
     const uint64_t np = d.src.num_pages;
     DevPtr rows_pp = ctx.alloc(std::max<uint64_t>(np, 1) * 4);
     DevPtr row_start = ctx.alloc((np + 1) * 8);
-    DevPtr scan_tmp = ctx.alloc(scan_temp_bytes(np));
-    d.col_flags = ctx.alloc(4);
-    ck(cudaMemsetAsync(d.col_flags->ptr, 0, 4, ctx.stream), "memset");
+    DevPtr partials = ctx.alloc(page_index_blocks(L, np) * 8);
+    d.col_flags = ctx.alloc(8); /* COL_* flags, then the index's finished-block count */
+    ck(cudaMemsetAsync(d.col_flags->ptr, 0, 8, ctx.stream), "memset");
     {
-        KScope k(*this, "page_rows");
-        ck(launch_page_rows(L, d.src.dev, np, d.type, rows_pp->as<uint32_t>(), d.col_flags->as<uint32_t>()),
-           "page_rows");
+        KScope k(*this, "page_index");
+        ck(launch_page_index(L, d.src.dev, np, d.type, d.rows, rows_pp->as<uint32_t>(), partials->as<uint64_t>(),
+                             row_start->as<uint64_t>(), d.col_flags->as<uint32_t>()),
+           "page_index");
     }
-    {
-        KScope k(*this, "scan");
-        ck(scan_u32_to_u64(L, rows_pp->as<uint32_t>(), row_start->as<uint64_t>(), np, scan_tmp->ptr), "scan");
-    }
-    ck(launch_check_rows(L, row_start->as<uint64_t>() + np, d.rows, d.col_flags->as<uint32_t>()), "check_rows");
     const uint64_t words = (d.rows + 31) / 32;
     d.valid = ctx.alloc(std::max<uint64_t>(words, 1) * 4);
     ck(cudaMemsetAsync(d.valid->ptr, 0, std::max<uint64_t>(words, 1) * 4, ctx.stream), "memset");

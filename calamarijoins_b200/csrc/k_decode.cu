@@ -66,16 +66,94 @@ CJ_DEV uint32_t page_flags(const uint8_t *pg, uint64_t p, uint64_t np, int32_t t
     return f;
 }
 
-__global__ void k_page_rows(const uint8_t *__restrict__ pages, uint64_t np, int32_t type,
-                            uint32_t *__restrict__ rows, uint32_t *col_flags, unsigned int *err) {
+/* Page index of one column in two launches. Block b of both kernels owns
+ * pages [b * chunk, (b + 1) * chunk).
+ * k_page_index: rows per page, the column's COL_* flags (ORed into
+ * state[0]) and each block's row total (partials[b]); the last block to
+ * finish (state[1] counts finished blocks) adds the totals, stores
+ * row_start[np] and checks the row count against the table's (a mismatch
+ * raises DEV_ERR_ROW_COUNT and makes the column NOT_DIRECT, so readers stay
+ * inside its decoded arrays).
+ * k_page_index_scan: row_start[p] = rows before page p; skipped for a
+ * column read in place (state[0] == 0), which needs no row offsets. */
+constexpr int kIndexThreads = 256;
+
+__global__ void __launch_bounds__(kIndexThreads)
+    k_page_index(const uint8_t *__restrict__ pages, uint64_t np, int32_t type, uint64_t chunk, uint64_t expected,
+                 uint32_t *__restrict__ rows, uint64_t *__restrict__ partials, uint64_t *__restrict__ row_start,
+                 uint32_t *state, unsigned int *err) {
+    __shared__ uint64_t wsum[kIndexThreads / 32];
+    __shared__ bool s_last;
+    const uint64_t p0 = (uint64_t)blockIdx.x * chunk, p1 = min(np, p0 + chunk);
+    uint64_t s = 0;
     uint32_t f = 0;
-    for (uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; p < np;
-         p += (uint64_t)gridDim.x * blockDim.x) {
-        rows[p] = page_rows_of(pages + p * kPageSize, type, err);
-        f |= page_flags(pages + p * kPageSize, p, np, type);
+    for (uint64_t p = p0 + threadIdx.x; p < p1; p += blockDim.x) {
+        const uint8_t *pg = pages + p * kPageSize;
+        const uint32_t r = page_rows_of(pg, type, err);
+        rows[p] = r;
+        s += r;
+        f |= page_flags(pg, p, np, type);
     }
     f = __reduce_or_sync(0xffffffffu, f);
-    if (f && lane_id() == 0 && col_flags) atomicOr(col_flags, f);
+    if (f && lane_id() == 0) atomicOr(state, f);
+    s = warp_sum(s);
+    if (lane_id() == 0) wsum[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint64_t t = 0;
+        for (int w = 0; w < kIndexThreads / 32; ++w) t += wsum[w];
+        partials[blockIdx.x] = t;
+        __threadfence();
+        s_last = atomicAdd(state + 1, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    uint64_t t = 0;
+    for (uint32_t b = threadIdx.x; b < gridDim.x; b += blockDim.x) t += __ldcg(partials + b);
+    t = warp_sum(t);
+    __syncthreads();
+    if (lane_id() == 0) wsum[threadIdx.x >> 5] = t;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint64_t total = 0;
+        for (int w = 0; w < kIndexThreads / 32; ++w) total += wsum[w];
+        row_start[np] = total;
+        if (total != expected) {
+            atomicOr(err, DEV_ERR_ROW_COUNT);
+            atomicOr(state, COL_NOT_DIRECT);
+        }
+    }
+}
+
+/* A column without pages: zero rows (any other count is an error). */
+__global__ void k_page_index_empty(uint64_t expected, uint64_t *row_start, uint32_t *state, unsigned int *err) {
+    row_start[0] = 0;
+    if (expected != 0) {
+        atomicOr(err, DEV_ERR_ROW_COUNT);
+        atomicOr(state, COL_NOT_DIRECT);
+    }
+}
+
+__global__ void __launch_bounds__(kIndexThreads)
+    k_page_index_scan(const uint32_t *__restrict__ rows, uint64_t np, uint64_t chunk,
+                      const uint64_t *__restrict__ partials, uint64_t *__restrict__ row_start,
+                      const uint32_t *state) {
+    __shared__ uint64_t wbuf[kIndexThreads / 32 + 1];
+    if (*state == 0u) return; /* uniform: read in place */
+    uint64_t o = 0;
+    for (uint32_t b = threadIdx.x; b < blockIdx.x; b += blockDim.x) o += partials[b];
+    uint64_t off;
+    block_exclusive_scan<uint64_t>(o, wbuf, &off);
+    const uint64_t p0 = (uint64_t)blockIdx.x * chunk, p1 = min(np, p0 + chunk);
+    for (uint64_t base = p0; base < p1; base += blockDim.x) {
+        const uint64_t p = base + threadIdx.x;
+        const uint64_t v = p < p1 ? rows[p] : 0;
+        uint64_t tot;
+        const uint64_t pre = block_exclusive_scan<uint64_t>(v, wbuf, &tot);
+        if (p < p1) row_start[p] = off + pre;
+        off += tot;
+    }
 }
 
 /* Loads a sparse page's bitmap into s_bm (bits past n_rows cleared) and the
@@ -366,13 +444,6 @@ __global__ void __launch_bounds__(kDecodeThreads)
     }
 }
 
-__global__ void k_check_rows(const uint64_t *total, uint64_t expected, unsigned int *err, uint32_t *col_flags) {
-    if (*total != expected) {
-        atomicOr(err, DEV_ERR_ROW_COUNT);
-        if (col_flags) atomicOr(col_flags, COL_NOT_DIRECT); /* readers stay inside the decoded arrays */
-    }
-}
-
 unsigned grid_for(const Launch &L, uint64_t units, int per_sm) {
     uint64_t g = (uint64_t)L.num_sms * per_sm;
     if (units < g) g = units;
@@ -381,13 +452,24 @@ unsigned grid_for(const Launch &L, uint64_t units, int per_sm) {
 
 } // namespace
 
-cudaError_t launch_page_rows(const Launch &L, const uint8_t *pages, uint64_t np, int32_t type,
-                             uint32_t *rows, uint32_t *col_flags) {
-    if (np == 0) return cudaSuccess;
-    unsigned g = (unsigned)((np + 255) / 256);
-    if (g > (unsigned)L.num_sms * 8) g = L.num_sms * 8;
-    k_page_rows<<<g, 256, 0, L.stream>>>(pages, np, type, rows, col_flags, L.dev_errors);
-    count_launches(1);
+uint64_t page_index_blocks(const Launch &L, uint64_t np) {
+    const uint64_t chunk = std::max<uint64_t>(kIndexThreads, (np + L.num_sms * 8 - 1) / (L.num_sms * 8));
+    return std::max<uint64_t>((np + chunk - 1) / chunk, 1);
+}
+
+cudaError_t launch_page_index(const Launch &L, const uint8_t *pages, uint64_t np, int32_t type, uint64_t rows,
+                              uint32_t *rows_pp, uint64_t *partials, uint64_t *row_start, uint32_t *state) {
+    if (np == 0) {
+        k_page_index_empty<<<1, 1, 0, L.stream>>>(rows, row_start, state, L.dev_errors);
+        count_launches(1);
+        return cudaGetLastError();
+    }
+    const unsigned g = (unsigned)page_index_blocks(L, np);
+    const uint64_t chunk = (np + g - 1) / g;
+    k_page_index<<<g, kIndexThreads, 0, L.stream>>>(pages, np, type, chunk, rows, rows_pp, partials, row_start,
+                                                     state, L.dev_errors);
+    k_page_index_scan<<<g, kIndexThreads, 0, L.stream>>>(rows_pp, np, chunk, partials, row_start, state);
+    count_launches(2);
     return cudaGetLastError();
 }
 
@@ -440,10 +522,5 @@ cudaError_t launch_decode_grouped(const Launch &L, const DecodeTask *tasks_dev, 
     return cudaGetLastError();
 }
 
-cudaError_t launch_check_rows(const Launch &L, const uint64_t *total, uint64_t expected, uint32_t *col_flags) {
-    k_check_rows<<<1, 1, 0, L.stream>>>(total, expected, L.dev_errors, col_flags);
-    count_launches(1);
-    return cudaGetLastError();
-}
 
 } // namespace cj

@@ -362,8 +362,11 @@ def test_row_count_mismatch_rejected(gpu_ctx):
     # fewer and more rows declared than the pages hold, on the probe side and
     # on the (NULL-free, full-page) build side, whose columns would otherwise
     # be read in place from their pages
-    for side, delta in ((1, -1), (1, 1), (0, 1), (0, 1000)):
-        plan = join2(3000, 5000, seed=7, build_payload=(L,), probe_payload=(F,))
+    # (the 1.2M-row probe side has 605 INT32 pages: the page index spans
+    # several blocks and the last one to finish checks the total)
+    for side, delta, npr in ((1, -1, 5000), (1, 1, 5000), (0, 1, 5000), (0, 1000, 5000), (1, -1, 1_200_000),
+                             (1, 1984, 1_200_000)):
+        plan = join2(3000, npr, seed=7, build_payload=(L,), probe_payload=(F,))
         plan.inputs[side].num_rows += delta
         with pytest.raises(CJError) as e:
             run_product(plan, gpu_ctx)
