@@ -323,6 +323,16 @@ Relation Executor::exec_join(uint64_t node_idx, int depth, bool is_root, cj_resu
     if (B.rows && P.rows) {
         const ColView bv = view(B, bk, nullptr);
         const ColView pv = view(P, pk, nullptr);
+        if (is_root) {
+            /* The root's other output columns whose pages are already in
+             * HBM are indexed (and decoded, if they must be) now, while the
+             * kernels above run, rather than after the probe's
+             * synchronisation, where the GPU would wait for the host to
+             * enqueue them. Columns still uploading stay lazy, so that the
+             * result downloads overlap their uploads. */
+            for (const auto &o : outs)
+                if (!o.from_keys && resident(o.col.input)) decode(o.col.input, o.col.col);
+        }
         const uint64_t nl_max = std::min<int64_t>(std::max<int64_t>(ctx.opt.nested_loop_max_build, 0), kNestedLoopMax);
         const bool nl = B.rows <= nl_max;
         DevPtr dir, tuples, nlk, nlr, nlc, slots;

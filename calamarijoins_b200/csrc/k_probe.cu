@@ -410,9 +410,11 @@ cudaError_t run_tiles(const Launch &L, const ColView &pkey, uint32_t n, const M 
     e = cudaMemsetAsync(out.counter, 0, sizeof(unsigned long long), L.stream);
     if (e != cudaSuccess) return e;
     if (n == 0) return cudaSuccess;
-    int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_probe_tiles<M>, kProbeThreads, 0);
-    if (per_sm < 1) per_sm = 1;
+    static const int per_sm = [] { /* once per matcher: a driver query per launch costs host time */
+        int n = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_probe_tiles<M>, kProbeThreads, 0);
+        return n < 1 ? 1 : n;
+    }();
     uint64_t grid = (uint64_t)L.num_sms * per_sm;
     if (grid > ts.num_tiles) grid = ts.num_tiles;
     k_probe_tiles<M><<<(unsigned)grid, kProbeThreads, 0, L.stream>>>(pkey, n, m, out, ts);
@@ -461,9 +463,11 @@ cudaError_t launch_nl_probe_tiles(const Launch &L, const ColView &pkey, uint32_t
 cudaError_t launch_probe_grouped(const Launch &L, const ProbeTask *tasks_dev, uint32_t ntasks, uint32_t total_tiles,
                                  unsigned int *ticket, const uint16_t *bloom) {
     if (total_tiles == 0) return cudaSuccess;
-    int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_probe_grouped, kProbeThreads, 0);
-    if (per_sm < 1) per_sm = 1;
+    static const int per_sm = [] {
+        int n = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_probe_grouped, kProbeThreads, 0);
+        return n < 1 ? 1 : n;
+    }();
     uint64_t grid = (uint64_t)L.num_sms * per_sm;
     if (grid > total_tiles) grid = total_tiles;
     k_probe_grouped<<<(unsigned)grid, kProbeThreads, 0, L.stream>>>(tasks_dev, ntasks, total_tiles, ticket, bloom);

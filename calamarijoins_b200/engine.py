@@ -12,6 +12,7 @@ from __future__ import annotations
 
 import ctypes as C
 import os
+import sys
 from dataclasses import dataclass, field
 from typing import Optional
 
@@ -20,6 +21,8 @@ import numpy as np
 from . import _lib
 from ._lib import PAGE_SIZE, check, lib
 from .plan import Column, ColumnarTable, DataType, Plan, PlanDescriptor
+
+_finalizing = sys.is_finalizing  # bound now: module globals are gone at exit
 
 
 @dataclass
@@ -49,7 +52,8 @@ class Context:
             self.handle = None
 
     def __del__(self):
-        self.close()
+        if not _finalizing():  # at exit the process releases everything
+            self.close()
 
     def set_option(self, option: int, value: int):
         check(lib().cj_context_set_option(self.handle, int(option), int(value)))
@@ -123,7 +127,8 @@ class ResidentTable:
             self.handle = None
 
     def __del__(self):
-        self.free()
+        if not _finalizing():
+            self.free()
 
 
 def read_cache_meta(path: str) -> dict:
@@ -198,7 +203,8 @@ class Catalog:
             self.handle = None
 
     def __del__(self):
-        self.close()
+        if not _finalizing():  # at exit the process releases everything
+            self.close()
 
 
 class Result:
@@ -247,7 +253,8 @@ class Result:
             self.handle = None
 
     def __del__(self):
-        self.free()
+        if not _finalizing():
+            self.free()
 
 
 def build_context(device: int = -1) -> Context:
@@ -348,4 +355,5 @@ class Server:
             self._pending.clear()
 
     def __del__(self):
-        self.close()
+        if not _finalizing():  # at exit the process releases everything
+            self.close()
