@@ -76,7 +76,7 @@ class ExecStatsC(C.Structure):
         + [(n, C.c_uint64) for n in (
             "h2d_bytes", "d2h_bytes", "num_joins", "num_hash_joins", "num_nested_loop_joins",
             "probe_rows", "matches", "probe_reruns", "output_rows", "output_pages",
-            "kernel_launches", "num_direct_joins")])
+            "kernel_launches", "num_direct_joins", "num_open_joins")])
 
 
 class CacheMetaC(C.Structure):

@@ -65,7 +65,9 @@ struct StatusBlock {
     unsigned int errors;          /* DevError bits                          */
     unsigned int pad;
     unsigned long long counter;   /* match counter of the last probe        */
-    unsigned long long aux[6];    /* direct-mapped table parameters        */
+    unsigned long long aux[8];    /* [0, kDirectParams): direct-mapped table
+                                     parameters; [kOpenDup]: a repeated key
+                                     in the open-addressing table          */
 };
 
 /* How a kernel reads one column of a relation: row i of the relation is
@@ -245,6 +247,19 @@ cudaError_t launch_direct_build(const Launch &L, const ColView &key, uint32_t n,
 /* Probe of a direct-mapped table; does nothing when params[3] is set. */
 cudaError_t launch_probe_tiles_array(const Launch &L, const ColView &pkey, uint32_t n_probe, const uint32_t *slots,
                                      const unsigned long long *params, const MatchOut &out, void *sched);
+
+/* Open-addressing table for unique INT32 build keys too spread out for a
+ * direct-mapped table: `nslots` 8-byte slots (key << 32 | build row, all
+ * ones when empty; at most half of them full), linear probing from the
+ * key's hash scaled to [0, nslots). The build sets *dup when a key repeats
+ * (the table cannot be used); the probe then does nothing. Two launches. */
+constexpr int kOpenDup = kDirectParams;
+constexpr uint64_t kOpenMaxRows = 1ull << 28;
+cudaError_t launch_open_build(const Launch &L, const ColView &key, uint32_t n, unsigned long long *slots,
+                              uint64_t nslots, unsigned long long *dup);
+cudaError_t launch_probe_tiles_open(const Launch &L, const ColView &pkey, uint32_t n_probe,
+                                    const unsigned long long *slots, uint64_t nslots,
+                                    const unsigned long long *dup, const MatchOut &out, void *sched);
 
 /* Probe and nested loop share one tiled kernel; `sched` is scratch of
  * probe_sched_bytes(n_probe) bytes (the tile ticket). */

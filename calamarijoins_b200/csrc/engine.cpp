@@ -337,8 +337,27 @@ Relation Executor::exec_join(uint64_t node_idx, int depth, bool is_root, cj_resu
         const bool nl = B.rows <= nl_max;
         DevPtr dir, tuples, nlk, nlr, nlc, slots;
         int log2_slots = 0;
-        bool direct = false; /* direct-mapped table tried (the device decides) */
         unsigned long long *d_params = &ctx.d_status->aux[0];
+        bool direct = false; /* direct-mapped table tried (the device decides) */
+        bool open = false;   /* open-addressing table tried (the device decides) */
+        DevPtr open_slots;
+        uint64_t open_n = 0;
+        /* Unique INT32 keys too spread out for the direct-mapped table: an
+         * open-addressing table (one slot walk per probe row, against a
+         * directory entry and a tuple range). Tried only after the
+         * direct-mapped table turned out unusable; a repeated key sends the
+         * join on to the hash table. */
+        auto build_open = [&]() -> bool {
+            if (bk.type != CJ_INT32 || B.rows > kOpenMaxRows) return false;
+            open_n = std::max<uint64_t>(2 * B.rows, 1024);
+            open_slots = ctx.alloc(open_n * 8);
+            ck(cudaMemsetAsync(d_params + kOpenDup, 0, 8, ctx.stream), "memset");
+            KScope k(*this, "open_build");
+            ck(launch_open_build(L, bv, (uint32_t)B.rows, open_slots->as<unsigned long long>(), open_n,
+                                 d_params + kOpenDup),
+               "open_build");
+            return true;
+        };
         auto build_hash = [&]() {
             BuildPlan bp;
             bp.num_rows = (uint32_t)B.rows;
@@ -413,6 +432,11 @@ Relation Executor::exec_join(uint64_t node_idx, int depth, bool is_root, cj_resu
                     ck(launch_nl_probe_tiles(L, pv, (uint32_t)P.rows, nlk->as<int64_t>(), nlr->as<uint32_t>(),
                                              nlc->as<uint32_t>(), mo, sched->ptr),
                        "nl_probe");
+                } else if (open) {
+                    KScope k(*this, "probe_open");
+                    ck(launch_probe_tiles_open(L, pv, (uint32_t)P.rows, open_slots->as<unsigned long long>(), open_n,
+                                               d_params + kOpenDup, mo, sched->ptr),
+                       "probe_open");
                 } else if (direct) {
                     KScope k(*this, "probe_array");
                     ck(launch_probe_tiles_array(L, pv, (uint32_t)P.rows, slots->as<uint32_t>(), d_params, mo,
@@ -428,9 +452,19 @@ Relation Executor::exec_join(uint64_t node_idx, int depth, bool is_root, cj_resu
             ctx.sync_status();
             if (direct && ctx.h_status->aux[3]) {
                 /* keys too spread out, or a key repeats: the direct-mapped
-                 * table is unusable (the probe did nothing); hash table */
+                 * table is unusable (the probe did nothing); an
+                 * open-addressing table, else the hash table */
                 direct = false;
                 slots.reset();
+                PhaseScope ph(*this, PH_BUILD);
+                open = build_open();
+                if (!open) build_hash();
+                continue;
+            }
+            if (open && ctx.h_status->aux[kOpenDup]) {
+                /* a key repeats: the probe did nothing; hash table */
+                open = false;
+                open_slots.reset();
                 PhaseScope ph(*this, PH_BUILD);
                 build_hash();
                 continue;
@@ -442,6 +476,7 @@ Relation Executor::exec_join(uint64_t node_idx, int depth, bool is_root, cj_resu
             cap = M;
         }
         if (direct) stats.num_direct_joins++;
+        if (open) stats.num_open_joins++;
     }
     if (M > 0xFFFFFFFFull) fail(CJ_ERR_LIMIT, "join result exceeds 2^32-1 rows");
     stats.matches += M;

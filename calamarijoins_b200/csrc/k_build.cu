@@ -411,6 +411,37 @@ __global__ void k_array_build(ColView key, uint32_t n, uint32_t *__restrict__ sl
     }
 }
 
+/* ---- open-addressing table (unique INT32 keys, any spread) ---- */
+constexpr unsigned long long kOpenEmpty = ~0ull; /* row 2^32-1 never exists */
+
+__global__ void k_open_fill(unsigned long long *__restrict__ slots, uint64_t nslots) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nslots;
+         i += (uint64_t)gridDim.x * blockDim.x)
+        slots[i] = kOpenEmpty;
+}
+
+/* Each non-NULL key claims the first empty slot from its hash on (at most
+ * half the slots fill, so a free one is always found); meeting its own key
+ * on the way means the key repeats. */
+__global__ void k_open_insert(ColView key, uint32_t n, unsigned long long *__restrict__ slots, uint64_t nslots,
+                              unsigned long long *dup) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        int64_t k;
+        if (!load_key(key, (uint32_t)i, &k)) continue;
+        const unsigned long long v = ((unsigned long long)(uint32_t)k << 32) | (unsigned long long)i;
+        uint64_t h = __umul64hi(hash_key(k), nslots);
+        for (uint64_t step = 0; step < nslots; ++step) {
+            const unsigned long long old = atomicCAS(slots + h, kOpenEmpty, v);
+            if (old == kOpenEmpty) break;
+            if ((uint32_t)(old >> 32) == (uint32_t)k) {
+                *dup = 1ull;
+                break;
+            }
+            if (++h == nslots) h = 0;
+        }
+    }
+}
+
 bool g_attrs_set = false;
 void set_smem_attrs() {
     if (g_attrs_set) return;
@@ -489,6 +520,17 @@ cudaError_t launch_direct_build(const Launch &L, const ColView &key, uint32_t n,
     g = std::min<uint64_t>(((uint64_t)n + 255) / 256, (uint64_t)L.num_sms * 8);
     k_array_build<<<(unsigned)g, 256, 0, L.stream>>>(key, n, slots, params);
     count_launches(4);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_open_build(const Launch &L, const ColView &key, uint32_t n, unsigned long long *slots,
+                              uint64_t nslots, unsigned long long *dup) {
+    if (nslots < 2ull * n) return cudaErrorInvalidValue; /* the insert loop needs free slots */
+    uint64_t g = std::min<uint64_t>(std::max<uint64_t>((nslots + 255) / 256, 1), (uint64_t)L.num_sms * 8);
+    k_open_fill<<<(unsigned)g, 256, 0, L.stream>>>(slots, nslots);
+    g = std::min<uint64_t>(std::max<uint64_t>(((uint64_t)n + 255) / 256, 1), (uint64_t)L.num_sms * 8);
+    k_open_insert<<<(unsigned)g, 256, 0, L.stream>>>(key, n, slots, nslots, dup);
+    count_launches(2);
     return cudaGetLastError();
 }
 

@@ -36,6 +36,16 @@ namespace {
 #ifndef CJ_PROBE_MIN_BLOCKS
 #define CJ_PROBE_MIN_BLOCKS 8
 #endif
+#ifndef CJ_HASH_MIN_BLOCKS
+#define CJ_HASH_MIN_BLOCKS 8
+#endif
+/* The grouped kernel carries every matcher's code: at 5 CTAs per SM (48
+ * registers) it spills nothing and ran C4 2 % faster than at 8 (32
+ * registers, 260 bytes of spills). The hash matchers alone spill a little at
+ * 8 CTAs but ran 11 % slower at 6 without spills: occupancy wins there. */
+#ifndef CJ_GROUPED_MIN_BLOCKS
+#define CJ_GROUPED_MIN_BLOCKS 5
+#endif
 constexpr int kProbeThreads = 256;
 constexpr int kProbeItems = CJ_PROBE_ITEMS; /* rows per thread (hash, nested loop)      */
 constexpr uint32_t kTileRows = kProbeThreads * kProbeItems; /* grouped kernel's tile */
@@ -68,6 +78,7 @@ CJ_DEV void put_key(const MatchOut &out, unsigned long long pos, int64_t key) {
  * the OR of their Bloom tags (15..0). */
 template <typename KB> struct HashMatcher {
     static constexpr bool kAtMostOne = false;
+    static constexpr int kMinBlocks = CJ_HASH_MIN_BLOCKS;
     static constexpr int kItems = kProbeItems;
     CJ_DEV HashMatcher resolved() const { return *this; }
     HashTableView<KB> ht;
@@ -123,6 +134,7 @@ template <typename KB> struct HashMatcher {
  * caller then builds the hash table instead). */
 struct ArrayMatcher {
     static constexpr bool kAtMostOne = true; /* unique keys: 0 or 1 match per row */
+    static constexpr int kMinBlocks = kProbeMinBlocks;
     static constexpr int kItems = 4;         /* one light chain per row: 4 rows per thread
                                                 fit 32 registers (387 us vs 434 us for 2
                                                 on 64M probe rows) */
@@ -159,8 +171,49 @@ struct ArrayMatcher {
     }
 };
 
+/* Open-addressing table of unique INT32 keys (launch_open_build): walk the
+ * slots from the key's hash until the key or an empty slot. */
+struct OpenMatcher {
+    static constexpr bool kAtMostOne = true; /* unique keys */
+    static constexpr int kItems = 4;
+    static constexpr int kMinBlocks = kProbeMinBlocks;
+    const unsigned long long *slots;
+    uint64_t nslots;
+    const unsigned long long *dup;
+    struct Shared {
+        uint32_t unused;
+    };
+    CJ_DEV bool skip() const { return *dup != 0ull; }
+    CJ_DEV OpenMatcher resolved() const { return *this; }
+    CJ_DEV void init(Shared &) const {}
+    CJ_DEV uint32_t count(const Shared &, int64_t key, uint32_t &first) const {
+        if (key != (int64_t)(int32_t)key) return 0; /* no INT32 build key equals it */
+        uint64_t h = __umul64hi(hash_key(key), nslots);
+        for (uint64_t step = 0; step < nslots; ++step) {
+            const unsigned long long v = __ldg(slots + h);
+            if (v == ~0ull) return 0;
+            if ((int32_t)(uint32_t)(v >> 32) == (int32_t)key) {
+                first = (uint32_t)v;
+                return 1;
+            }
+            if (++h == nslots) h = 0;
+        }
+        return 0;
+    }
+    CJ_DEV void write_all(const Shared &sh, int64_t key, unsigned long long pos, uint32_t prow,
+                          const MatchOut &out) const {
+        uint32_t r;
+        if (count(sh, key, r) && pos < out.capacity) {
+            if (out.build_rids) out.build_rids[pos] = r;
+            if (out.probe_rids) out.probe_rids[pos] = prow;
+            put_key(out, pos, key);
+        }
+    }
+};
+
 struct LoopMatcher {
     static constexpr bool kAtMostOne = false;
+    static constexpr int kMinBlocks = kProbeMinBlocks;
     static constexpr int kItems = kProbeItems;
     CJ_DEV LoopMatcher resolved() const { return *this; }
     const int64_t *g_keys;
@@ -281,7 +334,7 @@ CJ_DEV void probe_tile(const ColView &pkey, uint32_t n, const M &m, const typena
 }
 
 template <class M>
-__global__ void __launch_bounds__(kProbeThreads, kProbeMinBlocks)
+__global__ void __launch_bounds__(kProbeThreads, M::kMinBlocks)
     k_probe_tiles(ColView pkey_arg, uint32_t n, M m_arg, MatchOut out, TileSched ts) {
     __shared__ typename M::Shared sh;
     __shared__ ProbeSmemT<M::kItems> ps;
@@ -308,7 +361,7 @@ struct GroupedShared {
     };
 };
 
-__global__ void __launch_bounds__(kProbeThreads, kProbeMinBlocks)
+__global__ void __launch_bounds__(kProbeThreads, CJ_GROUPED_MIN_BLOCKS)
     k_probe_grouped(const ProbeTask *__restrict__ tasks, uint32_t ntasks, uint32_t total_tiles,
                     unsigned int *ticket, const uint16_t *__restrict__ g_bloom) {
     __shared__ GroupedShared sh;
@@ -442,6 +495,13 @@ cudaError_t launch_probe_tiles_hash(const Launch &L, const ColView &pkey, uint32
 cudaError_t launch_probe_tiles_array(const Launch &L, const ColView &pkey, uint32_t n_probe, const uint32_t *slots,
                                      const unsigned long long *params, const MatchOut &out, void *sched_mem) {
     ArrayMatcher m{slots, params};
+    return run_tiles(L, pkey, n_probe, m, out, sched_mem);
+}
+
+cudaError_t launch_probe_tiles_open(const Launch &L, const ColView &pkey, uint32_t n_probe,
+                                    const unsigned long long *slots, uint64_t nslots,
+                                    const unsigned long long *dup, const MatchOut &out, void *sched_mem) {
+    OpenMatcher m{slots, nslots, dup};
     return run_tiles(L, pkey, n_probe, m, out, sched_mem);
 }
 

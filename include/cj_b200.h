@@ -165,6 +165,9 @@ typedef struct cj_exec_stats {
     uint64_t kernel_launches;
     uint64_t num_direct_joins; /* hash joins served by a direct-mapped table
                                   (CJ_OPT_DENSE_KEYS); within num_hash_joins */
+    uint64_t num_open_joins;   /* hash joins served by an open-addressing
+                                  table (unique INT32 keys too spread out for
+                                  a direct-mapped one); within num_hash_joins */
 } cj_exec_stats;
 
 /* ------------------------------------------------------------------------ */

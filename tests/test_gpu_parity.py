@@ -219,9 +219,10 @@ def _direct_case(kind, rng):
     raise ValueError(kind)
 
 
-@pytest.mark.parametrize("kind,direct2,direct8", [("dense_i32", 1, 1), ("dense_i64", 1, 1), ("dense_dups", 0, 0),
-                                                  ("spread5", 0, 1), ("sparse", 0, 0), ("extremes", 0, 0)])
-def test_direct_mapped_build(gpu_ctx, kind, direct2, direct8):
+@pytest.mark.parametrize("kind,direct2,direct8,open2,open8", [
+    ("dense_i32", 1, 1, 0, 0), ("dense_i64", 1, 1, 0, 0), ("dense_dups", 0, 0, 0, 0), ("spread5", 0, 1, 1, 0),
+    ("sparse", 0, 0, 1, 1), ("extremes", 0, 0, 1, 1)])
+def test_direct_mapped_build(gpu_ctx, kind, direct2, direct8, open2, open8):
     """Unique build keys spread over at most CJ_OPT_DENSE_KEYS times the
     build rows take a direct-mapped table; duplicates, wider spans and the
     option turned off take the hash table. Every path gives the oracle's
@@ -252,14 +253,52 @@ def test_direct_mapped_build(gpu_ctx, kind, direct2, direct8):
     default = gpu_ctx.get_option(_lib.CJ_OPT_DENSE_KEYS)
     assert default == 8
     try:
-        for opt, expect in ((2, direct2), (8, direct8), (0, 0)):
+        for opt, expect, expect_open in ((2, direct2, open2), (8, direct8, open8), (0, 0, 0)):
             gpu_ctx.set_option(_lib.CJ_OPT_DENSE_KEYS, opt)
             r, st = run_product(plan, gpu_ctx)
             assert_same(r, want, f"{kind} dense_keys={opt}")
             assert st.exec["num_direct_joins"] == expect
+            assert st.exec["num_open_joins"] == expect_open
             assert st.exec["num_hash_joins"] == 1
     finally:
         gpu_ctx.set_option(_lib.CJ_OPT_DENSE_KEYS, default)
+
+
+@pytest.mark.parametrize("case", ["unique", "dups", "nulls", "negative", "many_probe_misses", "int64_keys"])
+def test_open_addressing_table(gpu_ctx, case):
+    """Unique INT32 build keys spread far wider than the direct-mapped table
+    allows take the open-addressing table; a repeated key, or INT64 build
+    keys, go on to the hash table. Every case gives the oracle's result."""
+    rng = np.random.default_rng(31)
+    nb, npr = 200_000, 1_000_000
+    kt = L if case == "int64_keys" else I
+    if case == "negative":
+        bkeys = -rng.choice(1 << 30, nb, replace=False).astype(np.int64)
+    elif case == "int64_keys":
+        bkeys = rng.choice(1 << 40, nb, replace=False).astype(np.int64) << 3
+    else:
+        bkeys = rng.choice(1 << 30, nb, replace=False).astype(np.int64) * 2
+    if case == "dups":
+        bkeys[rng.integers(0, nb, 50)] = bkeys[7]
+    bv = (rng.random(nb) > 0.1).astype(np.uint8) if case == "nulls" else None
+    pkeys = bkeys[rng.integers(0, nb, npr)]
+    miss = rng.random(npr) < (0.9 if case == "many_probe_misses" else 0.25)
+    pkeys[miss] = pkeys[miss] + 1  # odd (or shifted) keys: never a build key
+    npt = np.int32 if kt == I else np.int64
+    plan = Plan()
+    plan.inputs.append(ColumnarTable(nb, [encode_column(kt, bkeys.astype(npt), bv),
+                                          encode_column(I, rng.integers(0, 1000, nb).astype(np.int32))]))
+    plan.inputs.append(ColumnarTable(npr, [encode_column(kt, pkeys.astype(npt), (rng.random(npr) > 0.02).astype(np.uint8)),
+                                           encode_column(F, rng.random(npr))]))
+    plan.new_scan_node(0, [(0, kt), (1, I)])
+    plan.new_scan_node(1, [(0, kt), (1, F)])
+    plan.new_join_node(True, 0, 1, 0, 0, [(0, kt), (1, I), (3, F)])
+    plan.root = 2
+    r, st = run_product(plan, gpu_ctx)
+    assert_same(r, run_oracle(plan), case)
+    assert st.exec["num_direct_joins"] == 0
+    assert st.exec["num_open_joins"] == (0 if case in ("dups", "int64_keys") else 1)
+    assert st.exec["num_hash_joins"] == 1
 
 
 def test_direct_mapped_all_null_build(gpu_ctx):
