@@ -237,8 +237,8 @@ cudaError_t launch_build_grouped(const Launch &L, const BuildTask *tasks_dev, ui
  * slots[key - lo] = build row, decided on the device. `params` (6 u64, set
  * by the caller to {~0, 0, 0, 0, 0, 0}) receives [0] min and [1] max of the
  * non-NULL keys (XOR 2^63: unsigned order is signed order), [2] their count,
- * [3] 1 when the table cannot be used (span above max_span, or a repeated
- * key), [4] lo, [5] span. `slots` holds max_span entries. Four launches, no
+ * [3] non-zero when the table cannot be used (1: span above max_span, 2: a
+ * repeated key), [4] lo, [5] span. `slots` holds max_span entries. Four launches, no
  * host round trip. */
 constexpr uint32_t kArrayEmpty = 0xFFFFFFFFu;
 constexpr int kDirectParams = 6;

@@ -451,13 +451,14 @@ Relation Executor::exec_join(uint64_t node_idx, int depth, bool is_root, cj_resu
             }
             ctx.sync_status();
             if (direct && ctx.h_status->aux[3]) {
-                /* keys too spread out, or a key repeats: the direct-mapped
-                 * table is unusable (the probe did nothing); an
-                 * open-addressing table, else the hash table */
+                /* keys too spread out (1) or a key repeats (2): the
+                 * direct-mapped table is unusable (the probe did nothing);
+                 * an open-addressing table for spread-out keys, else the
+                 * hash table */
                 direct = false;
                 slots.reset();
                 PhaseScope ph(*this, PH_BUILD);
-                open = build_open();
+                open = ctx.h_status->aux[3] == 1 && build_open();
                 if (!open) build_hash();
                 continue;
             }

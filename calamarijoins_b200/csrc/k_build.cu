@@ -381,7 +381,7 @@ __global__ void __launch_bounds__(kBuildThreads)
 }
 
 /* params: [0] min ^ 2^63, [1] max ^ 2^63, [2] count (from k_key_range),
- * [3] unusable, [4] lo, [5] span. */
+ * [3] unusable (1: span too wide, 2: a key repeats), [4] lo, [5] span. */
 __global__ void k_array_prep(unsigned long long *p, uint64_t max_span) {
     if (p[2] == 0) return; /* no non-NULL key: span 0, nothing matches */
     const unsigned long long width = p[1] - p[0]; /* max - min: the bias cancels */
@@ -407,7 +407,7 @@ __global__ void k_array_build(ColView key, uint32_t n, uint32_t *__restrict__ sl
         if (!load_key(key, (uint32_t)i, &k)) continue;
         const uint64_t off = (uint64_t)k - lo;
         if (off >= span) continue; /* cannot happen: lo and span come from these keys */
-        if (atomicCAS(slots + off, kArrayEmpty, (uint32_t)i) != kArrayEmpty) p[3] = 1ull;
+        if (atomicCAS(slots + off, kArrayEmpty, (uint32_t)i) != kArrayEmpty) p[3] = 2ull; /* a key repeats */
     }
 }
 
@@ -422,18 +422,25 @@ __global__ void k_open_fill(unsigned long long *__restrict__ slots, uint64_t nsl
 
 /* Each non-NULL key claims the first empty slot from its hash on (at most
  * half the slots fill, so a free one is always found); meeting its own key
- * on the way means the key repeats. */
+ * on the way means the key repeats. A slot is read before it is CASed
+ * (slots only go from empty to full, so a full one read from L2 is final):
+ * the copies of a heavily repeated key see it taken without hammering one
+ * address with atomics, and once a repeat is flagged every thread stops. */
 __global__ void k_open_insert(ColView key, uint32_t n, unsigned long long *__restrict__ slots, uint64_t nslots,
                               unsigned long long *dup) {
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        if (*reinterpret_cast<volatile unsigned long long *>(dup)) return;
         int64_t k;
         if (!load_key(key, (uint32_t)i, &k)) continue;
         const unsigned long long v = ((unsigned long long)(uint32_t)k << 32) | (unsigned long long)i;
         uint64_t h = __umul64hi(hash_key(k), nslots);
         for (uint64_t step = 0; step < nslots; ++step) {
-            const unsigned long long old = atomicCAS(slots + h, kOpenEmpty, v);
-            if (old == kOpenEmpty) break;
-            if ((uint32_t)(old >> 32) == (uint32_t)k) {
+            unsigned long long cur = __ldcg(slots + h);
+            if (cur == kOpenEmpty) {
+                cur = atomicCAS(slots + h, kOpenEmpty, v);
+                if (cur == kOpenEmpty) break;
+            }
+            if ((uint32_t)(cur >> 32) == (uint32_t)k) {
                 *dup = 1ull;
                 break;
             }
