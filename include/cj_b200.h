@@ -202,8 +202,10 @@ typedef enum cj_option {
                                          times its row count (and 2^28
                                          values) uses a direct-mapped table
                                          (slot = key - min) instead of the
-                                         hash table; same results; 0 = off;
-                                         default 8                          */
+                                         hash table; unique INT32 keys that
+                                         span more use an open-addressing
+                                         table; same results; 0 = both off
+                                         (hash table only); default 8       */
     CJ_OPT_BUFFER_CACHE_BYTES = 7     /* device buffers freed by a plan are
                                          kept for the next one up to this
                                          many bytes (default 16 GiB; 0 = off;
