@@ -31,6 +31,8 @@ the data path ("scaling": "weak").
 Other workloads (not the default line; --workload):
   c1  100K x 1M join (INT32 build payload, INT64 probe payload), same
       measurements as the default line.
+  c2s C2 with the build keys spread 500x (unique multiples of 500): the
+      open-addressing table instead of the direct-mapped one.
   c3  6-way left-deep join: a 36M-row fact table with 5 foreign keys into
       dimensions of 2.5K-4.2M rows (pre-filtered to 10-40 %), VARCHAR
       outputs (lengths log-normal, mean 20 B, 0.01 % long strings);
@@ -71,6 +73,11 @@ WORKLOADS = {
            "desc": ("C1: build 100,000 unique shuffled INT32 keys + INT32 payload; probe 1,000,000 rows, INT32 FK "
                     "Zipf(1.0), 5% NULL, + INT64 payload; output build key, build payload, probe payload"),
            "units": "probe rows"},
+    "c2s": {"metric": "probe rows/s, 4M x 64M INT32 equi-join, build keys spread 500x (plain execute)",
+            "unit": UNIT,
+            "desc": ("C2 with the 4,000,000 unique build keys spread over multiples of 500 below 2^31 (too wide "
+                     "for a direct-mapped table: open-addressing table); probe and outputs as C2"),
+            "units": "probe rows"},
     "c3": {"metric": "fact rows/s, 6-way join of a 36M-row fact table (plain execute)", "unit": UNIT,
            "desc": ("C3: fact 36,000,000 rows x 5 INT32 FKs (Zipf 0.5-1.2) into dimensions of 2,500 / 130,000 / "
                     "1,200,000 / 2,500,000 / 4,200,000 rows kept at 40/40/30/20/10 %; outputs the fact's first FK, "
@@ -227,6 +234,11 @@ def algorithmic_bytes(kernel: str, st: dict, plan_info: dict):
         # build rows) once; per match 2 x 4 B row ids and the 4 B key the
         # probe emits for the root's key columns
         return npr * (4 + 1 / 8) + nb * 4 + m * 12
+    if kernel == "probe_open":
+        # probe keys (4 B + validity bit), the open-addressing table (8 B
+        # slots, 2 per build row) once; per match 2 x 4 B row ids and the
+        # 4 B key the probe emits for the root's key columns
+        return npr * (4 + 1 / 8) + nb * 2 * 8 + m * 12
     if kernel == "write_pages_int32":
         # per output row: 4 B match row id + 4 B value + validity bit read; page bytes written
         pages = (m + 1983) // 1984
@@ -253,6 +265,9 @@ def gen_workload(pinned: bool, scale: float, int32_standin: bool = False, worklo
         return config_c1(scale=scale, pinned=pinned)
     if workload == "c3":  # INT32 keys, VARCHAR without NULLs: the reference runs it as it is
         return config_c3(scale=scale, pinned=pinned)
+    if workload == "c2s":
+        from calamarijoins_b200.datagen import config_c2s
+        return config_c2s(scale=scale, pinned=pinned, int32_standin=int32_standin)
     if int32_standin:
         return join2(max(int(4_000_000 * scale), 16), max(int(64_000_000 * scale), 16), seed=202, zipf=0.8,
                      outside=0.30, probe_null=0.02, build_payload=(DataType.INT32,),
@@ -675,7 +690,7 @@ def main(argv=None):
     ap.add_argument("--cpu-scale", type=float, default=0.25, help="scale of the CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-worker", type=int, default=0, help=argparse.SUPPRESS)
-    ap.add_argument("--workload", choices=["c2", "c1", "c3", "c4", "c5"], default="c2",
+    ap.add_argument("--workload", choices=["c2", "c1", "c2s", "c3", "c4", "c5"], default="c2",
                     help="c2 (default): the headline line; the others: see the module docstring")
     args = ap.parse_args(argv)
     global WL

@@ -37,6 +37,13 @@ CJ_DEV uint32_t slot_of(uint64_t h, int log2_slots) {
 
 CJ_DEV uint32_t bloom_index(uint64_t h) { return (uint32_t)(h & 0x7FFu); }
 
+/* First slot of an INT32 key in an open-addressing table of nslots (< 2^32)
+ * slots: Knuth's multiplicative hashing (the key times 2^32 / golden ratio,
+ * mod 2^32), whose top bits are scaled to [0, nslots). Two instructions. */
+CJ_DEV uint32_t open_slot(int64_t key, uint32_t nslots) {
+    return __umulhi((uint32_t)key * 0x9E3779B9u, nslots);
+}
+
 /* Loads the 2048-entry Bloom tag table into shared memory. */
 CJ_DEV void load_bloom(uint16_t *s_bloom, const uint16_t *g_bloom) {
     const uint32_t *src = reinterpret_cast<const uint32_t *>(g_bloom);

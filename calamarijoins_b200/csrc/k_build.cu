@@ -426,15 +426,15 @@ __global__ void k_open_fill(unsigned long long *__restrict__ slots, uint64_t nsl
  * (slots only go from empty to full, so a full one read from L2 is final):
  * the copies of a heavily repeated key see it taken without hammering one
  * address with atomics, and once a repeat is flagged every thread stops. */
-__global__ void k_open_insert(ColView key, uint32_t n, unsigned long long *__restrict__ slots, uint64_t nslots,
+__global__ void k_open_insert(ColView key, uint32_t n, unsigned long long *__restrict__ slots, uint32_t nslots,
                               unsigned long long *dup) {
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
         if (*reinterpret_cast<volatile unsigned long long *>(dup)) return;
         int64_t k;
         if (!load_key(key, (uint32_t)i, &k)) continue;
         const unsigned long long v = ((unsigned long long)(uint32_t)k << 32) | (unsigned long long)i;
-        uint64_t h = __umul64hi(hash_key(k), nslots);
-        for (uint64_t step = 0; step < nslots; ++step) {
+        uint32_t h = open_slot(k, nslots);
+        for (uint32_t step = 0; step < nslots; ++step) {
             unsigned long long cur = __ldcg(slots + h);
             if (cur == kOpenEmpty) {
                 cur = atomicCAS(slots + h, kOpenEmpty, v);
@@ -532,11 +532,11 @@ cudaError_t launch_direct_build(const Launch &L, const ColView &key, uint32_t n,
 
 cudaError_t launch_open_build(const Launch &L, const ColView &key, uint32_t n, unsigned long long *slots,
                               uint64_t nslots, unsigned long long *dup) {
-    if (nslots < 2ull * n) return cudaErrorInvalidValue; /* the insert loop needs free slots */
+    if (nslots < 2ull * n || nslots > 0xFFFFFFFFull) return cudaErrorInvalidValue; /* free slots; u32 indices */
     uint64_t g = std::min<uint64_t>(std::max<uint64_t>((nslots + 255) / 256, 1), (uint64_t)L.num_sms * 8);
     k_open_fill<<<(unsigned)g, 256, 0, L.stream>>>(slots, nslots);
     g = std::min<uint64_t>(std::max<uint64_t>(((uint64_t)n + 255) / 256, 1), (uint64_t)L.num_sms * 8);
-    k_open_insert<<<(unsigned)g, 256, 0, L.stream>>>(key, n, slots, nslots, dup);
+    k_open_insert<<<(unsigned)g, 256, 0, L.stream>>>(key, n, slots, (uint32_t)nslots, dup);
     count_launches(2);
     return cudaGetLastError();
 }

@@ -178,7 +178,7 @@ struct OpenMatcher {
     static constexpr int kItems = 4;
     static constexpr int kMinBlocks = kProbeMinBlocks;
     const unsigned long long *slots;
-    uint64_t nslots;
+    uint32_t nslots; /* < 2^32 (launch_probe_tiles_open checks) */
     const unsigned long long *dup;
     struct Shared {
         uint32_t unused;
@@ -188,8 +188,8 @@ struct OpenMatcher {
     CJ_DEV void init(Shared &) const {}
     CJ_DEV uint32_t count(const Shared &, int64_t key, uint32_t &first) const {
         if (key != (int64_t)(int32_t)key) return 0; /* no INT32 build key equals it */
-        uint64_t h = __umul64hi(hash_key(key), nslots);
-        for (uint64_t step = 0; step < nslots; ++step) {
+        uint32_t h = open_slot(key, nslots);
+        for (uint32_t step = 0; step < nslots; ++step) {
             const unsigned long long v = __ldg(slots + h);
             if (v == ~0ull) return 0;
             if ((int32_t)(uint32_t)(v >> 32) == (int32_t)key) {
@@ -501,7 +501,8 @@ cudaError_t launch_probe_tiles_array(const Launch &L, const ColView &pkey, uint3
 cudaError_t launch_probe_tiles_open(const Launch &L, const ColView &pkey, uint32_t n_probe,
                                     const unsigned long long *slots, uint64_t nslots,
                                     const unsigned long long *dup, const MatchOut &out, void *sched_mem) {
-    OpenMatcher m{slots, nslots, dup};
+    if (nslots > 0xFFFFFFFFull) return cudaErrorInvalidValue;
+    OpenMatcher m{slots, (uint32_t)nslots, dup};
     return run_tiles(L, pkey, n_probe, m, out, sched_mem);
 }
 

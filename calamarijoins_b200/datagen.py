@@ -127,14 +127,16 @@ def fk_column(build_keys: np.ndarray, n: int, s: float, outside: float, null_fra
 def join2(n_build: int, n_probe: int, *, seed: int = 1, zipf: float = 1.0, outside: float = 0.0,
           build_null: float = 0.0, probe_null: float = 0.0, key_type=DataType.INT32,
           build_payload=(DataType.INT32,), probe_payload=(DataType.INT64,), build_left: bool = True,
-          output=None, pinned: bool = False, unique_build: bool = True, varchar_kw=None) -> Plan:
+          output=None, pinned: bool = False, unique_build: bool = True, varchar_kw=None,
+          key_scale: int = 1) -> Plan:
     """A 2-table equi-join plan: table 0 (build candidate) = key + build
     payloads, table 1 = foreign key + probe payloads. `output` lists
-    (side, column) pairs over (left ++ right); default = every column."""
+    (side, column) pairs over (left ++ right); default = every column.
+    Unique build keys are a permutation of 0, key_scale, 2 key_scale, ..."""
     rng = np.random.default_rng(seed)
     vkw = varchar_kw or {}
     if unique_build:
-        bkeys = rng.permutation(n_build).astype(np.int64)
+        bkeys = rng.permutation(n_build).astype(np.int64) * key_scale
     else:
         bkeys = rng.integers(0, max(n_build // 4, 1), size=n_build).astype(np.int64)
     npt = np.int32 if key_type == DataType.INT32 else np.int64
@@ -174,6 +176,17 @@ def config_c2(seed: int = 202, scale: float = 1.0, pinned: bool = False) -> Plan
     return join2(nb, npr, seed=seed, zipf=0.8, outside=0.30, probe_null=0.02,
                  build_payload=(DataType.INT64,), probe_payload=(DataType.FP64,), output=[0, 1, 2, 3],
                  pinned=pinned)
+
+
+def config_c2s(seed: int = 212, scale: float = 1.0, pinned: bool = False, int32_standin: bool = False) -> Plan:
+    """C2's shape with the build keys spread 500x (unique multiples of 500
+    below 2^31): too wide for a direct-mapped table, so the join takes the
+    open-addressing table."""
+    nb, npr = max(int(4_000_000 * scale), 16), max(int(64_000_000 * scale), 16)
+    payloads = (DataType.INT32,) if int32_standin else None
+    return join2(nb, npr, seed=seed, zipf=0.8, outside=0.30, probe_null=0.02,
+                 build_payload=payloads or (DataType.INT64,), probe_payload=payloads or (DataType.FP64,),
+                 output=[0, 1, 2, 3], pinned=pinned, key_scale=500)
 
 
 C3_DIMS = (2_500, 130_000, 1_200_000, 2_500_000, 4_200_000)
