@@ -7,7 +7,8 @@ import numpy as np
 import pytest
 
 from calamarijoins_b200 import DataType, PlanDescriptor
-from calamarijoins_b200.datagen import chain_plan, config_c3, join2
+from calamarijoins_b200 import decode_column
+from calamarijoins_b200.datagen import chain_plan, config_c2s, config_c3, join2
 from oracle import oracle_api as oa
 
 pytestmark = pytest.mark.skipif(not oa.ref_available(), reason="reference not compiled (oracle/build_oracle.py)")
@@ -48,3 +49,13 @@ def test_chains(seed):
 def test_c3_small():
     o = agree(config_c3(seed=5, scale=0.002, varchar_nulls=False, long_frac=0.002))
     assert o.num_rows > 0
+
+
+def test_c2s_small():
+    """C2s's spread build keys (unique multiples of 500 below 2^31, probe keys
+    outside the domain above them) are inside the reference's domain."""
+    plan = config_c2s(scale=0.005, int32_standin=True)
+    keys, valid = decode_column(plan.inputs[0].columns[0])
+    assert len(np.unique(keys)) == len(keys) and (keys % 500 == 0).all() and keys.max() < 2 ** 31
+    o = agree(plan)
+    assert 0 < o.num_rows < plan.inputs[1].num_rows
