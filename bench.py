@@ -96,6 +96,46 @@ def rank_info():
             int(os.environ.get("LOCAL_RANK", "0")))
 
 
+class Replicas:
+    """One process per GPU (torchrun): each rank runs its own replica of the
+    workload; the only collectives are the barriers around a timed region and
+    the maximum over ranks of each measured time (no collective on the data
+    path). With one rank every call is a no-op."""
+
+    def __init__(self, backend: str = "nccl", device: str = "cpu", timeout_s: int = 120):
+        self.rank, self.world, self.local = rank_info()
+        self.device = device
+        self.dist = None
+        if self.world > 1:
+            import datetime
+            import torch.distributed as dist
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=timeout_s))
+            self.dist = dist
+
+    def barrier(self):
+        if self.dist:
+            self.dist.barrier()
+
+    def max(self, x: float) -> float:
+        """The largest `x` over the ranks (every rank gets it)."""
+        if not self.dist:
+            return x
+        import torch
+        t = torch.tensor([float(x)], dtype=torch.float64, device=self.device)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.dist:
+            self.dist.destroy_process_group()
+            self.dist = None
+
+
+def whole_job_rate(units_per_rank: int, world: int, seconds_max: float) -> float:
+    """Units all ranks processed over the slowest rank's time."""
+    return units_per_rank * world / seconds_max
+
+
 class ClockSampler:
     """SM clock and clock-event-reason samples during the timed region.
 
@@ -395,11 +435,7 @@ def run_ours(args):
 
     rank, world, local = rank_info()
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    reps = Replicas("nccl", device=f"cuda:{local}")
 
     ctx = cj.Context(local)
     log("generating workload")
@@ -431,8 +467,7 @@ def run_ours(args):
     for _ in range(args.warmup):
         st = step_device()
     log("timed device steps")
-    if dist:
-        dist.barrier()
+    reps.barrier()
     torch.cuda.synchronize()
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
     launches = 0
@@ -447,11 +482,8 @@ def run_ours(args):
     clk.stop()
     ms_total = ev[0].elapsed_time(ev[-1])
     step_ms = [ev[i].elapsed_time(ev[i + 1]) for i in range(args.steps)]
-    if dist:
-        t = torch.tensor([ms_total], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_total = float(t.item())
-        dist.barrier()
+    ms_total = reps.max(ms_total)
+    reps.barrier()
     # per-kernel times (CUDA events around every launch) from a separate
     # pass over the same steps, so the headline steps carry no event records
     ctx.set_option(_lib.CJ_OPT_PROFILE_KERNELS, 1)
@@ -462,16 +494,14 @@ def run_ours(args):
     prof = ctx.profile()
     ctx.set_option(_lib.CJ_OPT_PROFILE_KERNELS, 0)
     ms_step = ms_total / args.steps
-    probe_rows = info["probe_rows"] * world
-    value = probe_rows / (ms_step / 1000.0)
+    value = whole_job_rate(info["probe_rows"], world, ms_step / 1000.0)
 
     # e2e through the public API with host buffers
     log("end-to-end steps")
     for _ in range(max(1, args.warmup)):
         res, st_h = cj.execute_raw(plan, ctx, 0, d_host)
         res.free()
-    if dist:
-        dist.barrier()
+    reps.barrier()
     walls = []
     h2d = d2h = 0
     for _ in range(args.steps):
@@ -482,11 +512,8 @@ def run_ours(args):
         h2d, d2h = st_h.exec["h2d_bytes"], st_h.exec["d2h_bytes"]
     e2e_s = statistics.mean(walls)
     e2e_steps = {"min": min(walls) * 1e3, "median": statistics.median(walls) * 1e3, "max": max(walls) * 1e3}
-    if dist:
-        t = torch.tensor([e2e_s], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e_value = probe_rows / e2e_s
+    e2e_s = reps.max(e2e_s)
+    e2e_value = whole_job_rate(info["probe_rows"], world, e2e_s)
 
     log("cpu baseline")
     # roofline of the dominant kernel
@@ -537,8 +564,7 @@ def run_ours(args):
     for t in resident.inputs:
         t.free()
     ctx.close()
-    if dist:
-        dist.destroy_process_group()
+    reps.close()
     return 0
 
 
