@@ -426,6 +426,35 @@ def run_reference(args):
     return 0
 
 
+def check_parity(plan, resident, ctx, d_res):
+    """Checker, outside every timed region: the row-multiset fingerprint of
+    one device result of the benchmarked plan (copied back) against the
+    fingerprint of the oracle's result for the same host pages."""
+    import calamarijoins_b200 as cj
+    from calamarijoins_b200 import _lib
+    from oracle import oracle_api as oa
+    res, _ = cj.execute_raw(resident, ctx, _lib.CJ_EXEC_RESULT_ON_DEVICE, d_res)
+    try:
+        got = oa.PagedResult.from_result(res)
+    finally:
+        res.free()
+    ok_pages, msg = oa.validate(got)
+    fp_gpu = oa.fingerprint(got)
+    rows_gpu = got.num_rows
+    del got
+    t0 = time.perf_counter()
+    want = oa.oracle_execute(cj.PlanDescriptor(plan))
+    oracle_s = time.perf_counter() - t0
+    fp_oracle = oa.fingerprint(want)
+    return {"equal": bool(ok_pages and fp_gpu == fp_oracle and rows_gpu == want.num_rows),
+            "pages_valid": bool(ok_pages), "page_error": msg or None,
+            "rows": rows_gpu, "oracle_rows": want.num_rows,
+            "fingerprint": f"{fp_gpu:016x}", "oracle_fingerprint": f"{fp_oracle:016x}",
+            "method": ("order-insensitive fingerprint of the row multiset (values, NULLs, bytes) of one "
+                       "device-resident execution against the oracle's (oracle/cj_oracle.c) on the same pages; "
+                       f"oracle {oracle_s:.1f} s single-threaded")}
+
+
 def run_ours(args):
     import ctypes as C
     import numpy as np
@@ -515,6 +544,10 @@ def run_ours(args):
     e2e_s = reps.max(e2e_s)
     e2e_value = whole_job_rate(info["probe_rows"], world, e2e_s)
 
+    parity = None
+    if rank == 0 and not args.no_parity:
+        log("parity: result fingerprint against the oracle's")
+        parity = check_parity(plan, resident, ctx, d_res)
     log("cpu baseline")
     # roofline of the dominant kernel
     peak, peak_kind = measured_peaks()
@@ -557,7 +590,7 @@ def run_ours(args):
                            "output_rows": st.exec["output_rows"], "output_pages": st.exec["output_pages"]},
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                         "ms_per_step": e2e_s * 1000.0, "step_ms": e2e_steps},
-                "roofline": roof, "cpu_baseline": cpu, "gpu_launches": launches,
+                "roofline": roof, "cpu_baseline": cpu, "gpu_launches": launches, "parity": parity,
                 "clocks": clk.summary(), "kernels": kernels,
                 "phases_us": {k: st.exec[k] for k in ("decode_us", "build_us", "probe_us", "materialize_us")}}
         print(json.dumps(line))
@@ -570,42 +603,66 @@ def run_ours(args):
 
 def run_batch(args):
     """c4: plans/s of 256 plans, batched (cj_execute_batch) and looped
-    (cj_execute), host pages in and out; the reference's execute() over
-    the same plans on the host cores."""
+    (cj_execute), twice: with the inputs' pages resident in HBM and results
+    left on the device, and with host pages in and host pages out; the
+    reference's execute() over the same plans on the host cores."""
     import calamarijoins_b200 as cj
+    from calamarijoins_b200 import _lib
     from calamarijoins_b200.datagen import batch_plans
     ctx = cj.Context(0)
     log("generating 256 plans")
     plans = batch_plans(C4_PLANS, seed=C4_SEED, scale=args.scale, pinned=True)
     descs = [cj.PlanDescriptor(p) for p in plans]
     rows = sum(p.inputs[0].num_rows for p in plans)
+    log("uploading resident tables")
+    rplans, tables = [], []
+    for p in plans:
+        rp = cj.Plan()
+        rp.nodes, rp.root = p.nodes, p.root
+        rp.inputs = [cj.ResidentTable(ctx, t) for t in p.inputs]
+        tables.extend(rp.inputs)
+        rplans.append(rp)
+    rdescs = [cj.PlanDescriptor(p) for p in rplans]
+    gc.collect()
+    gc.freeze()
 
-    def batched():
-        results, statuses, st = cj.execute_batch(plans, ctx, descs=descs)
-        assert all(x == 0 for x in statuses), statuses
-        for r in results:
-            r.free()
-        return st
+    def batched(ps, ds, flags):
+        def fn():
+            results, statuses, st = cj.execute_batch(ps, ctx, flags, descs=ds)
+            assert all(x == 0 for x in statuses), statuses
+            for r in results:
+                r.free()
+            return st
+        return fn
 
-    def looped():
-        for p, d in zip(plans, descs):
-            r, _ = cj.execute_raw(p, ctx, 0, d)
-            r.free()
+    def looped(ps, ds, flags):
+        def fn():
+            for p, d in zip(ps, ds):
+                r, _ = cj.execute_raw(p, ctx, flags, d)
+                r.free()
+        return fn
 
+    dev = _lib.CJ_EXEC_RESULT_ON_DEVICE
+    arms = {"resident": {"batched": batched(rplans, rdescs, dev), "looped": looped(rplans, rdescs, dev)},
+            "host": {"batched": batched(plans, descs, 0), "looped": looped(plans, descs, 0)}}
     out = {}
-    for name, fn in (("batched", batched), ("looped", looped)):
-        log(f"{name}: warm-up")
-        for _ in range(args.warmup):
-            fn()
-        walls = []
-        for _ in range(args.steps):
-            t0 = time.perf_counter()
-            fn()
-            walls.append(time.perf_counter() - t0)
-        out[name] = {"plans_per_s": C4_PLANS / statistics.mean(walls), "ms_per_pass": statistics.mean(walls) * 1e3,
-                     "pass_ms": {"min": min(walls) * 1e3, "median": statistics.median(walls) * 1e3,
-                                 "max": max(walls) * 1e3}}
-    st = batched()
+    for where, fns in arms.items():
+        out[where] = {}
+        for name, fn in fns.items():
+            log(f"{where} {name}: warm-up")
+            for _ in range(args.warmup):
+                fn()
+            walls = []
+            for _ in range(args.steps):
+                t0 = time.perf_counter()
+                fn()
+                walls.append(time.perf_counter() - t0)
+            out[where][name] = {"plans_per_s": C4_PLANS / statistics.mean(walls),
+                                "ms_per_pass": statistics.mean(walls) * 1e3,
+                                "pass_ms": {"min": min(walls) * 1e3, "median": statistics.median(walls) * 1e3,
+                                            "max": max(walls) * 1e3}}
+        out[where]["batched_over_looped"] = out[where]["batched"]["plans_per_s"] / out[where]["looped"]["plans_per_s"]
+    st = arms["resident"]["batched"]()
     ref = None
     if not args.no_cpu_baseline:
         r = time_reference(args.scale, 1, 3)
@@ -614,17 +671,21 @@ def run_batch(args):
                    "kind": "reference", "sample": (f"the reference's execute() over the same {C4_PLANS} plans one "
                                                    f"after another, median of 3 passes after 1 warm-up; best of "
                                                    f"thread counts {sorted(r['all_ms'])} on {os.cpu_count()} CPUs")}
-    line = {"metric": "plans/s, 256 batched 2-4-way INT32 plans", "value": out["batched"]["plans_per_s"],
+    line = {"metric": "plans/s, 256 batched 2-4-way INT32 plans", "value": out["resident"]["batched"]["plans_per_s"],
             "unit": "plans/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": out["batched"]["ms_per_pass"], "higher_is_better": True, "scaling": "weak",
+            "ms_per_step": out["resident"]["batched"]["ms_per_pass"], "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "int32", "data": "synthetic",
             "config": {"workload": ("C4: 256 seeded 2-4-way INT32 chain plans, builds log-uniform 10-1e6 rows, "
-                                    "probes 1e3-1e7 rows; host pages in, host pages out"), "scale": args.scale,
-                       "fact_rows_total": rows},
-            "batched": out["batched"], "looped": out["looped"],
+                                    "probes 1e3-1e7 rows; value: inputs resident in HBM, results on the device"),
+                       "scale": args.scale, "fact_rows_total": rows},
+            "resident": out["resident"], "host": out["host"],
+            "e2e": {"value": out["host"]["batched"]["plans_per_s"], "unit": "plans/s",
+                    "note": "host pages in, host pages out, through cj_execute_batch"},
             "batch_stats": {k: st[k] for k in ("num_levels", "num_joins", "kernel_launches", "syncs")},
             "cpu_baseline": ref}
     print(json.dumps(line))
+    for t in tables:
+        t.free()
     ctx.close()
     return 0
 
@@ -713,7 +774,8 @@ def main(argv=None):
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--scale", type=float, default=1.0, help="row-count scale of the workload")
-    ap.add_argument("--cpu-scale", type=float, default=0.25, help="scale of the CPU-baseline sample")
+    ap.add_argument("--cpu-scale", type=float, default=1.0, help="scale of the CPU-baseline sample")
+    ap.add_argument("--no-parity", action="store_true", help="skip the oracle fingerprint check")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-worker", type=int, default=0, help=argparse.SUPPRESS)
     ap.add_argument("--workload", choices=["c2", "c1", "c2s", "c3", "c4", "c5"], default="c2",

@@ -34,6 +34,7 @@ CJ_OPT_VARCHAR_TILE_ROWS = 4
 CJ_OPT_CTAS_PER_SM = 5
 CJ_OPT_DENSE_KEYS = 6
 CJ_OPT_BUFFER_CACHE_BYTES = 7
+CJ_OPT_FAIL_ALLOC_AT = 8
 
 
 class ColumnDesc(C.Structure):

@@ -13,7 +13,6 @@
  *
  * Build: compile this file instead of src/execute.cpp with
  *   -I<repo>/include  and link  <repo>/calamarijoins_b200/libcj_b200.so
- * (INTEGRATION.md has the CMake lines).
  */
 #include <data_model/plan.h>
 

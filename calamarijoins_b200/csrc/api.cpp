@@ -77,6 +77,10 @@ int cj_context_set_option(cj_context *ctx, int32_t option, int64_t value) {
         set_device(ctx);
         ctx->trim_buffers();
         break;
+    case CJ_OPT_FAIL_ALLOC_AT:
+        if (value < 0) return set_error(CJ_ERR_INVALID_ARGUMENT, "allocation index must be >= 0");
+        ctx->opt.fail_alloc_at = value;
+        break;
     default: return set_error(CJ_ERR_INVALID_ARGUMENT, "unknown option");
     }
     return CJ_OK;
@@ -93,6 +97,7 @@ int cj_context_get_option(const cj_context *ctx, int32_t option, int64_t *value)
     case CJ_OPT_CTAS_PER_SM: *value = ctx->opt.ctas_per_sm; break;
     case CJ_OPT_DENSE_KEYS: *value = ctx->opt.dense_keys; break;
     case CJ_OPT_BUFFER_CACHE_BYTES: *value = ctx->opt.buffer_cache_bytes; break;
+    case CJ_OPT_FAIL_ALLOC_AT: *value = ctx->opt.fail_alloc_at; break;
     default: return set_error(CJ_ERR_INVALID_ARGUMENT, "unknown option");
     }
     return CJ_OK;

@@ -26,6 +26,8 @@
 #include <memory>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "exec_common.h"
 
 namespace cj {
@@ -523,8 +525,20 @@ void BatchExecutor::run(cj_result **results, int32_t *statuses, cj_batch_stats *
             p.root_types.push_back(c.type);
         }
     }
-    for (int lvl = 1; lvl <= maxl; ++lvl) run_level(lvl);
-    materialize_roots();
+    for (int lvl = 1; lvl <= maxl; ++lvl) {
+        nvtxRangePushA("cj:batch_level");
+        struct Pop {
+            ~Pop() { nvtxRangePop(); }
+        } pop;
+        run_level(lvl);
+    }
+    nvtxRangePushA("cj:batch_materialize");
+    {
+        struct Pop {
+            ~Pop() { nvtxRangePop(); }
+        } pop;
+        materialize_roots();
+    }
     ctx.sync_status();
     stats.syncs++;
     for (size_t i = 0; i < ps.size(); ++i) {

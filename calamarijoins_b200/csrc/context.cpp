@@ -77,6 +77,8 @@ DevPtr Context::alloc(size_t bytes) {
     b->ctx = this;
     b->bytes = bytes;
     if (bytes == 0) return b;
+    if (opt.fail_alloc_at > 0 && --opt.fail_alloc_at == 0) /* injected fault (CJ_OPT_FAIL_ALLOC_AT) */
+        fail(CJ_ERR_OUT_OF_MEMORY, "device allocation of " + std::to_string(bytes) + " bytes failed (injected)");
     const size_t cls = device_class(bytes);
     b->cls = cls;
     {

@@ -19,6 +19,8 @@
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "engine.h"
 
 #include "exec_common.h"
@@ -27,6 +29,11 @@ namespace cj {
 namespace {
 
 enum Phase { PH_UPLOAD, PH_DECODE, PH_BUILD, PH_PROBE, PH_NL, PH_INTER, PH_MAT, PH_DOWNLOAD, PH_COUNT };
+/* NVTX range names of the phases (host-side ranges around the enqueueing of
+ * each phase; visible in Nsight Systems timelines). */
+constexpr const char *kPhaseNames[PH_COUNT] = {"cj:upload", "cj:decode",       "cj:build",       "cj:probe",
+                                               "cj:nested_loop", "cj:intermediate", "cj:materialize",
+                                               "cj:download"};
 
 class Executor {
   public:
@@ -53,6 +60,7 @@ class Executor {
     class PhaseScope {
       public:
         PhaseScope(Executor &e, int ph) : e_(e), ph_(ph) {
+            nvtxRangePushA(kPhaseNames[ph]);
             a_ = e.ctx.get_event();
             cudaEventRecord(a_, e.ctx.stream);
         }
@@ -60,6 +68,7 @@ class Executor {
             cudaEvent_t b = e_.ctx.get_event();
             cudaEventRecord(b, e_.ctx.stream);
             e_.phase_events.push_back({ph_, a_, b});
+            nvtxRangePop();
         }
 
       private:
@@ -727,6 +736,10 @@ cj_result *Executor::run(cj_exec_stats *st) {
 } // namespace
 
 cj_result *execute_plan(Context &ctx, const cj_plan_desc &plan, uint32_t flags, cj_exec_stats *stats) {
+    struct Range {
+        Range() { nvtxRangePushA("cj_execute"); }
+        ~Range() { nvtxRangePop(); }
+    } range;
     Executor ex(ctx, plan, flags);
     return ex.run(stats);
 }

@@ -46,6 +46,7 @@ struct Options {
     int64_t ctas_per_sm = 0;
     int64_t dense_keys = 8; /* max key span / build rows for a direct-mapped table; 0 = off */
     int64_t buffer_cache_bytes = 16ll << 30; /* freed device buffers kept for reuse */
+    int64_t fail_alloc_at = 0; /* injected failure of the N-th device allocation from now; 0 = off */
 };
 
 struct Context;

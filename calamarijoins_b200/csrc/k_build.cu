@@ -31,6 +31,8 @@
  * NULL keys are skipped (hashtable.h:439-478).
  */
 #include <algorithm>
+#include <atomic>
+#include <mutex>
 
 #include "cj_device.cuh"
 
@@ -449,9 +451,20 @@ __global__ void k_open_insert(ColView key, uint32_t n, unsigned long long *__res
     }
 }
 
-bool g_attrs_set = false;
+/* cudaFuncSetAttribute applies to the current device only: track which
+ * devices have had the limits raised. */
+constexpr int kMaxAttrDevices = 64;
+std::atomic<bool> g_attrs_set[kMaxAttrDevices];
+std::mutex g_attrs_mu;
 void set_smem_attrs() {
-    if (g_attrs_set) return;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxAttrDevices) {
+        cudaGetLastError();
+        dev = 0;
+    }
+    if (g_attrs_set[dev].load(std::memory_order_acquire)) return;
+    std::lock_guard<std::mutex> lk(g_attrs_mu);
+    if (g_attrs_set[dev].load(std::memory_order_relaxed)) return;
     cudaFuncSetAttribute(k_part_hist, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
     cudaFuncSetAttribute(k_part_scatter<int32_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
     cudaFuncSetAttribute(k_part_scatter<int64_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
@@ -460,7 +473,7 @@ void set_smem_attrs() {
     cudaFuncSetAttribute(k_part_hist_grouped, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
     cudaFuncSetAttribute(k_part_scatter_grouped, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
     cudaFuncSetAttribute(k_part_build_grouped, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
-    g_attrs_set = true;
+    g_attrs_set[dev].store(true, std::memory_order_release);
 }
 
 } // namespace

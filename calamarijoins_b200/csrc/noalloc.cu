@@ -17,8 +17,16 @@
  * device is current, on the first call on that device (that first call
  * should therefore be made before any stream capture). All calls share the
  * array and it keeps the previous call's contents: the parts that must
- * start at zero (error word, tile ticket, match counter) are cleared by every call, and two calls whose work overlaps on
- * the GPU (different streams or threads at the same time) race on it.
+ * start at zero (tile ticket, match counter) are cleared by every call, and
+ * the directory and tuples are rewritten in full; two calls whose work
+ * overlaps on the GPU (different streams or threads at the same time) race
+ * on it.
+ *
+ * Output order: the probe hands out tiles from an atomic ticket and each
+ * tile reserves its output range with one atomicAdd, so pairs keep probe
+ * order only within a tile; across tiles the order is unspecified, and when
+ * capacity is below the match count the pairs written are an arbitrary
+ * subset of them (call again with capacity >= *d_count for all of them).
  */
 #include <cstring>
 #include <mutex>
@@ -43,8 +51,10 @@ struct DeviceScratch {
 DeviceScratch g_dev[kMaxDevices];
 std::mutex g_mu;
 
-/* layout: [error word | Bloom tags | directory | tuples | build scratch |
- * probe scratch], each 256-byte aligned */
+/* layout: [reserved word | Bloom tags | directory | tuples | build scratch |
+ * probe scratch], each 256-byte aligned. The build and probe kernels of
+ * this path raise no device error bits; the launch's error word points at
+ * the reserved word only because the launch descriptor requires one. */
 constexpr size_t kErrOff = 0;
 constexpr size_t kBloomOff = 256;
 constexpr size_t kDirOff = kBloomOff + 4096;
@@ -119,8 +129,6 @@ extern "C" int cj_hash_join_noalloc(const int32_t *build_keys, const uint32_t *b
     L.block_threads = 0;
     L.dev_errors = reinterpret_cast<unsigned int *>(ds->base + kErrOff);
 
-    e = cudaMemsetAsync(ds->base + kErrOff, 0, 256, s);
-    if (e != cudaSuccess) return cuda_status(e, "cudaMemsetAsync");
     if (n_build && n_probe) {
         cj::BuildPlan bp;
         bp.num_rows = n_build;
@@ -162,10 +170,6 @@ extern "C" int cj_hash_join_noalloc(const int32_t *build_keys, const uint32_t *b
     }
     e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return cuda_status(e, "cudaStreamSynchronize");
-    unsigned int err = 0;
-    e = cudaMemcpy(&err, ds->base + kErrOff, sizeof(err), cudaMemcpyDeviceToHost);
-    if (e != cudaSuccess) return cuda_status(e, "cudaMemcpy");
-    if (err) return cj::set_last_error(CJ_ERR_INTERNAL, "device reported error bits " + std::to_string(err));
     if (h_count) {
         e = cudaMemcpy(h_count, d_count, sizeof(uint64_t), cudaMemcpyDeviceToHost);
         if (e != cudaSuccess) return cuda_status(e, "cudaMemcpy");

@@ -206,10 +206,17 @@ typedef enum cj_option {
                                          span more use an open-addressing
                                          table; same results; 0 = both off
                                          (hash table only); default 8       */
-    CJ_OPT_BUFFER_CACHE_BYTES = 7     /* device buffers freed by a plan are
+    CJ_OPT_BUFFER_CACHE_BYTES = 7,    /* device buffers freed by a plan are
                                          kept for the next one up to this
                                          many bytes (default 16 GiB; 0 = off;
                                          always 0 for server workers)       */
+    CJ_OPT_FAIL_ALLOC_AT = 8          /* fault injection on the host: the
+                                         N-th device allocation of this
+                                         context from now on fails as if the
+                                         pool were exhausted (the call
+                                         returns CJ_ERR_OUT_OF_MEMORY and the
+                                         context stays usable); one-shot;
+                                         0 = off (default)                  */
 } cj_option;
 int cj_context_set_option(cj_context *ctx, int32_t option, int64_t value);
 int cj_context_get_option(const cj_context *ctx, int32_t option, int64_t *value);
@@ -335,9 +342,13 @@ int cj_execute_batch(cj_context *ctx, const cj_plan_desc *plans,
  * in the reference. All pointers are device pointers except h_count (host,
  * may be NULL); valid arrays are bitmaps of ceil(n/32) u32 words, bit r set
  * when row r has a key (NULL keys never match). The matching (build row,
- * probe row) pairs are written in probe-row order to out_build_rows /
- * out_probe_rows (at most `capacity` of them); *d_count receives the full
- * match count, and *h_count too when given. Work runs on `stream`
+ * probe row) pairs are written to out_build_rows / out_probe_rows (at most
+ * `capacity` of them) in an unspecified order: probe order within each
+ * tile of probe rows, tiles in the order they finish counting. *d_count
+ * receives the full match count, and *h_count too when given; when it
+ * exceeds `capacity` the pairs written are an arbitrary subset (nothing is
+ * written past `capacity`): call again with capacity >= *d_count to get
+ * them all. Work runs on `stream`
  * (a cudaStream_t) and the call returns after it completes.
  * Allocates nothing: the hash table and every scratch buffer live in one
  * fixed 8 MiB device array that each GPU loading the library holds until

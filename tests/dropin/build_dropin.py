@@ -3,7 +3,7 @@
 own plan.h, plus a driver that runs one serialized plan through
 Contest::build_context / execute / destroy_context.
 
-Needs the reference source tree (CJ_REFERENCE_DIR, default /root/reference);
+Needs the reference source tree (located by oracle/build_oracle.reference_dir);
 the reference's re2 / range-v3 includes are satisfied by oracle/ref_shim.
 The binary links libcj_b200.so through an rpath relative to itself.
 """
@@ -19,8 +19,10 @@ OUT = os.path.join(HERE, "dropin_harness")
 
 
 def build(force: bool = False) -> str | None:
-    ref = os.environ.get("CJ_REFERENCE_DIR", "/root/reference")
-    if not os.path.isfile(os.path.join(ref, "include", "data_model", "plan.h")):
+    sys.path.insert(0, ROOT)
+    from oracle.build_oracle import reference_dir
+    ref = reference_dir()
+    if ref is None or not os.path.isfile(os.path.join(ref, "include", "data_model", "plan.h")):
         return None
     import torch
     fmt_inc = os.path.join(os.path.dirname(torch.__file__), "include")

@@ -33,16 +33,23 @@ def test_reference_unit_case(case):
     assert ok, msg
 
 
-def test_golden_fixture_is_current():
-    """unit_cases.json matches its generator."""
+def test_golden_fixture_is_current(tmp_path):
+    """unit_cases.json is exactly what its generator writes today: run the
+    generator into a scratch directory and compare the two files' data."""
     import json
+    import shutil
     import subprocess
     import sys
-    import tempfile
     here = os.path.join(os.path.dirname(__file__), "golden")
+    gen = tmp_path / "make_unit_cases.py"
+    shutil.copy(os.path.join(here, "make_unit_cases.py"), gen)
+    subprocess.run([sys.executable, str(gen)], check=True, capture_output=True, cwd=tmp_path)
+    with open(tmp_path / "unit_cases.json") as f:
+        fresh = json.load(f)
     with open(os.path.join(here, "unit_cases.json")) as f:
         current = json.load(f)
     assert len(current["cases"]) == 21
+    assert fresh == current
 
 
 @pytest.mark.parametrize("dtype", [DataType.INT32, DataType.INT64, DataType.FP64])
@@ -92,7 +99,13 @@ def test_empty_and_edge_strings():
     assert oa.validate(r)[0]
 
 
-REF_BLOOM = "/root/reference/include/join_execution/bloom_tags.h"
+def _ref_bloom():
+    from oracle.build_oracle import reference_dir
+    ref = reference_dir()
+    return os.path.join(ref, "include", "join_execution", "bloom_tags.h") if ref else ""
+
+
+REF_BLOOM = _ref_bloom()
 
 
 @pytest.mark.skipif(not os.path.exists(REF_BLOOM), reason="reference tree not present")

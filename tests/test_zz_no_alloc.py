@@ -15,7 +15,7 @@ import torch
 from calamarijoins_b200 import ColumnarTable, DataType, Plan, encode_column
 from calamarijoins_b200 import _lib
 from calamarijoins_b200.datagen import fk_column
-from tests.helpers import run_product
+from tests.helpers import run_oracle, run_product
 
 pytestmark = pytest.mark.gpu
 I = DataType.INT32
@@ -30,9 +30,9 @@ def make_tables(seed, nb, npr):
     return bkeys, bvalid, pkeys.astype(np.int32), pvalid
 
 
-def pairs_from_execute(ctx, bkeys, bvalid, pkeys, pvalid):
-    """The regular entry point: a 2-table plan whose outputs are the row
-    numbers of the matching build and probe rows."""
+def pairs_plan(bkeys, bvalid, pkeys, pvalid):
+    """A 2-table plan whose outputs are the row numbers of the matching
+    build and probe rows."""
     plan = Plan()
     nb, npr = len(bkeys), len(pkeys)
     plan.inputs.append(ColumnarTable(nb, [encode_column(I, bkeys, bvalid),
@@ -43,11 +43,24 @@ def pairs_from_execute(ctx, bkeys, bvalid, pkeys, pvalid):
     plan.new_scan_node(1, [(0, I), (1, I)])
     plan.new_join_node(True, 0, 1, 0, 0, [(1, I), (3, I)])
     plan.root = 2
-    r, _ = run_product(plan, ctx)
+    return plan
+
+
+def pairs_of(r):
     from calamarijoins_b200 import Column, decode_column
     b, _ = decode_column(Column(I, r.pages[0]))
     p, _ = decode_column(Column(I, r.pages[1]))
     return np.stack([b, p], axis=1).astype(np.int64)
+
+
+def pairs_from_execute(ctx, bkeys, bvalid, pkeys, pvalid):
+    """The regular, allocating entry point (cj_execute)."""
+    r, _ = run_product(pairs_plan(bkeys, bvalid, pkeys, pvalid), ctx)
+    return pairs_of(r)
+
+
+def pairs_from_oracle(bkeys, bvalid, pkeys, pvalid):
+    return pairs_of(run_oracle(pairs_plan(bkeys, bvalid, pkeys, pvalid)))
 
 
 def bitmap(valid):
@@ -58,13 +71,17 @@ def bitmap(valid):
     return torch.from_numpy(words.view(np.int32).copy()).cuda()
 
 
-def pairs_from_noalloc(bkeys, bvalid, pkeys, pvalid, capacity):
+def pairs_from_noalloc(bkeys, bvalid, pkeys, pvalid, capacity, slack=0):
+    """Calls the no-allocation entry point through the C ABI; returns the
+    pairs written and the full match count. `slack` extra output entries
+    past `capacity` are checked to stay untouched."""
     lib = _lib.lib()
-    bk = torch.from_numpy(bkeys).cuda()
-    pk = torch.from_numpy(pkeys).cuda()
-    bv, pv = bitmap(bvalid), bitmap(pvalid)
-    ob = torch.full((capacity,), -1, dtype=torch.int32, device="cuda")
-    op = torch.full((capacity,), -1, dtype=torch.int32, device="cuda")
+    bk = torch.from_numpy(bkeys).cuda() if len(bkeys) else torch.zeros(1, dtype=torch.int32, device="cuda")
+    pk = torch.from_numpy(pkeys).cuda() if len(pkeys) else torch.zeros(1, dtype=torch.int32, device="cuda")
+    bv = bitmap(bvalid) if len(bvalid) else torch.zeros(1, dtype=torch.int32, device="cuda")
+    pv = bitmap(pvalid) if len(pvalid) else torch.zeros(1, dtype=torch.int32, device="cuda")
+    ob = torch.full((capacity + slack + 1,), -1, dtype=torch.int32, device="cuda")
+    op = torch.full((capacity + slack + 1,), -1, dtype=torch.int32, device="cuda")
     dc = torch.zeros(1, dtype=torch.int64, device="cuda")
     hc = C.c_uint64(0)
     torch.cuda.synchronize()
@@ -72,10 +89,11 @@ def pairs_from_noalloc(bkeys, bvalid, pkeys, pvalid, capacity):
                                   len(pkeys), ob.data_ptr(), op.data_ptr(), capacity, dc.data_ptr(), C.byref(hc),
                                   C.c_void_p(torch.cuda.current_stream().cuda_stream))
     assert rc == 0, lib.cj_last_error()
-    n = hc.value
-    assert n == int(dc.item())
-    assert n <= capacity
-    return np.stack([ob[:n].cpu().numpy(), op[:n].cpu().numpy()], axis=1).astype(np.int64)
+    total = hc.value
+    assert total == int(dc.item())
+    n = min(total, capacity)
+    assert (ob[capacity:] == -1).all() and (op[capacity:] == -1).all(), "written past capacity"
+    return np.stack([ob[:n].cpu().numpy(), op[:n].cpu().numpy()], axis=1).astype(np.int64), total
 
 
 def sorted_pairs(a):
@@ -83,15 +101,45 @@ def sorted_pairs(a):
 
 
 def test_noalloc_matches_execute_twice(gpu_ctx):
-    # two calls in a row, the second larger than the first: the shared
-    # scratch array keeps the first call's contents and must not leak into
-    # the second result
-    for seed, nb, npr in ((1, 5_000, 100_000), (2, 200_000, 400_000)):
+    # calls in a row, smaller, larger, then smaller again: the shared
+    # scratch array keeps the previous call's directory and tuples, which
+    # must not leak into the next result. Each result equals the regular
+    # entry point's pairs and the oracle's.
+    for seed, nb, npr in ((1, 5_000, 100_000), (2, 200_000, 400_000), (3, 3_000, 50_000)):
         bkeys, bvalid, pkeys, pvalid = make_tables(seed, nb, npr)
         want = sorted_pairs(pairs_from_execute(gpu_ctx, bkeys, bvalid, pkeys, pvalid))
-        got = sorted_pairs(pairs_from_noalloc(bkeys, bvalid, pkeys, pvalid, capacity=len(want) + 1000))
+        assert np.array_equal(want, sorted_pairs(pairs_from_oracle(bkeys, bvalid, pkeys, pvalid)))
+        got, total = pairs_from_noalloc(bkeys, bvalid, pkeys, pvalid, capacity=len(want) + 1000)
+        got = sorted_pairs(got)
+        assert total == len(want)
         assert got.shape == want.shape
         assert np.array_equal(got, want)
+
+
+def test_noalloc_capacity_below_count(gpu_ctx):
+    """Fewer output slots than matches: the full count comes back, nothing is
+    written past capacity, and what is written is a subset of the pairs."""
+    bkeys, bvalid, pkeys, pvalid = make_tables(4, 20_000, 200_000)
+    want = sorted_pairs(pairs_from_oracle(bkeys, bvalid, pkeys, pvalid))
+    cap = len(want) // 3
+    got, total = pairs_from_noalloc(bkeys, bvalid, pkeys, pvalid, capacity=cap, slack=4096)
+    assert total == len(want)
+    assert got.shape == (cap, 2)
+    wset = set(map(tuple, want.tolist()))
+    gl = list(map(tuple, got.tolist()))
+    assert len(set(gl)) == cap and all(g in wset for g in gl)
+    # and the next call with room for all of them gets all of them
+    got, total = pairs_from_noalloc(bkeys, bvalid, pkeys, pvalid, capacity=total)
+    assert np.array_equal(sorted_pairs(got), want)
+
+
+@pytest.mark.parametrize("nb,npr", [(0, 1000), (1000, 0), (0, 0)])
+def test_noalloc_empty_side(gpu_ctx, nb, npr):
+    """An empty side joins to nothing: count 0, outputs untouched."""
+    bkeys, bvalid, pkeys, pvalid = make_tables(5, max(nb, 2), max(npr, 2))
+    bkeys, bvalid, pkeys, pvalid = bkeys[:nb], bvalid[:nb], pkeys[:npr], pvalid[:npr]
+    got, total = pairs_from_noalloc(bkeys, bvalid, pkeys, pvalid, capacity=16, slack=16)
+    assert total == 0 and got.shape == (0, 2)
 
 
 def test_noalloc_rejects_oversized_build():
