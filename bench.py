@@ -33,6 +33,8 @@ Other workloads (not the default line; --workload):
       measurements as the default line.
   c2s C2 with the build keys spread 500x (unique multiples of 500): the
       open-addressing table instead of the direct-mapped one.
+  c2h C2 with a non-unique build side (4M rows over 3M distinct keys): the
+      unchained hash table; roofline of the hash path's kernels.
   c3  6-way left-deep join: a 36M-row fact table with 5 foreign keys into
       dimensions of 2.5K-4.2M rows (pre-filtered to 10-40 %), VARCHAR
       outputs (lengths log-normal, mean 20 B, 0.01 % long strings);
@@ -41,11 +43,13 @@ Other workloads (not the default line; --workload):
       1e3-1e7): plans/s through cj_execute_batch, beside a loop of
       cj_execute over the same plans and the reference's execute() on
       the host cores; host pages in, host pages out.
-  c5  the server (cj_server_*, 4 worker streams, 150 GB admission budget)
-      under Poisson arrivals at several rates over a pool of 32 2-16-way
-      plans (probes 1e4-3e6 rows) with INT32 / INT64 keys and 10 % VARCHAR
-      outputs; a client thread takes and frees each result as it
-      completes: p50 / p99 latency and plans/s per rate.
+  c5  Poisson arrivals at several rates over a pool of 32 2-16-way plans
+      (probes 1e4-1e7 rows) with INT32 / INT64 keys and 10 % VARCHAR
+      outputs, served two ways over the same trace: the server
+      (cj_server_*, 4 worker streams, 150 GB admission budget, continuous
+      batching; a client thread takes and frees each result as it
+      completes) and plain cj_execute one plan at a time in arrival order:
+      p50 / p99 latency and plans/s per rate and arm.
 """
 from __future__ import annotations
 
@@ -77,6 +81,13 @@ WORKLOADS = {
             "unit": UNIT,
             "desc": ("C2 with the 4,000,000 unique build keys spread over multiples of 500 below 2^31 (too wide "
                      "for a direct-mapped table: open-addressing table); probe and outputs as C2"),
+            "units": "probe rows"},
+    "c2h": {"metric": "probe rows/s, 4M x 64M INT32 equi-join, non-unique build keys (plain execute)",
+            "unit": UNIT,
+            "desc": ("C2 with a non-unique build side: 4,000,000 build rows over 3,000,000 distinct INT32 keys (a "
+                     "third twice) + INT64 payload; probe 64,000,000 rows, FK Zipf(0.8) over the distinct keys, "
+                     "30% outside, 2% NULL, + FP64 payload; the unchained hash table (radix-partitioned build, "
+                     "Bloom-tag probe); about 58.5M output rows"),
             "units": "probe rows"},
     "c3": {"metric": "fact rows/s, 6-way join of a 36M-row fact table (plain execute)", "unit": UNIT,
            "desc": ("C3: fact 36,000,000 rows x 5 INT32 FKs (Zipf 0.5-1.2) into dimensions of 2,500 / 130,000 / "
@@ -308,6 +319,9 @@ def gen_workload(pinned: bool, scale: float, int32_standin: bool = False, worklo
     if workload == "c2s":
         from calamarijoins_b200.datagen import config_c2s
         return config_c2s(scale=scale, pinned=pinned, int32_standin=int32_standin)
+    if workload == "c2h":
+        from calamarijoins_b200.datagen import config_c2h
+        return config_c2h(scale=scale, pinned=pinned, int32_standin=int32_standin)
     if int32_standin:
         return join2(max(int(4_000_000 * scale), 16), max(int(64_000_000 * scale), 16), seed=202, zipf=0.8,
                      outside=0.30, probe_null=0.02, build_payload=(DataType.INT32,),
@@ -691,9 +705,12 @@ def run_batch(args):
 
 
 def run_serve(args):
-    """c5: the server under Poisson arrivals over a pool of plans: p50 / p99
-    latency (submit to completion) and plans/s per arrival rate. A client
-    thread takes and frees each result as it completes."""
+    """c5: Poisson arrivals over a pool of plans, at several rates, served
+    two ways over the same arrival trace: the server (cj_server_*: worker
+    streams, admission by estimated bytes, continuous batching), and the
+    plain one-plan-at-a-time cj_execute in arrival order on one context
+    (a plan waits for the one before it). Latency = completion - arrival;
+    p50 / p99 and plans/s per rate and arm."""
     import queue
     import numpy as np
     import calamarijoins_b200 as cj
@@ -704,63 +721,104 @@ def run_serve(args):
     pool = []
     for i in range(32):
         ways = int(rng.integers(2, 17))
-        nprobe = int(10 ** rng.uniform(4, 4 + 2.5 * max(args.scale, 0.01) ** 0.25))
+        nprobe = int(10 ** rng.uniform(4, 4 + 3 * max(min(args.scale, 1.0), 0.01) ** 0.25))
         pool.append(chain_plan(ways, nprobe, rng, max_build=max(int(1_000_000 * args.scale), 1000),
                                key_types=[DataType.INT32 if rng.random() < 0.7 else DataType.INT64
                                           for _ in range(ways - 1)],
                                varchar_frac=0.1, pinned=True))
     descs = [cj.PlanDescriptor(p) for p in pool]
+    probe_rows = [p.inputs[0].num_rows for p in pool]
+    gc.collect()
+    gc.freeze()
+
+    def pct(xs, q):
+        xs = sorted(xs)
+        return xs[min(len(xs) - 1, int(q * (len(xs) - 1) + 0.5))]
+
+    def trace(lam):
+        n = int(min(max(lam * 4, 100), 2000))
+        return np.cumsum(rng.exponential(1.0 / lam, n)), rng.integers(0, len(descs), n)
+
+    def served(srv, arrivals, order):
+        q = queue.Queue()
+
+        def consume():
+            while True:
+                t = q.get()
+                if t is None:
+                    return
+                r, _ = srv.wait(t)
+                r.free()
+        th = threading.Thread(target=consume)
+        th.start()
+        t0 = time.perf_counter()
+        for at, k in zip(arrivals, order):
+            d = at - (time.perf_counter() - t0)
+            if d > 0:
+                time.sleep(d)
+            q.put(srv.submit(descs[k]))
+        q.put(None)
+        th.join()
+        st = srv.stats(reset=True)
+        return {"plans_per_s": st["plans_per_s"], "p50_ms": st["p50_us"] / 1e3, "p99_ms": st["p99_us"] / 1e3,
+                "mean_ms": st["mean_us"] / 1e3, "max_ms": st["max_us"] / 1e3, "failed": st["failed"],
+                "rejected": st["rejected"], "peak_admitted_gb": st["peak_admitted_bytes"] / 1e9,
+                "batches": st["batches"], "mean_batch": st["mean_batch"], "skipped_ahead": st["skipped_ahead"]}
+
+    def plain(ctx, arrivals, order):
+        lat = []
+        t0 = time.perf_counter()
+        last = t0
+        for at, k in zip(arrivals, order):
+            d = at - (time.perf_counter() - t0)
+            if d > 0:
+                time.sleep(d)
+            r, _ = cj.execute_raw(pool[k], ctx, 0, descs[k])
+            r.free()
+            last = time.perf_counter()
+            lat.append((last - t0) - at)
+        wall = last - (t0 + arrivals[0])
+        return {"plans_per_s": len(lat) / wall, "p50_ms": pct(lat, 0.5) * 1e3, "p99_ms": pct(lat, 0.99) * 1e3,
+                "mean_ms": statistics.mean(lat) * 1e3, "max_ms": max(lat) * 1e3}
+
     srv = cj.Server(device=0, slots=4, memory_budget=150 << 30)
+    ctx = cj.Context(0)
     try:
         log("warm-up")
         for d in descs:
             r, _ = srv.wait(srv.submit(d))
             r.free()
         srv.stats(reset=True)
+        for p, d in zip(pool, descs):
+            r, _ = cj.execute_raw(p, ctx, 0, d)
+            r.free()
         per_rate = []
         for lam in C5_RATES:
-            n = int(min(max(lam * 4, 100), 2000))
-            gaps = rng.exponential(1.0 / lam, n)
-            order = rng.integers(0, len(descs), n)
-            log(f"rate {lam}/s: {n} plans")
-            q = queue.Queue()
-
-            def consume():
-                while True:
-                    t = q.get()
-                    if t is None:
-                        return
-                    r, _ = srv.wait(t)
-                    r.free()
-            th = threading.Thread(target=consume)
-            th.start()
-            t0 = time.perf_counter()
-            at = 0.0
-            for g, k in zip(gaps, order):
-                at += g
-                d = at - (time.perf_counter() - t0)
-                if d > 0:
-                    time.sleep(d)
-                q.put(srv.submit(descs[k]))
-            q.put(None)
-            th.join()
-            st = srv.stats(reset=True)
-            per_rate.append({"rate": lam, "plans": n, "p50_ms": st["p50_us"] / 1e3, "p99_ms": st["p99_us"] / 1e3,
-                             "mean_ms": st["mean_us"] / 1e3, "max_ms": st["max_us"] / 1e3,
-                             "plans_per_s": st["plans_per_s"], "failed": st["failed"], "rejected": st["rejected"],
-                             "peak_admitted_gb": st["peak_admitted_bytes"] / 1e9})
+            arrivals, order = trace(lam)
+            log(f"rate {lam}/s: {len(order)} plans, served")
+            sv = served(srv, arrivals, order)
+            log(f"rate {lam}/s: plain")
+            pl = plain(ctx, arrivals, order)
+            per_rate.append({"rate": lam, "plans": len(order), "served": sv, "plain": pl,
+                             "served_over_plain": sv["plans_per_s"] / pl["plans_per_s"]})
     finally:
         srv.close()
-    best = max(per_rate, key=lambda x: x["plans_per_s"])
-    line = {"metric": "served plans/s (Poisson arrivals), p50 / p99 latency", "value": best["plans_per_s"],
+        ctx.close()
+    best = max(per_rate, key=lambda x: x["served"]["plans_per_s"])
+    plain_best = max(x["plain"]["plans_per_s"] for x in per_rate)
+    line = {"metric": "served plans/s (Poisson arrivals), p50 / p99 latency", "value": best["served"]["plans_per_s"],
             "unit": "plans/s", "n_gpus": 1, "steps": len(C5_RATES), "warmup": 1, "ms_per_step": None,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32/int64",
             "data": "synthetic",
             "config": {"workload": ("C5: pool of 32 seeded 2-16-way chain plans, 70 % INT32 / 30 % INT64 keys, "
-                                    "10 % VARCHAR outputs, probes log-uniform 1e4-3e6 rows, dimensions 10-1e6 rows, "
-                                    "4 worker streams, 150 GB admission budget; Poisson arrivals, each plan drawn "
-                                    "from the pool"), "scale": args.scale},
+                                    "10 % VARCHAR outputs, probes log-uniform 1e4-1e7 rows, dimensions 10-1e6 rows, "
+                                    "host pages in and out; Poisson arrivals, each plan drawn from the pool; served: "
+                                    "4 worker streams, 150 GB admission budget, continuous batching; plain: "
+                                    "cj_execute one plan at a time in arrival order"), "scale": args.scale,
+                       "probe_rows": {"min": min(probe_rows), "max": max(probe_rows)}},
             "rates": per_rate,
+            "plain_best_plans_per_s": plain_best,
+            "served_over_plain_at_saturation": best["served"]["plans_per_s"] / plain_best,
             "cpu_baseline": {"unavailable": "the reference joins INT32 keys only (30 % of the pool has INT64 keys) "
                                             "and has no serving front end"}}
     print(json.dumps(line))
@@ -778,7 +836,7 @@ def main(argv=None):
     ap.add_argument("--no-parity", action="store_true", help="skip the oracle fingerprint check")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-worker", type=int, default=0, help=argparse.SUPPRESS)
-    ap.add_argument("--workload", choices=["c2", "c1", "c2s", "c3", "c4", "c5"], default="c2",
+    ap.add_argument("--workload", choices=["c2", "c1", "c2s", "c2h", "c3", "c4", "c5"], default="c2",
                     help="c2 (default): the headline line; the others: see the module docstring")
     args = ap.parse_args(argv)
     global WL

@@ -94,14 +94,15 @@ class BatchStatsC(C.Structure):
 
 class ServerConfigC(C.Structure):
     _fields_ = [("device", C.c_int32), ("slots", C.c_uint32), ("memory_budget", C.c_uint64),
-                ("exec_flags", C.c_uint32), ("reserved", C.c_uint32)]
+                ("exec_flags", C.c_uint32), ("max_batch", C.c_uint32), ("age_limit_us", C.c_uint64)]
 
 
 class ServerStatsC(C.Structure):
     _fields_ = ([(n, C.c_uint64) for n in (
         "submitted", "completed", "failed", "rejected", "cancelled", "queued", "running", "admitted_bytes",
         "peak_admitted_bytes", "memory_budget")]
-        + [(n, C.c_double) for n in ("p50_us", "p99_us", "mean_us", "max_us", "wall_s", "plans_per_s")])
+        + [(n, C.c_double) for n in ("p50_us", "p99_us", "mean_us", "max_us", "wall_s", "plans_per_s")]
+        + [("batches", C.c_uint64), ("skipped_ahead", C.c_uint64), ("mean_batch", C.c_double)])
 
 
 # every function of include/cj_b200.h: name -> (restype, argtypes)

@@ -257,7 +257,7 @@ void BatchExecutor::run_level(int lvl) {
         w.log2_slots = bp.log2_slots;
         w.log2_parts = bp.log2_parts;
         const int kb = w.bk.type == CJ_INT32 ? 4 : 8;
-        w.dir = ctx.alloc(build_dir_bytes(bp.log2_slots));
+        w.dir = ctx.alloc(build_dir_bytes(bp.log2_slots, kb));
         w.tuples = ctx.alloc(w.B->rows * build_tuple_bytes(kb));
         w.part_buf = ctx.alloc(w.B->rows * build_tuple_bytes(kb));
         BuildGeometry g = build_geometry(L, bp);

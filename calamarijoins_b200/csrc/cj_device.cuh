@@ -12,30 +12,33 @@ namespace cj {
 
 #define CJ_DEV __device__ __forceinline__
 
-/* 64-bit key hash: the MurmurHash3 64-bit finaliser (Austin Appleby,
- * public domain). The reference hashes with the x86/ARM CRC32C instruction
- * times a multiplier (include/join_execution/hashtable.h:146-154); the GPU
- * has no CRC instruction and the hash does not change any result, only the
- * slot a key lands in, so a multiply-xorshift finaliser is used instead.
- * Slot = top bits (as slot_for, hashtable.h:167-169); Bloom tag index = the
- * low 11 bits, which stay independent of the slot bits for every directory
- * size (the reference takes bits 32..42, which overlap the slot bits once
- * the directory exceeds 2^21 slots). */
+/* Key hash for the unchained table, a function of the key's 64-bit value
+ * (INT32 and INT64 keys of equal value hash alike). The 64-bit value is
+ * folded to 32 bits (a bijection on INT32 values), then two 32-bit
+ * multiplicative hashes (Knuth's method: the product's top bits are the
+ * well-mixed ones) give the high word, whose top bits are the radix
+ * partition and the directory slot, and the low word, whose top 11 bits
+ * index the Bloom tag table. The reference hashes with the x86/ARM CRC32C
+ * instruction times a multiplier (include/join_execution/hashtable.h:
+ * 146-154); the GPU has no CRC instruction, and the hash changes no result,
+ * only where a key lands. Three 32-bit multiplies; the slot bits and the
+ * Bloom bits come from different products, so a slot's keys still differ
+ * in their tags for every directory size. */
 __host__ __device__ __forceinline__ uint64_t hash_key(int64_t key) {
-    uint64_t x = (uint64_t)key;
-    x ^= x >> 33;
-    x *= 0xff51afd7ed558ccdull;
-    x ^= x >> 33;
-    x *= 0xc4ceb9fe1a85ec53ull;
-    x ^= x >> 33;
-    return x;
+    const uint64_t x = (uint64_t)key;
+    const uint32_t m = (uint32_t)x ^ ((uint32_t)(x >> 32) * 0x2545F491u);
+    const uint32_t hi = m * 0x9E3779B1u;
+    const uint32_t lo = (m ^ (m >> 15)) * 0x85EBCA77u;
+    return ((uint64_t)hi << 32) | lo;
 }
 
+/* Slot = top log2_slots bits (as slot_for, hashtable.h:167-169);
+ * log2_slots <= 32. */
 CJ_DEV uint32_t slot_of(uint64_t h, int log2_slots) {
     return (uint32_t)(h >> (64 - log2_slots));
 }
 
-CJ_DEV uint32_t bloom_index(uint64_t h) { return (uint32_t)(h & 0x7FFu); }
+CJ_DEV uint32_t bloom_index(uint64_t h) { return (uint32_t)h >> 21; }
 
 /* First slot of an INT32 key in an open-addressing table of nslots (< 2^32)
  * slots: Knuth's multiplicative hashing (the key times 2^32 / golden ratio,

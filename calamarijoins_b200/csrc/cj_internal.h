@@ -108,8 +108,19 @@ template <> struct alignas(16) Tuple<int64_t> {
     uint32_t pad;
 };
 
+/* Directory entry of a table with INT32 keys: the entry word (start of the
+ * slot's tuples << 32 | count << 16 | Bloom tags) and the slot's first
+ * tuple inline, 16 bytes in one sector: a probe row whose slot holds one
+ * tuple needs one random access. Tables with INT64 keys keep 8-byte entries
+ * (the word alone). */
+struct alignas(16) DirEntry32 {
+    uint64_t word;
+    int32_t key0;
+    uint32_t rid0;
+};
+
 template <typename K> struct HashTableView {
-    const uint64_t *dir;
+    const uint64_t *dir; /* DirEntry32[] for K = int32_t, entry words for int64_t */
     const Tuple<K> *tuples;
     int log2_slots;
 };
@@ -191,13 +202,17 @@ cudaError_t launch_decode_grouped(const Launch &L, const DecodeTask *tasks_dev, 
 
 /* Build */
 struct BuildPlan {
-    int log2_slots;      /* directory = 2^log2_slots u64 entries + 1      */
-    int log2_parts;      /* radix partitions                              */
+    int log2_slots;      /* directory = 2^log2_slots entries + 1          */
+    int log2_parts;      /* radix partition bits in all: one pass up to 12
+                            bits, two passes above (launch_build)         */
     uint32_t num_rows;   /* rows of the build relation                    */
 };
-/* Directory entry: start (63..32) | count (31..16, saturated) | tags (15..0);
- * one sentinel entry after the last slot. */
-inline size_t build_dir_bytes(int log2_slots) { return ((1ull << log2_slots) + 1) * sizeof(uint64_t); }
+/* Directory entry word: start (63..32) | count (31..16, saturated) | tags
+ * (15..0); INT32 keys add the first tuple (DirEntry32); one sentinel entry
+ * after the last slot. */
+inline size_t build_dir_bytes(int log2_slots, int key_bytes) {
+    return ((1ull << log2_slots) + 1) * (key_bytes == 4 ? sizeof(DirEntry32) : sizeof(uint64_t));
+}
 size_t build_temp_bytes(const Launch &L, const BuildPlan &bp, int key_bytes);
 size_t build_tuple_bytes(int key_bytes);
 cudaError_t launch_build(const Launch &L, const BuildPlan &bp, const ColView &key,

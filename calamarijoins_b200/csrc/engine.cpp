@@ -371,15 +371,17 @@ Relation Executor::exec_join(uint64_t node_idx, int depth, bool is_root, cj_resu
             BuildPlan bp;
             bp.num_rows = (uint32_t)B.rows;
             bp.log2_slots = std::max(11, ceil_log2(B.rows)); /* hashtable.h:255-264 */
+            /* 2^11 directory slots per partition by default (the slot
+             * counters of one partition fit shared memory); the partition
+             * bits are spread over one radix pass, or two above 12 bits
+             * (build sides of more than 2^23 rows) */
             int log2_spp = 11;
             if (ctx.opt.slots_per_partition > 0) log2_spp = ceil_log2((uint64_t)ctx.opt.slots_per_partition);
-            log2_spp = std::min(log2_spp, bp.log2_slots);
-            bp.log2_parts = std::min(bp.log2_slots - log2_spp, 12);
-            if (bp.log2_slots - bp.log2_parts > 14)
-                fail(CJ_ERR_LIMIT, "build side too large for one radix pass (max 2^26 rows)");
+            log2_spp = std::min(std::min(log2_spp, 14), bp.log2_slots);
+            bp.log2_parts = bp.log2_slots - log2_spp;
             log2_slots = bp.log2_slots;
             const int kb = bk.type == CJ_INT32 ? 4 : 8;
-            dir = ctx.alloc(build_dir_bytes(bp.log2_slots));
+            dir = ctx.alloc(build_dir_bytes(bp.log2_slots, kb));
             tuples = ctx.alloc(B.rows * build_tuple_bytes(kb));
             DevPtr tmp = ctx.alloc(build_temp_bytes(L, bp, kb));
             KScope k(*this, "build");

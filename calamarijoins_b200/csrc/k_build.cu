@@ -36,11 +36,31 @@
 
 #include "cj_device.cuh"
 
+#define CJ_DEV_HOST_INLINE __host__ __device__ __forceinline__
+
 namespace cj {
 namespace {
 
 constexpr int kBuildThreads = 256;
-constexpr int kHistItems = 16;
+/* Radix histogram and scatter passes: 512 threads per CTA, at most four
+ * CTAs per SM, each over a contiguous chunk of at least kPartMinRows build
+ * rows (64 warps per SM stream the keys; fewer chunks keep the partition x
+ * chunk offset matrix and its scan small). */
+constexpr int kPartThreads = 512;
+constexpr uint32_t kPartMinRows = 2048;
+constexpr int kPartCtasPerSm = 4;
+/* Radix bits one pass can take: 2^12 shared-memory counters (16 KB) per
+ * CTA. More partition bits than that are split over two passes: the first
+ * over the build keys (top b1 bits), the second refining every first-pass
+ * partition by the next b2 bits (k_part_refine), b1 >= 8 so that the second
+ * pass has at least 256 partitions to spread over the SMs. */
+constexpr int kMaxPassBits = 12;
+constexpr int kMinFirstPassBits = 8;
+CJ_DEV_HOST_INLINE int first_pass_bits(int log2_parts) {
+    if (log2_parts <= kMaxPassBits) return log2_parts;
+    const int b2 = log2_parts - kMinFirstPassBits < kMaxPassBits ? log2_parts - kMinFirstPassBits : kMaxPassBits;
+    return log2_parts - b2;
+}
 
 struct PartGeom {
     uint32_t n;        /* build relation rows                */
@@ -75,52 +95,46 @@ CJ_DEV void hist_chunk(const ColView &key, const PartGeom &g, uint32_t chunk, ui
 }
 
 /* Scatter of one chunk into the partitioned buffer. `offsets` is the
- * exclusive scan of the matrix, `off_base` subtracted from every entry. */
+ * exclusive scan of the matrix, `off_base` subtracted from every entry.
+ * The rows of one partition inside a warp are ranked with
+ * __match_any_sync and the group's leader reserves their places with one
+ * shared-memory atomicAdd on the partition's cursor: each tuple is written
+ * as soon as its key is read, with no block barrier in the loop and no
+ * rows held in registers. The order of a chunk's tuples inside a partition
+ * is therefore not row order; nothing depends on it (the per-partition
+ * build sorts them by slot, and the order of equal-slot tuples, like the
+ * order of a join's output rows, is unspecified). */
 template <typename K>
 CJ_DEV void scatter_chunk(const ColView &key, const PartGeom &g, uint32_t chunk, const uint64_t *__restrict__ offsets,
                           uint64_t off_base, Tuple<K> *__restrict__ out, uint32_t *smem) {
     const uint32_t P = 1u << g.log2_parts;
-    uint32_t *s_cursor = smem;   /* next output slot per partition  */
-    uint32_t *s_tile = smem + P; /* rows per partition in this tile */
+    uint32_t *s_cursor = smem; /* next output position per partition */
     for (uint32_t b = threadIdx.x; b < P; b += blockDim.x)
         s_cursor[b] = (uint32_t)(offsets[(uint64_t)b * g.grid + chunk] - off_base);
+    __syncthreads();
     const uint64_t r0 = (uint64_t)chunk * g.chunk;
     const uint64_t r1 = min((uint64_t)g.n, r0 + g.chunk);
-    const uint32_t tile = blockDim.x * kHistItems;
-    for (uint64_t t0 = r0; t0 < r1; t0 += tile) {
-        for (uint32_t b = threadIdx.x; b < P; b += blockDim.x) s_tile[b] = 0;
-        __syncthreads();
-        uint32_t part[kHistItems], rank[kHistItems];
-        K keys[kHistItems];
-#pragma unroll
-        for (int it = 0; it < kHistItems; ++it) {
-            uint64_t i = t0 + (uint64_t)it * blockDim.x + threadIdx.x;
-            int64_t k = 0;
-            bool v = i < r1 && load_key(key, (uint32_t)i, &k);
-            uint32_t p = v ? part_of(hash_key(k), g.log2_parts) : 0xffffffffu;
-            uint32_t peers = __match_any_sync(0xffffffffu, p);
-            uint32_t leader = __ffs(peers) - 1;
-            uint32_t base = 0;
-            if (v && lane_id() == leader) base = atomicAdd(&s_tile[p], (uint32_t)__popc(peers));
-            base = __shfl_sync(0xffffffffu, base, leader);
-            part[it] = p;
-            rank[it] = base + __popc(peers & lanemask_lt());
-            keys[it] = (K)k;
-        }
-        __syncthreads();
-#pragma unroll
-        for (int it = 0; it < kHistItems; ++it) {
-            if (part[it] == 0xffffffffu) continue;
-            uint64_t i = t0 + (uint64_t)it * blockDim.x + threadIdx.x;
+    /* whole warps iterate together (match_any needs every lane) */
+    const uint64_t span = (r1 > r0 ? r1 - r0 : 0);
+    const uint64_t iters = (span + blockDim.x - 1) / blockDim.x;
+    for (uint64_t k = 0; k < iters; ++k) {
+        const uint64_t i = r0 + k * blockDim.x + threadIdx.x;
+        int64_t kv = 0;
+        const bool v = i < r1 && load_key(key, (uint32_t)i, &kv);
+        const uint32_t p = v ? part_of(hash_key(kv), g.log2_parts) : 0xffffffffu;
+        const uint32_t peers = __match_any_sync(0xffffffffu, p);
+        const uint32_t leader = __ffs(peers) - 1;
+        uint32_t base = 0;
+        if (v && lane_id() == leader) base = atomicAdd(&s_cursor[p], (uint32_t)__popc(peers));
+        base = __shfl_sync(0xffffffffu, base, leader);
+        if (v) {
             Tuple<K> tp;
-            tp.key = keys[it];
+            tp.key = (K)kv;
             tp.rid = (uint32_t)i;
-            out[s_cursor[part[it]] + rank[it]] = tp;
+            out[base + __popc(peers & lanemask_lt())] = tp;
         }
-        __syncthreads();
-        for (uint32_t b = threadIdx.x; b < P; b += blockDim.x) s_cursor[b] += s_tile[b];
-        __syncthreads();
     }
+    __syncthreads();
 }
 
 /* Counting sort of one partition into slot order + its directory entries
@@ -153,36 +167,115 @@ CJ_DEV void build_partition(const Tuple<K> *__restrict__ in, const uint64_t *__r
         if (s0 + k < S) sum += s_cnt[s0 + k];
     uint32_t tot;
     uint32_t pre = block_exclusive_scan<uint32_t>(sum, wbuf, &tot);
+    constexpr bool kInline = sizeof(K) == 4; /* DirEntry32: first tuple in the entry */
+    DirEntry32 *dir16 = reinterpret_cast<DirEntry32 *>(dir);
     for (uint32_t k = 0; k < per; ++k) {
         uint32_t s = s0 + k;
         if (s >= S) break;
         uint32_t c = s_cnt[s];
         const uint64_t start = ps + pre;
-        dir[(uint64_t)p * S + s] =
-            (start << 32) | ((uint64_t)min(c, 0xFFFFu) << 16) | (uint64_t)(s_tag[s] & 0xFFFFu);
+        const uint64_t word = (start << 32) | ((uint64_t)min(c, 0xFFFFu) << 16) | (uint64_t)(s_tag[s] & 0xFFFFu);
+        if (kInline) dir16[(uint64_t)p * S + s].word = word;
+        else dir[(uint64_t)p * S + s] = word;
         s_cnt[s] = pre; /* becomes the scatter cursor */
+        s_tag[s] = pre; /* the slot's first position */
         pre += c;
     }
-    if (threadIdx.x == 0 && p == (1u << log2_parts) - 1) dir[(uint64_t)(p + 1) * S] = pe << 32; /* sentinel */
+    if (threadIdx.x == 0 && p == (1u << log2_parts) - 1) { /* sentinel */
+        if (kInline) dir16[(uint64_t)(p + 1) * S].word = pe << 32;
+        else dir[(uint64_t)(p + 1) * S] = pe << 32;
+    }
     __syncthreads();
     for (uint64_t t = ps + threadIdx.x; t < pe; t += blockDim.x) {
         Tuple<K> tp = in[t];
         uint32_t ls = slot_of(hash_key((int64_t)tp.key), log2_slots) & (S - 1);
         uint32_t pos = atomicAdd(&s_cnt[ls], 1u);
         out[ps + pos] = tp;
+        if (kInline && pos == s_tag[ls]) { /* the slot's first tuple, also in its entry */
+            dir16[(uint64_t)p * S + ls].key0 = (int32_t)tp.key;
+            dir16[(uint64_t)p * S + ls].rid0 = tp.rid;
+        }
     }
     __syncthreads();
 }
 
+/* Second radix pass: one CTA per first-pass partition (a contiguous range
+ * of `in`, bounded by offsets[p1 * grid_hist]) counts its tuples over the
+ * next b2 hash bits in shared memory, scans the counts into the global
+ * partition starts part_start[p1 * 2^b2 + q], and scatters the tuples into
+ * `out` with warp-aggregated shared-memory cursors. Afterwards `out` is
+ * ordered by the top b1 + b2 hash bits, as one pass over 2^(b1 + b2)
+ * partitions would have left it, and part_start (2^(b1+b2) + 1 entries)
+ * bounds each partition for k_part_build. */
+template <typename K>
+__global__ void __launch_bounds__(kPartThreads)
+    k_part_refine(const Tuple<K> *__restrict__ in, const uint64_t *__restrict__ offsets, uint32_t grid_hist, int b1,
+                  int b2, Tuple<K> *__restrict__ out, uint64_t *__restrict__ part_start) {
+    extern __shared__ uint32_t s_cnt[];
+    __shared__ uint32_t wbuf[kPartThreads / 32 + 1];
+    const uint32_t Q = 1u << b2;
+    const uint32_t P1 = 1u << b1;
+    const int top = b1 + b2;
+    for (uint32_t p1 = blockIdx.x; p1 < P1; p1 += gridDim.x) {
+        const uint64_t ps = offsets[(uint64_t)p1 * grid_hist], pe = offsets[(uint64_t)(p1 + 1) * grid_hist];
+        for (uint32_t q = threadIdx.x; q < Q; q += blockDim.x) s_cnt[q] = 0;
+        __syncthreads();
+        const uint64_t iters = (pe - ps + blockDim.x - 1) / blockDim.x;
+        for (uint64_t k = 0; k < iters; ++k) {
+            const uint64_t t = ps + k * blockDim.x + threadIdx.x;
+            const bool v = t < pe;
+            const uint32_t q = v ? (uint32_t)(hash_key((int64_t)in[t].key) >> (64 - top)) & (Q - 1) : 0xffffffffu;
+            const uint32_t peers = __match_any_sync(0xffffffffu, q);
+            if (v && lane_id() == (uint32_t)(__ffs(peers) - 1)) atomicAdd(&s_cnt[q], (uint32_t)__popc(peers));
+        }
+        __syncthreads();
+        /* exclusive scan of the Q counts, each thread a run of them */
+        const uint32_t per = (Q + blockDim.x - 1) / blockDim.x;
+        const uint32_t q0 = threadIdx.x * per;
+        uint32_t sum = 0;
+        for (uint32_t j = 0; j < per; ++j)
+            if (q0 + j < Q) sum += s_cnt[q0 + j];
+        uint32_t tot;
+        uint32_t pre = block_exclusive_scan<uint32_t>(sum, wbuf, &tot);
+        for (uint32_t j = 0; j < per; ++j) {
+            const uint32_t q = q0 + j;
+            if (q >= Q) break;
+            const uint32_t c = s_cnt[q];
+            part_start[(uint64_t)p1 * Q + q] = ps + pre;
+            s_cnt[q] = (uint32_t)(ps + pre); /* tuple counts stay below 2^32 */
+            pre += c;
+        }
+        if (p1 == P1 - 1 && threadIdx.x == 0) part_start[(uint64_t)P1 * Q] = pe;
+        __syncthreads();
+        for (uint64_t k = 0; k < iters; ++k) {
+            const uint64_t t = ps + k * blockDim.x + threadIdx.x;
+            const bool v = t < pe;
+            Tuple<K> tp;
+            uint32_t q = 0xffffffffu;
+            if (v) {
+                tp = in[t];
+                q = (uint32_t)(hash_key((int64_t)tp.key) >> (64 - top)) & (Q - 1);
+            }
+            const uint32_t peers = __match_any_sync(0xffffffffu, q);
+            const uint32_t leader = __ffs(peers) - 1;
+            uint32_t base = 0;
+            if (v && lane_id() == leader) base = atomicAdd(&s_cnt[q], (uint32_t)__popc(peers));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            if (v) out[base + __popc(peers & lanemask_lt())] = tp;
+        }
+        __syncthreads();
+    }
+}
+
 /* ---- single-join kernels ---- */
-__global__ void __launch_bounds__(kBuildThreads)
+__global__ void __launch_bounds__(kPartThreads)
     k_part_hist(ColView key, PartGeom g, uint32_t *__restrict__ matrix) {
     extern __shared__ uint32_t s_hist[];
     hist_chunk(key, g, blockIdx.x, matrix, s_hist);
 }
 
 template <typename K>
-__global__ void __launch_bounds__(kBuildThreads)
+__global__ void __launch_bounds__(kPartThreads)
     k_part_scatter(ColView key, PartGeom g, const uint64_t *__restrict__ offsets, Tuple<K> *__restrict__ out) {
     extern __shared__ uint32_t smem[];
     scatter_chunk<K>(key, g, blockIdx.x, offsets, 0, out, smem);
@@ -226,7 +319,7 @@ CJ_DEV PartGeom task_geom(const BuildTask &T) {
     return g;
 }
 
-__global__ void __launch_bounds__(kBuildThreads)
+__global__ void __launch_bounds__(kPartThreads)
     k_part_hist_grouped(const BuildTask *__restrict__ tasks, uint32_t ntasks, uint32_t *__restrict__ matrix) {
     extern __shared__ uint32_t s_hist[];
     __shared__ uint32_t s_task;
@@ -236,7 +329,7 @@ __global__ void __launch_bounds__(kBuildThreads)
     hist_chunk(T.key, task_geom(T), blockIdx.x - T.chunk_base, matrix + T.cell_base, s_hist);
 }
 
-__global__ void __launch_bounds__(kBuildThreads)
+__global__ void __launch_bounds__(kPartThreads)
     k_part_scatter_grouped(const BuildTask *__restrict__ tasks, uint32_t ntasks,
                            const uint64_t *__restrict__ offsets) {
     extern __shared__ uint32_t smem[];
@@ -282,11 +375,11 @@ __global__ void __launch_bounds__(kBuildThreads)
 PartGeom geometry(const Launch &L, const BuildPlan &bp) {
     PartGeom g;
     g.n = bp.num_rows;
-    g.log2_parts = bp.log2_parts;
+    g.log2_parts = first_pass_bits(bp.log2_parts);
     g.log2_slots = bp.log2_slots;
-    uint64_t tiles = ((uint64_t)bp.num_rows + kBuildThreads * kHistItems - 1) / (kBuildThreads * kHistItems);
-    uint64_t grid = (uint64_t)L.num_sms * 2;
-    if (tiles < grid) grid = tiles;
+    uint64_t chunks = ((uint64_t)bp.num_rows + kPartMinRows - 1) / kPartMinRows;
+    uint64_t grid = (uint64_t)L.num_sms * kPartCtasPerSm;
+    if (chunks < grid) grid = chunks;
     if (grid == 0) grid = 1;
     g.grid = (uint32_t)grid;
     g.chunk = (uint32_t)(((uint64_t)bp.num_rows + grid - 1) / grid);
@@ -299,8 +392,9 @@ template <typename K>
 cudaError_t build_impl(const Launch &L, const BuildPlan &bp, const ColView &key,
                        const uint16_t *bloom, uint64_t *dir, Tuple<K> *tuples, void *temp) {
     PartGeom g = geometry(L, bp);
-    const uint64_t P = 1ull << bp.log2_parts;
-    const uint64_t cells = P * g.grid;
+    const int b1 = g.log2_parts, b2 = bp.log2_parts - b1; /* b2 > 0: a second pass */
+    const uint64_t P1 = 1ull << b1;
+    const uint64_t cells = P1 * g.grid;
     char *t = reinterpret_cast<char *>(temp);
     uint32_t *matrix = reinterpret_cast<uint32_t *>(t);
     t += align256(cells * sizeof(uint32_t));
@@ -308,25 +402,48 @@ cudaError_t build_impl(const Launch &L, const BuildPlan &bp, const ColView &key,
     t += align256((cells + 1) * sizeof(uint64_t));
     Tuple<K> *part_buf = reinterpret_cast<Tuple<K> *>(t);
     t += align256((size_t)bp.num_rows * sizeof(Tuple<K>));
+    Tuple<K> *part_buf2 = nullptr;
+    uint64_t *part_start = nullptr;
+    if (b2 > 0) {
+        part_buf2 = reinterpret_cast<Tuple<K> *>(t);
+        t += align256((size_t)bp.num_rows * sizeof(Tuple<K>));
+        part_start = reinterpret_cast<uint64_t *>(t);
+        t += align256(((1ull << bp.log2_parts) + 1) * sizeof(uint64_t));
+    }
     void *scan_tmp = t;
 
-    const size_t hist_smem = P * sizeof(uint32_t);
-    k_part_hist<<<g.grid, kBuildThreads, hist_smem, L.stream>>>(key, g, matrix);
+    const size_t hist_smem = P1 * sizeof(uint32_t);
+    k_part_hist<<<g.grid, kPartThreads, hist_smem, L.stream>>>(key, g, matrix);
     count_launches(1);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     e = scan_u32_to_u64(L, matrix, offsets, cells, scan_tmp);
     if (e != cudaSuccess) return e;
-    const size_t scat_smem = 2 * P * sizeof(uint32_t);
-    k_part_scatter<K><<<g.grid, kBuildThreads, scat_smem, L.stream>>>(key, g, offsets, part_buf);
+    const size_t scat_smem = P1 * sizeof(uint32_t);
+    k_part_scatter<K><<<g.grid, kPartThreads, scat_smem, L.stream>>>(key, g, offsets, part_buf);
     count_launches(1);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
+    const Tuple<K> *parts = part_buf;
+    const uint64_t *bounds = offsets;
+    uint32_t bounds_stride = g.grid;
+    if (b2 > 0) {
+        const unsigned grid_r = (unsigned)std::min<uint64_t>(P1, (uint64_t)L.num_sms * 4);
+        k_part_refine<K><<<grid_r, kPartThreads, (1u << b2) * sizeof(uint32_t), L.stream>>>(
+            part_buf, offsets, g.grid, b1, b2, part_buf2, part_start);
+        count_launches(1);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+        parts = part_buf2;
+        bounds = part_start;
+        bounds_stride = 1;
+    }
+    const uint64_t P = 1ull << bp.log2_parts;
     const uint64_t S = 1ull << (bp.log2_slots - bp.log2_parts);
     const size_t build_smem = 2 * S * sizeof(uint32_t);
     unsigned grid_b = (unsigned)(P < (uint64_t)L.num_sms * 16 ? P : (uint64_t)L.num_sms * 16);
     k_part_build<K><<<grid_b, kBuildThreads, build_smem, L.stream>>>(
-        part_buf, offsets, g.grid, bp.log2_parts, bp.log2_slots, bloom, dir, tuples);
+        parts, bounds, bounds_stride, bp.log2_parts, bp.log2_slots, bloom, dir, tuples);
     count_launches(1);
     return cudaGetLastError();
 }
@@ -473,6 +590,8 @@ void set_smem_attrs() {
     cudaFuncSetAttribute(k_part_hist_grouped, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
     cudaFuncSetAttribute(k_part_scatter_grouped, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
     cudaFuncSetAttribute(k_part_build_grouped, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
+    cudaFuncSetAttribute(k_part_refine<int32_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
+    cudaFuncSetAttribute(k_part_refine<int64_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
     g_attrs_set[dev].store(true, std::memory_order_release);
 }
 
@@ -480,10 +599,13 @@ void set_smem_attrs() {
 
 size_t build_temp_bytes(const Launch &L, const BuildPlan &bp, int key_bytes) {
     PartGeom g = geometry(L, bp);
-    uint64_t cells = (1ull << bp.log2_parts) * g.grid;
+    uint64_t cells = (1ull << g.log2_parts) * g.grid;
     size_t tuple = key_bytes == 4 ? sizeof(Tuple<int32_t>) : sizeof(Tuple<int64_t>);
-    return align256(cells * 4) + align256((cells + 1) * 8) + align256((size_t)bp.num_rows * tuple) +
-           scan_temp_bytes(cells) + 256;
+    size_t b = align256(cells * 4) + align256((cells + 1) * 8) + align256((size_t)bp.num_rows * tuple) +
+               scan_temp_bytes(cells) + 256;
+    if (bp.log2_parts > g.log2_parts) /* second pass: its output and the partition starts */
+        b += align256((size_t)bp.num_rows * tuple) + align256(((1ull << bp.log2_parts) + 1) * 8);
+    return b;
 }
 
 BuildGeometry build_geometry(const Launch &L, const BuildPlan &bp) {
@@ -505,14 +627,14 @@ cudaError_t launch_build_grouped(const Launch &L, const BuildTask *tasks_dev, ui
     t += align256(total_cells * sizeof(uint32_t));
     uint64_t *offsets = reinterpret_cast<uint64_t *>(t);
     t += align256((total_cells + 1) * sizeof(uint64_t));
-    k_part_hist_grouped<<<total_chunks, kBuildThreads, max_parts * sizeof(uint32_t), L.stream>>>(tasks_dev, ntasks,
+    k_part_hist_grouped<<<total_chunks, kPartThreads, max_parts * sizeof(uint32_t), L.stream>>>(tasks_dev, ntasks,
                                                                                                   matrix);
     count_launches(1);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     e = scan_u32_to_u64(L, matrix, offsets, total_cells, t);
     if (e != cudaSuccess) return e;
-    k_part_scatter_grouped<<<total_chunks, kBuildThreads, 2 * max_parts * sizeof(uint32_t), L.stream>>>(
+    k_part_scatter_grouped<<<total_chunks, kPartThreads, max_parts * sizeof(uint32_t), L.stream>>>(
         tasks_dev, ntasks, offsets);
     count_launches(1);
     e = cudaGetLastError();

@@ -73,11 +73,14 @@ CJ_DEV void put_key(const MatchOut &out, unsigned long long pos, int64_t key) {
         __stcs(reinterpret_cast<long long *>(out.key_pages + 8 + 8 * q + 136 * (q / kRowsPerPage8B)), (long long)key);
 }
 
-/* Directory entry: start of the slot's tuples (bits 63..32), their count
- * (31..16, saturated at 0xFFFF: then the next entry's start bounds them) and
- * the OR of their Bloom tags (15..0). */
+/* Directory entry word: start of the slot's tuples (bits 63..32), their
+ * count (31..16, saturated at 0xFFFF: then the next entry's start bounds
+ * them) and the OR of their Bloom tags (15..0). INT32-key tables hold the
+ * slot's first tuple in the entry too (DirEntry32, 16 bytes, one sector):
+ * a row whose slot has one tuple is answered by that one random load. */
 template <typename KB> struct HashMatcher {
     static constexpr bool kAtMostOne = false;
+    static constexpr bool kInline = sizeof(KB) == 4;
     static constexpr int kMinBlocks = CJ_HASH_MIN_BLOCKS;
     static constexpr int kItems = kProbeItems;
     CJ_DEV HashMatcher resolved() const { return *this; }
@@ -86,24 +89,51 @@ template <typename KB> struct HashMatcher {
     struct Shared {
         uint16_t bloom[2048];
     };
+    struct Entry {
+        uint32_t s, n;   /* tuple range                      */
+        int32_t key0;    /* inline first tuple (INT32 keys)  */
+        uint32_t rid0;
+    };
     CJ_DEV bool skip() const { return false; }
     CJ_DEV void init(Shared &sh) const { load_bloom(sh.bloom, g_bloom); }
-    CJ_DEV void range(const Shared &sh, int64_t key, uint32_t &s, uint32_t &n) const {
+    /* The slot's tuple range, empty when the Bloom tags rule the key out. */
+    CJ_DEV Entry entry(const Shared &sh, int64_t key) const {
         const uint64_t h = hash_key(key);
         const uint32_t slot = slot_of(h, ht.log2_slots);
-        const uint64_t e = __ldg(ht.dir + slot);
+        Entry en{0, 0, 0, 0};
+        uint64_t e;
+        if (kInline) {
+            const uint4 v = __ldg(reinterpret_cast<const uint4 *>(ht.dir) + slot);
+            e = (uint64_t)v.x | ((uint64_t)v.y << 32);
+            en.key0 = (int32_t)v.z;
+            en.rid0 = v.w;
+        } else {
+            e = __ldg(ht.dir + slot);
+        }
         const uint32_t tag = sh.bloom[bloom_index(h)];
-        n = 0;
-        s = (uint32_t)(e >> 32);
-        if (((uint32_t)e & tag) != tag) return;
-        n = (uint32_t)(e >> 16) & 0xFFFFu;
-        if (n == 0xFFFFu) n = (uint32_t)(__ldg(ht.dir + slot + 1) >> 32) - s;
+        en.s = (uint32_t)(e >> 32);
+        if (((uint32_t)e & tag) != tag) return en;
+        en.n = (uint32_t)(e >> 16) & 0xFFFFu;
+        if (en.n == 0xFFFFu) {
+            const uint64_t nx = kInline ? __ldg(reinterpret_cast<const unsigned long long *>(
+                                              reinterpret_cast<const DirEntry32 *>(ht.dir) + slot + 1))
+                                        : __ldg(ht.dir + slot + 1);
+            en.n = (uint32_t)(nx >> 32) - en.s;
+        }
+        return en;
     }
     CJ_DEV uint32_t count(const Shared &sh, int64_t key, uint32_t &first) const {
-        uint32_t s, n, c = 0;
-        range(sh, key, s, n);
-        for (uint32_t j = 0; j < n; ++j) {
-            const Tuple<KB> t = ht.tuples[s + j];
+        const Entry en = entry(sh, key);
+        uint32_t c = 0, j = 0;
+        if (kInline && en.n) { /* tuple 0 came with the entry */
+            if ((int64_t)en.key0 == key) {
+                first = en.rid0;
+                c = 1;
+            }
+            j = 1;
+        }
+        for (; j < en.n; ++j) {
+            const Tuple<KB> t = ht.tuples[en.s + j];
             if ((int64_t)t.key == key) {
                 if (!c) first = t.rid;
                 ++c;
@@ -113,10 +143,9 @@ template <typename KB> struct HashMatcher {
     }
     CJ_DEV void write_all(const Shared &sh, int64_t key, unsigned long long pos, uint32_t prow,
                           const MatchOut &out) const {
-        uint32_t s, n;
-        range(sh, key, s, n);
-        for (uint32_t j = 0; j < n; ++j) {
-            const Tuple<KB> t = ht.tuples[s + j];
+        const Entry en = entry(sh, key);
+        for (uint32_t j = 0; j < en.n; ++j) {
+            const Tuple<KB> t = ht.tuples[en.s + j];
             if ((int64_t)t.key != key) continue;
             if (pos < out.capacity) {
                 if (out.build_rids) out.build_rids[pos] = t.rid;

@@ -38,7 +38,7 @@ namespace {
 
 constexpr uint64_t kNoAllocMaxBuild = 1ull << 18;  /* 262,144 build rows     */
 constexpr uint64_t kNoAllocMaxProbe = 1ull << 27;  /* 134,217,728 probe rows */
-constexpr size_t kNoAllocScratchBytes = 8u << 20;  /* 8 MiB per device      */
+constexpr size_t kNoAllocScratchBytes = 12u << 20; /* 12 MiB per device     */
 constexpr int kMaxDevices = 64;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
@@ -113,7 +113,7 @@ extern "C" int cj_hash_join_noalloc(const int32_t *build_keys, const uint32_t *b
         return cj::set_last_error(CJ_ERR_INVALID_ARGUMENT, "null argument");
     if (n_build > kNoAllocMaxBuild || n_probe > kNoAllocMaxProbe)
         return cj::set_last_error(CJ_ERR_LIMIT, "cj_hash_join_noalloc takes at most 262144 build rows and "
-                                                "134217728 probe rows (fixed 8 MiB scratch)");
+                                                "134217728 probe rows (fixed 12 MiB scratch)");
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return cuda_status(e, "cudaGetDevice");
@@ -134,7 +134,7 @@ extern "C" int cj_hash_join_noalloc(const int32_t *build_keys, const uint32_t *b
         bp.num_rows = n_build;
         bp.log2_slots = ceil_log2(n_build) > 11 ? ceil_log2(n_build) : 11;
         bp.log2_parts = bp.log2_slots - 11 < 12 ? bp.log2_slots - 11 : 12;
-        const size_t dir_bytes = align256(cj::build_dir_bytes(bp.log2_slots));
+        const size_t dir_bytes = align256(cj::build_dir_bytes(bp.log2_slots, 4));
         const size_t tup_off = kDirOff + dir_bytes;
         const size_t build_off = tup_off + align256((size_t)n_build * cj::build_tuple_bytes(4));
         const size_t probe_off = build_off + align256(cj::build_temp_bytes(L, bp, 4));

@@ -5,13 +5,23 @@
  *
  * A server owns `slots` worker threads, each with its own context (CUDA
  * stream, status block, staging) and all allocating from one shared,
- * stream-ordered memory pool. Requests queue in arrival order; the head of
- * the queue is admitted as soon as a slot is free and its estimated device
- * footprint fits in the memory budget next to the plans already running,
- * so work of different plans overlaps on the device while the sum of their
- * estimates never exceeds the budget. A plan whose estimate alone exceeds
- * the budget is rejected at submission (CJ_ERR_REJECTED). Latency is
- * measured from submission to completion.
+ * stream-ordered memory pool. Requests queue in arrival order. A worker
+ * that frees up admits queued plans whose estimated device footprint fits
+ * in the memory budget next to the plans already running, and runs them
+ * together (continuous batching):
+ *   - up to max_batch plans per admission, and no more than an even share of
+ *     the queue per idle worker, so that a short queue spreads over the
+ *     workers and a long one is taken in batches;
+ *   - one plan runs through the one-plan executor; several run as one
+ *     grouped execution (execute_batch: every phase of a plan level is one
+ *     launch over all of them), whose results equal each plan run alone;
+ *   - admission goes in arrival order, but a plan that does not fit may be
+ *     passed over by later ones that do until it has waited age_limit_us;
+ *     after that nothing passes it, so it cannot starve.
+ * Work of different workers overlaps on the device through their streams,
+ * while the sum of the running plans' estimates stays within the budget. A
+ * plan whose estimate alone exceeds the budget is rejected at submission
+ * (CJ_ERR_REJECTED). Latency is measured from submission to completion.
  */
 #include <algorithm>
 #include <chrono>
@@ -110,6 +120,8 @@ struct cj_server {
     cudaMemPool_t pool = nullptr;
     uint64_t budget = 0;
     uint32_t flags = 0;
+    uint32_t max_batch = 32;
+    double age_limit_us = 20000;
     std::vector<std::unique_ptr<cj::Context>> workers;
     std::vector<std::thread> threads;
 
@@ -129,74 +141,143 @@ struct cj_server {
     std::unordered_map<uint64_t, Req> reqs;
     uint64_t next_ticket = 1;
     uint64_t admitted = 0, peak_admitted = 0;
-    uint32_t running = 0;
+    uint32_t running = 0;      /* plans running                       */
+    uint32_t busy_workers = 0; /* workers running a plan or a batch   */
+    uint64_t batches = 0, batched_plans = 0, skipped_ahead = 0;
     bool stop = false;
     /* statistics */
     uint64_t submitted = 0, completed = 0, failed = 0, rejected = 0, cancelled = 0;
     std::vector<double> latencies;
     double t_first = 0, t_last = 0;
 
+    /* Takes the plans this worker runs next (lock held): queued plans that
+     * fit in the budget, in arrival order, passing over one that does not
+     * fit unless it has waited past the age limit. */
+    bool take(std::vector<uint64_t> &out) {
+        if (queue.empty()) return false;
+        const double now = now_us();
+        const size_t idle = std::max<size_t>(1, workers.size() - busy_workers);
+        const size_t share = (queue.size() + idle - 1) / idle;
+        const size_t limit = std::max<size_t>(1, std::min<size_t>(max_batch, share));
+        uint64_t room = budget > admitted ? budget - admitted : 0;
+        bool passed = false;
+        for (auto it = queue.begin(); it != queue.end() && out.size() < limit;) {
+            Req &r = reqs[*it];
+            if (r.est <= room) {
+                if (passed) ++skipped_ahead;
+                out.push_back(*it);
+                room -= r.est;
+                it = queue.erase(it);
+                continue;
+            }
+            if (now - r.t_submit > age_limit_us) break; /* aged: it goes first */
+            passed = true;
+            ++it;
+        }
+        return !out.empty();
+    }
+
+    void finish(uint64_t ticket, int status, const std::string &err, cj_result *res, const cj_exec_stats &st) {
+        Req &r = reqs[ticket];
+        r.status = status;
+        r.err = err;
+        r.res = res;
+        r.stats = st;
+        r.done = true;
+        r.t_done = now_us();
+        admitted -= r.est;
+        --running;
+        if (status == CJ_OK) {
+            ++completed;
+            latencies.push_back(r.t_done - r.t_submit);
+        } else {
+            ++failed;
+        }
+        t_last = r.t_done;
+    }
+
+    /* One plan through the one-plan executor; the status and message of a
+     * failure, the context left usable. */
+    static int run_one(cj::Context &ctx, const cj_plan_desc &plan, uint32_t flags, cj_result **res,
+                       cj_exec_stats *st, std::string &err) {
+        try {
+            *res = cj::execute_plan(ctx, plan, flags, st);
+            return CJ_OK;
+        } catch (const cj::Error &e) {
+            err = e.msg;
+            cudaStreamSynchronize(ctx.stream);
+            cudaGetLastError();
+            return e.code;
+        } catch (const std::bad_alloc &) {
+            err = "host allocation failed";
+            return CJ_ERR_OUT_OF_MEMORY;
+        } catch (...) {
+            err = "unexpected exception";
+            return CJ_ERR_INTERNAL;
+        }
+    }
+
     void worker(size_t w) {
         cj::Context &ctx = *workers[w];
         cudaSetDevice(device);
         for (;;) {
-            uint64_t ticket = 0;
-            const cj_plan_desc *plan = nullptr;
+            std::vector<uint64_t> tickets;
+            std::vector<cj_plan_desc> plans;
             {
                 std::unique_lock<std::mutex> lk(mu);
-                cv_work.wait(lk, [&] {
-                    if (stop) return true;
-                    if (queue.empty()) return false;
-                    const Req &h = reqs[queue.front()];
-                    return admitted + h.est <= budget || running == 0;
-                });
+                /* wake on new work, on freed budget, and at least every
+                 * millisecond so that ageing takes effect */
+                while (!stop && !take(tickets)) cv_work.wait_for(lk, std::chrono::milliseconds(1));
                 if (stop) return;
-                ticket = queue.front();
-                queue.pop_front();
-                Req &r = reqs[ticket];
-                r.started = true;
-                r.t_start = now_us();
-                admitted += r.est;
+                ++busy_workers;
+                ++batches;
+                batched_plans += tickets.size();
+                for (uint64_t t : tickets) {
+                    Req &r = reqs[t];
+                    r.started = true;
+                    r.t_start = now_us();
+                    admitted += r.est;
+                    ++running;
+                    plans.push_back(*r.plan);
+                }
                 peak_admitted = std::max(peak_admitted, admitted);
-                ++running;
-                plan = r.plan;
             }
-            int status = CJ_OK;
-            std::string err;
-            cj_result *res = nullptr;
-            cj_exec_stats st{};
-            try {
-                res = cj::execute_plan(ctx, *plan, flags, &st);
-            } catch (const cj::Error &e) {
-                status = e.code;
-                err = e.msg;
-                cudaStreamSynchronize(ctx.stream);
-                cudaGetLastError();
-            } catch (const std::bad_alloc &) {
-                status = CJ_ERR_OUT_OF_MEMORY;
-                err = "host allocation failed";
-            } catch (...) {
-                status = CJ_ERR_INTERNAL;
-                err = "unexpected exception";
+            const size_t n = tickets.size();
+            std::vector<cj_result *> res(n, nullptr);
+            std::vector<int> status(n, CJ_OK);
+            std::vector<std::string> err(n);
+            std::vector<cj_exec_stats> st(n, cj_exec_stats{});
+            bool done = false;
+            if (n > 1) {
+                /* one grouped execution; if it fails as a whole (a device
+                 * error, memory), each plan runs alone so that one plan's
+                 * failure is not every plan's */
+                std::vector<int32_t> sts(n, CJ_OK);
+                cj_batch_stats bst{};
+                try {
+                    cj::execute_batch(ctx, plans.data(), n, flags, res.data(), sts.data(), &bst);
+                    for (size_t i = 0; i < n; ++i) {
+                        status[i] = sts[i];
+                        if (sts[i] != CJ_OK) err[i] = "plan failed validation";
+                        st[i].total_us = bst.total_us;
+                        st[i].kernel_launches = bst.kernel_launches;
+                    }
+                    done = true;
+                } catch (...) {
+                    for (auto &r : res) {
+                        if (r) cj_result_free(r);
+                        r = nullptr;
+                    }
+                    cudaStreamSynchronize(ctx.stream);
+                    cudaGetLastError();
+                }
             }
+            if (!done)
+                for (size_t i = 0; i < n; ++i) status[i] = run_one(ctx, plans[i], flags, &res[i], &st[i], err[i]);
             {
                 std::lock_guard<std::mutex> lk(mu);
-                Req &r = reqs[ticket];
-                r.status = status;
-                r.err = err;
-                r.res = res;
-                r.stats = st;
-                r.done = true;
-                r.t_done = now_us();
-                admitted -= r.est;
-                --running;
-                if (status == CJ_OK) {
-                    ++completed;
-                    latencies.push_back(r.t_done - r.t_submit);
-                } else {
-                    ++failed;
-                }
-                t_last = r.t_done;
+                for (size_t i = 0; i < n; ++i) finish(tickets[i], status[i], err[i], res[i], st[i]);
+                --busy_workers;
             }
             cv_done.notify_all();
             cv_work.notify_all();
@@ -228,6 +309,8 @@ int cj_server_create(const cj_server_config *cfg, cj_server **out) {
         s->device = dev;
         s->pool = cj::create_pool(dev);
         s->flags = cfg->exec_flags;
+        s->max_batch = cfg->max_batch ? cfg->max_batch : 32;
+        s->age_limit_us = cfg->age_limit_us ? (double)cfg->age_limit_us : 20000.0;
         size_t free_b = 0, total_b = 0;
         cj::check_cuda(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo");
         s->budget = cfg->memory_budget ? cfg->memory_budget : (uint64_t)(free_b * 0.85);
@@ -329,10 +412,14 @@ int cj_server_get_stats(cj_server *s, cj_server_stats *out, int reset) {
     }
     st.wall_s = s->t_last > s->t_first ? (s->t_last - s->t_first) / 1e6 : 0;
     st.plans_per_s = st.wall_s > 0 ? s->completed / st.wall_s : 0;
+    st.batches = s->batches;
+    st.skipped_ahead = s->skipped_ahead;
+    st.mean_batch = s->batches ? (double)s->batched_plans / s->batches : 0;
     *out = st;
     if (reset) {
         s->latencies.clear();
         s->completed = s->failed = s->rejected = s->cancelled = s->submitted = 0;
+        s->batches = s->batched_plans = s->skipped_ahead = 0;
         s->t_first = s->t_last = 0;
         s->peak_admitted = s->admitted;
     }

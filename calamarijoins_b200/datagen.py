@@ -10,6 +10,8 @@ sizes and value distributions of the benchmark configurations instead:
   config_c2  4,000,000 unique shuffled build keys joined with 64,000,000
              probe rows: Zipf(0.8) foreign keys, 30% outside the build
              domain, 2% NULL; outputs 2 INT32 + INT64 + FP64
+  config_c2h C2's shape with a non-unique build side (4M rows over 3M
+             distinct keys): the unchained hash table's workload
   config_c3  left-deep 6-way pipeline: 36,000,000-row fact table with five
              INT32 foreign keys (Zipf s in {0.5, 1.0, 1.2}) into dimensions of
              2,500 / 130,000 / 1,200,000 / 2,500,000 / 4,200,000 rows filtered
@@ -187,6 +189,35 @@ def config_c2s(seed: int = 212, scale: float = 1.0, pinned: bool = False, int32_
     return join2(nb, npr, seed=seed, zipf=0.8, outside=0.30, probe_null=0.02,
                  build_payload=payloads or (DataType.INT64,), probe_payload=payloads or (DataType.FP64,),
                  output=[0, 1, 2, 3], pinned=pinned, key_scale=500)
+
+
+def config_c2h(seed: int = 222, scale: float = 1.0, pinned: bool = False, int32_standin: bool = False) -> Plan:
+    """C2's shape with a non-unique build side, so that only the unchained
+    hash table serves it: 4,000,000 build rows over 3,000,000 distinct keys
+    (a third of them appear twice), INT64 payload; 64,000,000 probe rows,
+    foreign keys Zipf(0.8) over the distinct keys, 30 % outside the build
+    domain, 2 % NULL, FP64 payload. About 58.5M output rows."""
+    rng = np.random.default_rng(seed)
+    nb, npr = max(int(4_000_000 * scale), 16), max(int(64_000_000 * scale), 16)
+    nd = max(nb * 3 // 4, 1)
+    distinct = rng.permutation(nd).astype(np.int64)
+    bkeys = np.concatenate([distinct, distinct[:nb - nd]])
+    rng.shuffle(bkeys)
+    I = DataType.INT32
+    bp = (I,) if int32_standin else (DataType.INT64,)
+    pp = (I,) if int32_standin else (DataType.FP64,)
+    bcols = [encode_column(I, bkeys.astype(np.int32), pinned=pinned)] + [_payload(t, nb, rng, pinned=pinned)
+                                                                         for t in bp]
+    fk, fv = fk_column(distinct, npr, 0.8, 0.30, 0.02, rng)
+    pcols = [encode_column(I, fk, fv, pinned=pinned)] + [_payload(t, npr, rng, pinned=pinned) for t in pp]
+    plan = Plan()
+    plan.inputs.append(ColumnarTable(nb, bcols))
+    plan.inputs.append(ColumnarTable(npr, pcols))
+    plan.new_scan_node(0, [(0, I), (1, bp[0])])
+    plan.new_scan_node(1, [(0, I), (1, pp[0])])
+    plan.new_join_node(True, 0, 1, 0, 0, [(0, I), (1, bp[0]), (2, I), (3, pp[0])])
+    plan.root = 2
+    return plan
 
 
 C3_DIMS = (2_500, 130_000, 1_200_000, 2_500_000, 4_200_000)

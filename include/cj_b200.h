@@ -351,7 +351,7 @@ int cj_execute_batch(cj_context *ctx, const cj_plan_desc *plans,
  * them all. Work runs on `stream`
  * (a cudaStream_t) and the call returns after it completes.
  * Allocates nothing: the hash table and every scratch buffer live in one
- * fixed 8 MiB device array that each GPU loading the library holds until
+ * fixed 12 MiB device array that each GPU loading the library holds until
  * exit. Limits: n_build <= 262,144 and n_probe <= 134,217,728; larger inputs
  * get CJ_ERR_LIMIT. The first call on a device looks up that array's device
  * address, so make it before any stream capture. Calls share the array:
@@ -389,11 +389,21 @@ typedef struct cj_server cj_server;
 
 typedef struct cj_server_config {
     int32_t device;          /* -1 = current device                          */
-    uint32_t slots;          /* plans running at once (worker streams); 0 = 4 */
+    uint32_t slots;          /* worker streams, each running one plan or one
+                                batch of plans at a time; 0 = 4              */
     uint64_t memory_budget;  /* device bytes that admitted plans may hold by
                                 estimate; 0 = 85% of the free memory         */
     uint32_t exec_flags;     /* cj_exec_flags for every result               */
-    uint32_t reserved;
+    uint32_t max_batch;      /* continuous batching: a slot that frees up
+                                takes up to this many queued plans that fit
+                                the budget and runs them as one grouped
+                                execution (cj_execute_batch); 0 = 32, 1 = one
+                                plan per slot                                */
+    uint64_t age_limit_us;   /* admission passes over a queued plan that
+                                does not fit beside the running ones to
+                                admit later plans that do, for at most this
+                                long after its submission; then it goes
+                                first; 0 = 20,000                            */
 } cj_server_config;
 
 typedef struct cj_server_stats {
@@ -403,6 +413,11 @@ typedef struct cj_server_stats {
     double p50_us, p99_us, mean_us, max_us; /* submit -> completion         */
     double wall_s;                          /* first submit -> last finish  */
     double plans_per_s;
+    uint64_t batches;                       /* executions (one plan or a
+                                               grouped batch)               */
+    uint64_t skipped_ahead;                 /* plans admitted ahead of an
+                                               earlier one that did not fit */
+    double mean_batch;                      /* plans per execution          */
 } cj_server_stats;
 
 int cj_server_create(const cj_server_config *config, cj_server **out);
@@ -410,8 +425,11 @@ int cj_server_create(const cj_server_config *config, cj_server **out);
 /* Queues a plan. The plan description and every page it points to must stay
  * valid until cj_server_wait returns for the ticket. Plans whose estimated
  * footprint (cj_server_estimate) exceeds the budget are refused with
- * CJ_ERR_REJECTED; others wait in arrival order until a slot is free and
- * their estimate fits beside the running plans. */
+ * CJ_ERR_REJECTED; others wait until a slot is free and their estimate fits
+ * beside the running plans. Admission goes in arrival order, except that a
+ * plan that does not fit may be passed over by later plans that do, for at
+ * most age_limit_us. Each result equals what cj_execute returns for the
+ * plan alone. */
 int cj_server_submit(cj_server *server, const cj_plan_desc *plan,
                      uint64_t *ticket);
 

@@ -492,3 +492,19 @@ def test_memory_returns_to_pool(gpu_ctx):
         run_product(plan, gpu_ctx)
     used2, _ = gpu_ctx.memory()
     assert used2 <= used1
+
+
+@pytest.mark.parametrize("spp", [64, 2048, 16384])
+def test_radix_passes_any_partition_size(gpu_ctx, spp):
+    """Directory slots per partition 64 (2^13 partitions for 2^19 slots: two
+    radix passes), 2048 (one pass) and 16384: the same results."""
+    gpu_ctx.set_option(_lib.CJ_OPT_SLOTS_PER_PARTITION, spp)
+    gpu_ctx.set_option(_lib.CJ_OPT_DENSE_KEYS, 0)
+    try:
+        for plan in (join2(300_000, 1_000_000, seed=41, unique_build=False, zipf=0.7, probe_null=0.05),
+                     join2(300_000, 900_000, seed=42, key_type=L, zipf=0.9, outside=0.2)):
+            r, st = run_product(plan, gpu_ctx)
+            assert_same(r, run_oracle(plan), f"spp {spp}")
+    finally:
+        gpu_ctx.set_option(_lib.CJ_OPT_SLOTS_PER_PARTITION, 0)
+        gpu_ctx.set_option(_lib.CJ_OPT_DENSE_KEYS, 8)

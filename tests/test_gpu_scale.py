@@ -81,6 +81,19 @@ def test_c2_full_size_hash_table(gpu_ctx):
         gpu_ctx.set_option(_lib.CJ_OPT_DENSE_KEYS, 8)
 
 
+def test_c2h_full_size(gpu_ctx):
+    """C2's shape with a non-unique build side (4M rows over 3M distinct
+    keys): only the unchained hash table can serve it; about 59M output
+    rows."""
+    from calamarijoins_b200.datagen import config_c2h
+    plan = config_c2h(scale=1.0)
+    want = run_oracle(plan)
+    assert want.num_rows > 50_000_000
+    got, st = run_product(plan, gpu_ctx)
+    assert st.exec["num_direct_joins"] == 0 and st.exec["num_open_joins"] == 0
+    assert_same(got, want, "c2h")
+
+
 @pytest.mark.parametrize("varchar_nulls", [False, True])
 def test_c3_full_size(gpu_ctx, varchar_nulls):
     """C3 at full size: the 36M-row fact table through five joins into
@@ -177,3 +190,28 @@ def test_direct_mapped_span_limit(gpu_ctx, span_extra, direct):
     assert st.exec["num_direct_joins"] == (1 if direct else 0)
     assert st.exec["num_open_joins"] == (0 if direct else 1)
     assert_same(got, want, f"span 2^28+{span_extra}")
+
+
+def test_two_pass_radix_build(gpu_ctx):
+    """A non-unique build side of 9,000,000 rows: 2^24 directory slots in
+    2^13 partitions, more radix bits than one pass takes, so the build runs
+    a second, per-partition radix pass."""
+    from calamarijoins_b200.datagen import fk_column
+    rng = np.random.default_rng(31)
+    nb, npr = 9_000_000, 20_000_000
+    distinct = rng.permutation(6_000_000).astype(np.int64) * 3 - 9_000_000
+    bk = np.concatenate([distinct, distinct[:nb - len(distinct)]])
+    rng.shuffle(bk)
+    pk, pv = fk_column(distinct, npr, 0.9, 0.2, 0.02, rng)
+    plan = Plan()
+    plan.inputs.append(ColumnarTable(nb, [encode_column(I, bk.astype(np.int32)),
+                                          encode_column(I, rng.integers(0, 1 << 30, nb).astype(np.int32))]))
+    plan.inputs.append(ColumnarTable(npr, [encode_column(I, pk, pv)]))
+    plan.new_scan_node(0, [(0, I), (1, I)])
+    plan.new_scan_node(1, [(0, I)])
+    plan.new_join_node(True, 0, 1, 0, 0, [(1, I), (2, I)])
+    plan.root = 2
+    want = run_oracle(plan)
+    got, st = run_product(plan, gpu_ctx)
+    assert st.exec["num_direct_joins"] == 0 and st.exec["num_open_joins"] == 0
+    assert_same(got, want, "two-pass build")

@@ -85,3 +85,51 @@ def test_failure_is_isolated():
         assert_same(r, run_oracle(good))
     finally:
         srv.close()
+
+
+def test_continuous_batching_equals_alone(gpu_ctx):
+    """One worker, many plans queued at once: the worker takes them in
+    batches (one grouped execution each) and every result equals the plan
+    run alone."""
+    plans = mixed_plans(30, seed=6)
+    alone = [run_product(p, gpu_ctx)[0] for p in plans]
+    srv = Server(slots=1, max_batch=16)
+    try:
+        tickets = [srv.submit(p) for p in plans]
+        got = []
+        for t in tickets:
+            res, _ = srv.wait(t)
+            got.append(oa.PagedResult.from_result(res))
+            res.free()
+        st = srv.stats()
+    finally:
+        srv.close()
+    assert st["completed"] == len(plans)
+    assert st["mean_batch"] > 1.5, st
+    for i, (a, g) in enumerate(zip(alone, got)):
+        assert_same(g, a, f"plan {i} batched vs alone")
+
+
+def test_admission_passes_over_a_plan_that_does_not_fit():
+    """Two slots, a budget that holds one large plan and a few small ones:
+    while the first large plan runs, a second large plan waits, and the
+    small plans behind it are admitted ahead of it (it has not waited past
+    the age limit); the second large plan runs once the first is done."""
+    big = [join2(500_000, 12_000_000, seed=20 + i, probe_payload=(I,)) for i in range(2)]
+    small = [join2(500, 5_000, seed=30 + i) for i in range(6)]
+    eb = max(Server.estimate(p) for p in big)
+    es = max(Server.estimate(p) for p in small)
+    srv = Server(slots=2, memory_budget=eb + 3 * es, max_batch=1, age_limit_us=10_000_000)
+    try:
+        t_big = [srv.submit(p) for p in big]
+        t_small = [srv.submit(p) for p in small]
+        for t, p in zip(t_big + t_small, big + small):
+            res, _ = srv.wait(t)
+            r = oa.PagedResult.from_result(res)
+            res.free()
+            assert_same(r, run_oracle(p))
+        st = srv.stats()
+    finally:
+        srv.close()
+    assert st["skipped_ahead"] >= 1, st
+    assert st["peak_admitted_bytes"] <= st["memory_budget"]
