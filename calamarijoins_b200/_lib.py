@@ -146,6 +146,9 @@ _SIGS = {
     "cj_result_column_device": (C.c_int, [_P, C.c_uint64, C.POINTER(_P)]),
     "cj_result_copy_column": (C.c_int, [_P, C.c_uint64, _P, C.c_uint64]),
     "cj_result_free": (None, [_P]),
+    "cj_batch_prepare": (C.c_int, [_P, _P, C.c_uint64, C.c_uint32, C.POINTER(_P)]),
+    "cj_batch_run": (C.c_int, [_P, C.POINTER(_P), C.POINTER(BatchStatsC)]),
+    "cj_prepared_free": (None, [_P]),
     "cj_server_create": (C.c_int, [C.POINTER(ServerConfigC), C.POINTER(_P)]),
     "cj_server_submit": (C.c_int, [_P, C.POINTER(PlanDesc), C.POINTER(C.c_uint64)]),
     "cj_server_wait": (C.c_int, [_P, C.c_uint64, C.c_int64, C.POINTER(_P), C.POINTER(ExecStatsC)]),

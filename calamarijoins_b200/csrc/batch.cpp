@@ -18,6 +18,16 @@
  *
  * Results are the same as cj_execute on each plan: the same kernels' unit
  * bodies run on the same data, only scheduled together.
+ *
+ * Prepared batches (cj_batch_prepare / cj_batch_run) run the same executor
+ * three ways: once as usual while it records every join's match count and
+ * every VARCHAR column's page count (learn), then once under CUDA stream
+ * capture with those counts as exact output sizes (capture): no host
+ * synchronisation and no host read of a device value anywhere, every buffer
+ * carved from one arena, every task table copied from pinned memory. The
+ * captured graph is replayed by cj_batch_run: one launch for the whole
+ * batch. Kernels in the graph compare each count with the recorded one and
+ * raise DEV_ERR_STALE when they differ (the inputs changed).
  */
 #include <algorithm>
 #include <chrono>
@@ -68,10 +78,43 @@ struct PlanState {
     std::vector<DevPtr> keep; /* match arrays the root views point into */
 };
 
+} // namespace
+
+/* What a learning run records for the capture: match counts of every join
+ * of every level, in the executor's work order, and page counts of every
+ * VARCHAR output column, in materialisation order. */
+struct BatchLearned {
+    std::vector<std::vector<uint64_t>> level_M;
+    std::vector<uint64_t> var_pages;
+};
+
+/* Pinned host memory, bump-allocated in 4 MiB blocks: the source of every
+ * host-to-device copy captured into a graph (it must outlive the graph). */
+struct PinnedBump {
+    Context *ctx = nullptr;
+    std::vector<PinnedPtr> blocks;
+    size_t used = 0;
+    void *take(size_t n) {
+        n = (n + 15) & ~size_t(15);
+        if (blocks.empty() || used + n > blocks.back()->bytes) {
+            blocks.push_back(ctx->alloc_pinned(std::max<size_t>(n, 4u << 20)));
+            used = 0;
+        }
+        void *p = static_cast<uint8_t *>(blocks.back()->ptr) + used;
+        used += n;
+        return p;
+    }
+};
+
+namespace {
+
+enum class Mode { Eager, Learn, Capture };
+
 class BatchExecutor {
   public:
-    BatchExecutor(Context &c, const cj_plan_desc *plans, size_t n, uint32_t flags)
-        : ctx(c), L(c.launch()), flags(flags) {
+    BatchExecutor(Context &c, const cj_plan_desc *plans, size_t n, uint32_t flags, Mode mode = Mode::Eager,
+                  BatchLearned *learned = nullptr, PinnedBump *bump = nullptr)
+        : ctx(c), L(c.launch()), flags(flags), mode(mode), learned(learned), bump(bump) {
         ps.resize(n);
         for (size_t i = 0; i < n; ++i) ps[i].plan = &plans[i];
     }
@@ -84,6 +127,11 @@ class BatchExecutor {
     Context &ctx;
     Launch L;
     uint32_t flags;
+    Mode mode;
+    BatchLearned *learned;
+    PinnedBump *bump;
+    size_t level_ix = 0; /* levels run so far (index into learned->level_M) */
+    size_t var_ix = 0;   /* VARCHAR columns planned so far                  */
     std::vector<PlanState> ps;
     std::map<std::tuple<size_t, uint64_t, uint64_t>, Decoded> decoded;
     cj_batch_stats stats{};
@@ -92,10 +140,25 @@ class BatchExecutor {
     void ck(cudaError_t e, const char *w) { check_cuda(e, w); }
     template <typename T> DevPtr upload_tasks(const std::vector<T> &v) {
         DevPtr d = ctx.alloc(std::max<size_t>(v.size(), 1) * sizeof(T));
-        if (!v.empty())
-            ck(cudaMemcpyAsync(d->ptr, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, ctx.stream), "tasks");
+        if (!v.empty()) {
+            const void *src = v.data();
+            if (mode == Mode::Capture) { /* a captured copy needs a source that outlives the graph */
+                void *h = bump->take(v.size() * sizeof(T));
+                std::memcpy(h, v.data(), v.size() * sizeof(T));
+                src = h;
+            }
+            ck(cudaMemcpyAsync(d->ptr, src, v.size() * sizeof(T), cudaMemcpyHostToDevice, ctx.stream), "tasks");
+        }
         return d;
     }
+    /* Device copy of recorded counts, then a check of `counts` against them. */
+    void check_counts(const unsigned long long *counts, const std::vector<uint64_t> &want) {
+        std::vector<unsigned long long> w(want.begin(), want.end());
+        DevPtr d = upload_tasks(w);
+        ck(launch_check_counts(L, counts, d->as<unsigned long long>(), (uint32_t)w.size()), "check_counts");
+        keep_checks.push_back(d);
+    }
+    std::vector<DevPtr> keep_checks;
     int levels(PlanState &p, uint64_t node, int depth);
     void decode_all();
     Decoded &dec(size_t plan, uint64_t t, uint64_t c) { return decoded.at({plan, t, c}); }
@@ -141,6 +204,8 @@ void BatchExecutor::decode_all() {
                 if (d.rows > 0xFFFFFFFFull) fail(CJ_ERR_LIMIT, "table exceeds 2^32-1 rows");
                 if (const cj_table *r = resident_input(plan, sn.base_table_id))
                     d.src = r->cols[sn.output_attrs[a].index];
+                else if (mode == Mode::Capture)
+                    fail(CJ_ERR_UNSUPPORTED, "a prepared batch needs device-resident inputs");
                 else
                     upload_pages(ctx, plan.inputs[sn.base_table_id].columns[sn.output_attrs[a].index], d.src,
                                  &stats.h2d_bytes);
@@ -291,6 +356,13 @@ void BatchExecutor::run_level(int lvl) {
     ck(launch_nl_collect_grouped(L, nt->as<NlCollectTask>(), (uint32_t)ntasks.size()), "nl_collect_grouped");
 
     /* ---- probe: one ticketed launch over the tiles of every join ---- */
+    const std::vector<uint64_t> *known = nullptr; /* capture: the recorded counts */
+    if (mode == Mode::Capture) {
+        if (level_ix >= learned->level_M.size() || learned->level_M[level_ix].size() != work.size())
+            fail(CJ_ERR_INTERNAL, "prepared batch: level shape differs from the learning run");
+        known = &learned->level_M[level_ix];
+        for (size_t k = 0; k < work.size(); ++k) work[k].cap = (*known)[k];
+    }
     for (int attempt = 0; attempt < 2; ++attempt) {
         std::vector<ProbeTask> ptasks;
         std::vector<size_t> pidx;
@@ -339,6 +411,17 @@ void BatchExecutor::run_level(int lvl) {
         DevPtr pt = upload_tasks(ptasks);
         ck(launch_probe_grouped(L, pt->as<ProbeTask>(), (uint32_t)ptasks.size(), tiles, ticket, ctx.d_bloom),
            "probe_grouped");
+        if (known) {
+            /* capture: outputs were sized to the recorded counts; the graph
+             * checks them instead of reading them back */
+            std::vector<uint64_t> want;
+            for (size_t k : pidx) want.push_back((*known)[k]);
+            check_counts(wp + 1, want);
+            for (size_t k : pidx) work[k].M = (*known)[k];
+            keep_checks.push_back(words);
+            keep_checks.push_back(pt);
+            break;
+        }
         std::vector<unsigned long long> counts(nwords);
         ck(cudaMemcpyAsync(counts.data(), words->ptr, counts.size() * 8, cudaMemcpyDeviceToHost, ctx.stream), "counts");
         ctx.sync_status();
@@ -352,6 +435,12 @@ void BatchExecutor::run_level(int lvl) {
         }
         if (!overflow) break;
     }
+    if (mode == Mode::Learn) {
+        std::vector<uint64_t> Ms;
+        for (auto &w : work) Ms.push_back(w.M);
+        learned->level_M.push_back(std::move(Ms));
+    }
+    ++level_ix;
     for (auto &w : work) {
         w.dir.reset();
         w.tuples.reset();
@@ -456,9 +545,19 @@ void BatchExecutor::materialize_roots() {
                "varchar_plan");
         }
         std::vector<unsigned long long> host(var.size());
-        ck(cudaMemcpyAsync(host.data(), totals->ptr, host.size() * 8, cudaMemcpyDeviceToHost, ctx.stream), "copy");
-        ctx.sync_status();
-        stats.syncs++;
+        if (mode == Mode::Capture) {
+            if (learned->var_pages.size() != var.size())
+                fail(CJ_ERR_INTERNAL, "prepared batch: VARCHAR columns differ from the learning run");
+            for (size_t k = 0; k < var.size(); ++k) host[k] = learned->var_pages[k];
+            check_counts(totals->as<unsigned long long>(), learned->var_pages);
+            keep_checks.push_back(totals);
+        } else {
+            ck(cudaMemcpyAsync(host.data(), totals->ptr, host.size() * 8, cudaMemcpyDeviceToHost, ctx.stream),
+               "copy");
+            ctx.sync_status();
+            stats.syncs++;
+            if (mode == Mode::Learn) learned->var_pages.assign(host.begin(), host.end());
+        }
         for (size_t k = 0; k < var.size(); ++k) {
             PlanState &p = ps[var[k].plan];
             cj_result *res = p.result;
@@ -539,8 +638,10 @@ void BatchExecutor::run(cj_result **results, int32_t *statuses, cj_batch_stats *
         } pop;
         materialize_roots();
     }
-    ctx.sync_status();
-    stats.syncs++;
+    if (mode != Mode::Capture) {
+        ctx.sync_status();
+        stats.syncs++;
+    }
     for (size_t i = 0; i < ps.size(); ++i) {
         results[i] = ps[i].result;
         ps[i].result = nullptr;
@@ -564,3 +665,147 @@ void execute_batch(Context &ctx, const cj_plan_desc *plans, size_t n, uint32_t f
 }
 
 } // namespace cj
+
+/* A batch captured as one CUDA graph over buffers it owns. */
+struct cj_prepared {
+    cj::Context *ctx = nullptr;
+    std::vector<cj_plan_desc> plans;
+    uint32_t flags = 0;
+    cj::DevPtr arena;            /* every device buffer of the graph   */
+    cj::PinnedBump bump;         /* sources of the captured task copies */
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    std::vector<cj_result *> templates; /* the results' layout, in the arena */
+    cj_batch_stats capture_stats{};
+    ~cj_prepared() {
+        for (auto *r : templates) delete r;
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+    }
+};
+
+namespace cj {
+
+cj_prepared *prepare_batch(Context &ctx, const cj_plan_desc *plans, size_t n, uint32_t flags) {
+    for (size_t i = 0; i < n; ++i)
+        for (uint64_t t = 0; t < plans[i].num_inputs; ++t)
+            if (!resident_input(plans[i], t))
+                fail(CJ_ERR_UNSUPPORTED, "a prepared batch needs device-resident inputs (cj_table)");
+    auto prep = std::make_unique<cj_prepared>();
+    prep->ctx = &ctx;
+    prep->plans.assign(plans, plans + n);
+    prep->flags = flags;
+    prep->bump.ctx = &ctx;
+    /* 1. learn: run once, recording every count; its allocations bound the
+     *    arena (the capture allocates the same buffers, outputs no larger) */
+    BatchLearned learned;
+    {
+        std::vector<cj_result *> res(n, nullptr);
+        std::vector<int32_t> sts(n, CJ_OK);
+        const uint64_t bytes0 = ctx.alloc_bytes;
+        BatchExecutor ex(ctx, prep->plans.data(), n, flags, Mode::Learn, &learned);
+        try {
+            ex.run(res.data(), sts.data(), nullptr);
+        } catch (...) {
+            for (auto *r : res) delete r;
+            throw;
+        }
+        for (auto *r : res) delete r;
+        for (size_t i = 0; i < n; ++i)
+            if (sts[i] != CJ_OK) fail(sts[i], "plan " + std::to_string(i) + " of the batch failed validation");
+        const uint64_t need = ctx.alloc_bytes - bytes0;
+        check_cuda(cudaStreamSynchronize(ctx.stream), "stream synchronize");
+        prep->arena = ctx.alloc(need + need / 8 + (8u << 20));
+    }
+    /* 2. capture the whole batch into one graph over the arena */
+    ctx.arena_base = prep->arena->as<uint8_t>();
+    ctx.arena_size = prep->arena->bytes;
+    ctx.arena_used = 0;
+    struct ArenaOff {
+        Context &c;
+        ~ArenaOff() { c.arena_base = nullptr; }
+    } arena_off{ctx};
+    check_cuda(cudaStreamBeginCapture(ctx.stream, cudaStreamCaptureModeRelaxed), "begin capture");
+    prep->templates.assign(n, nullptr);
+    try {
+        std::vector<int32_t> sts(n, CJ_OK);
+        BatchExecutor ex(ctx, prep->plans.data(), n, flags, Mode::Capture, &learned, &prep->bump);
+        ex.run(prep->templates.data(), sts.data(), &prep->capture_stats);
+    } catch (...) {
+        cudaGraph_t g = nullptr;
+        cudaStreamEndCapture(ctx.stream, &g);
+        if (g) cudaGraphDestroy(g);
+        cudaGetLastError();
+        throw;
+    }
+    check_cuda(cudaStreamEndCapture(ctx.stream, &prep->graph), "end capture");
+    check_cuda(cudaGraphInstantiate(&prep->exec, prep->graph, 0), "graph instantiate");
+    return prep.release();
+}
+
+void run_prepared(cj_prepared &p, cj_result **results, cj_batch_stats *stats) {
+    Context &ctx = *p.ctx;
+    auto t0 = std::chrono::steady_clock::now();
+    check_cuda(cudaGraphLaunch(p.exec, ctx.stream), "graph launch");
+    ctx.sync_status();
+    for (size_t i = 0; i < p.templates.size(); ++i) {
+        const cj_result *t = p.templates[i];
+        auto *r = new cj_result(*t); /* pages are the prepared batch's: shared, not copied */
+        r->keep = p.arena;
+        results[i] = r;
+    }
+    auto t1 = std::chrono::steady_clock::now();
+    if (stats) {
+        *stats = p.capture_stats;
+        stats->syncs = 1;
+        stats->total_us = std::chrono::duration<double, std::micro>(t1 - t0).count();
+    }
+}
+
+} // namespace cj
+
+extern "C" {
+
+int cj_batch_prepare(cj_context *ctx, const cj_plan_desc *plans, uint64_t num_plans, uint32_t flags,
+                     cj_prepared **out) {
+    if (!ctx || !out || (num_plans && !plans)) return cj::set_last_error(CJ_ERR_INVALID_ARGUMENT, "null argument");
+    *out = nullptr;
+    cudaSetDevice(ctx->device);
+    try {
+        *out = cj::prepare_batch(*ctx, plans, (size_t)num_plans, flags);
+    } catch (const cj::Error &e) {
+        cudaStreamSynchronize(ctx->stream);
+        cudaGetLastError();
+        return cj::set_last_error(e.code, e.msg);
+    } catch (const std::bad_alloc &) {
+        return cj::set_last_error(CJ_ERR_OUT_OF_MEMORY, "host allocation failed");
+    } catch (...) {
+        return cj::set_last_error(CJ_ERR_INTERNAL, "unexpected exception");
+    }
+    cj::clear_last_error();
+    return CJ_OK;
+}
+
+int cj_batch_run(cj_prepared *p, cj_result **results, cj_batch_stats *stats) {
+    if (!p || (!p->templates.empty() && !results)) return cj::set_last_error(CJ_ERR_INVALID_ARGUMENT, "null argument");
+    cudaSetDevice(p->ctx->device);
+    try {
+        cj::run_prepared(*p, results, stats);
+    } catch (const cj::Error &e) {
+        cudaGetLastError();
+        return cj::set_last_error(e.code, e.msg);
+    } catch (const std::bad_alloc &) {
+        return cj::set_last_error(CJ_ERR_OUT_OF_MEMORY, "host allocation failed");
+    }
+    cj::clear_last_error();
+    return CJ_OK;
+}
+
+void cj_prepared_free(cj_prepared *p) {
+    if (!p) return;
+    cudaSetDevice(p->ctx->device);
+    cudaStreamSynchronize(p->ctx->stream);
+    delete p;
+}
+
+} // extern "C"

@@ -57,6 +57,8 @@ enum DevError : uint32_t {
     DEV_ERR_BAD_PAGE_KIND = 1u << 3, /* 0xffff/0xfffe page in a fixed column */
     DEV_ERR_ROW_COUNT = 1u << 5,     /* pages hold more/fewer rows than the
                                         table declares                       */
+    DEV_ERR_STALE = 1u << 6,         /* a prepared batch's counts no longer
+                                        match its inputs                     */
     DEV_ERR_INTERNAL = 1u << 31
 };
 
@@ -320,6 +322,10 @@ struct NlCollectTask {
     uint32_t *count;
 };
 cudaError_t launch_nl_collect_grouped(const Launch &L, const NlCollectTask *tasks_dev, uint32_t ntasks);
+
+/* Raises DEV_ERR_STALE unless counts[i] == expected[i] for every i < n. */
+cudaError_t launch_check_counts(const Launch &L, const unsigned long long *counts,
+                                const unsigned long long *expected, uint32_t n);
 
 /* Headers (n_rows = n_values), zero gaps and all-ones bitmaps of the
  * ceil(rows / R) pages of a NULL-free fixed-width column whose values are

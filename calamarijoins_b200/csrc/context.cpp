@@ -35,7 +35,7 @@ void check_cuda(cudaError_t e, const char *what) {
 }
 
 DevBuf::~DevBuf() {
-    if (ptr && ctx) ctx->release(ptr, cls);
+    if (ptr && ctx && !arena) ctx->release(ptr, cls);
 }
 
 /* Four size classes per power of two (at most 25 % above the request),
@@ -80,6 +80,15 @@ DevPtr Context::alloc(size_t bytes) {
     if (opt.fail_alloc_at > 0 && --opt.fail_alloc_at == 0) /* injected fault (CJ_OPT_FAIL_ALLOC_AT) */
         fail(CJ_ERR_OUT_OF_MEMORY, "device allocation of " + std::to_string(bytes) + " bytes failed (injected)");
     const size_t cls = device_class(bytes);
+    alloc_bytes += cls;
+    if (arena_base) {
+        const size_t off = (arena_used + 255) & ~size_t(255);
+        if (off + bytes > arena_size) fail(CJ_ERR_OUT_OF_MEMORY, "prepared batch arena exhausted");
+        b->ptr = arena_base + off;
+        b->arena = true;
+        arena_used = off + bytes;
+        return b;
+    }
     b->cls = cls;
     {
         std::lock_guard<std::mutex> g(dev_mu);
@@ -168,7 +177,10 @@ void Context::sync_status() {
         if (err & DEV_ERR_BAD_PAGE_KIND) what += " special page in fixed-width column;";
         if (err & DEV_ERR_ROW_COUNT) what += " pages hold a row count other than the table's;";
         if (err & DEV_ERR_INTERNAL) what += " internal;";
-        int code = (err & DEV_ERR_INTERNAL) ? CJ_ERR_INTERNAL : CJ_ERR_MALFORMED_PAGE;
+        if (err & DEV_ERR_STALE) what += " match counts differ from the prepared batch's (inputs changed);";
+        int code = (err & DEV_ERR_INTERNAL) ? CJ_ERR_INTERNAL
+                   : (err & DEV_ERR_STALE)  ? CJ_ERR_INVALID_ARGUMENT
+                                            : CJ_ERR_MALFORMED_PAGE;
         fail(code, "device reported:" + what);
     }
 }

@@ -56,7 +56,8 @@ struct DevBuf {
     Context *ctx = nullptr;
     void *ptr = nullptr;
     size_t bytes = 0;
-    size_t cls = 0; /* bytes actually held (size class) */
+    size_t cls = 0;     /* bytes actually held (size class) */
+    bool arena = false; /* carved from the context's arena: not freed alone */
     ~DevBuf();
     template <typename T> T *as() const { return reinterpret_cast<T *>(ptr); }
 };
@@ -106,6 +107,14 @@ struct Context {
     std::mutex dev_mu;
     void release(void *ptr, size_t cls);
     void trim_buffers(); /* returns every cached buffer to the pool */
+
+    /* Bump arena (a prepared batch's buffers): while arena_base is set,
+     * alloc() carves 256-byte-aligned buffers from it instead of the pool;
+     * they are never freed one by one. alloc_bytes sums the size classes
+     * of every allocation (what an arena for the same work needs). */
+    uint8_t *arena_base = nullptr;
+    size_t arena_size = 0, arena_used = 0;
+    uint64_t alloc_bytes = 0;
 
     /* profiler */
     std::vector<KernelProfile> profile;
@@ -172,6 +181,7 @@ struct cj_result {
     std::vector<cj::DevPtr> dev_pages;
     cj::PinnedPtr host;
     std::vector<uint8_t *> host_cols;
+    cj::DevPtr keep; /* memory the pages live in, when not their own (a prepared batch's arena) */
 };
 
 struct cj_context : cj::Context {};

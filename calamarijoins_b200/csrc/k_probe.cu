@@ -565,6 +565,22 @@ cudaError_t launch_probe_grouped(const Launch &L, const ProbeTask *tasks_dev, ui
     return cudaGetLastError();
 }
 
+namespace {
+__global__ void k_check_counts(const unsigned long long *__restrict__ counts,
+                               const unsigned long long *__restrict__ expected, uint32_t n, unsigned int *errors) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        if (counts[i] != expected[i]) atomicOr(errors, (unsigned int)DEV_ERR_STALE);
+}
+} // namespace
+
+cudaError_t launch_check_counts(const Launch &L, const unsigned long long *counts, const unsigned long long *expected,
+                                uint32_t n) {
+    if (!n) return cudaSuccess;
+    k_check_counts<<<(n + 255) / 256, 256, 0, L.stream>>>(counts, expected, n, L.dev_errors);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_nl_collect_grouped(const Launch &L, const NlCollectTask *tasks_dev, uint32_t ntasks) {
     if (!ntasks) return cudaSuccess;
     k_nl_collect_grouped<<<ntasks, 64, 0, L.stream>>>(tasks_dev);

@@ -305,6 +305,38 @@ def execute_batch(plans, ctx: Context, flags: int = 0, descs=None):
     return results, [sts[i] for i in range(n)], {k: getattr(bs, k) for k, _ in _lib.BatchStatsC._fields_}
 
 
+class PreparedBatch:
+    """A batch of plans over device-resident tables captured as one CUDA
+    graph (cj_batch_prepare); run() replays it (cj_batch_run). The pages of
+    a run's results are overwritten by the next run."""
+
+    def __init__(self, plans, ctx: Context, flags: int = 0, descs=None):
+        self.descs = descs or [p if isinstance(p, PlanDescriptor) else PlanDescriptor(p) for p in plans]
+        self.n = len(self.descs)
+        self._arr = (_lib.PlanDesc * max(self.n, 1))()
+        for i, d in enumerate(self.descs):
+            self._arr[i] = d.desc
+        h = C.c_void_p()
+        check(lib().cj_batch_prepare(ctx.handle, self._arr, self.n, int(flags), C.byref(h)))
+        self.handle = h.value
+        self.ctx = ctx
+
+    def run(self):
+        outs = (C.c_void_p * max(self.n, 1))()
+        bs = _lib.BatchStatsC()
+        check(lib().cj_batch_run(self.handle, outs, C.byref(bs)))
+        return [Result(outs[i]) for i in range(self.n)], {k: getattr(bs, k) for k, _ in _lib.BatchStatsC._fields_}
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib().cj_prepared_free(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        if not _finalizing():
+            self.close()
+
+
 class Server:
     """Serving front end (cj_server): plans submitted as they arrive run
     concurrently in `slots` worker streams under a device-memory budget; a

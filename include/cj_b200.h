@@ -336,6 +336,26 @@ int cj_execute_batch(cj_context *ctx, const cj_plan_desc *plans,
                      uint64_t num_plans, uint32_t flags, cj_result **results,
                      int32_t *statuses, cj_batch_stats *stats);
 
+/* Prepared batches (no reference counterpart): a batch of plans whose
+ * inputs are all device-resident (cj_table), captured once as one CUDA
+ * graph and replayed as often as wanted. cj_batch_prepare runs the batch
+ * once to learn every join's match count and every VARCHAR column's page
+ * count, then captures the same execution with outputs sized to those
+ * counts, without any host synchronisation inside, over device buffers it
+ * owns. cj_batch_run launches that graph (one launch for all the plans'
+ * kernels) and waits for it. The results of a run equal cj_execute's for
+ * each plan; their pages live in the prepared batch's buffers and are
+ * overwritten by the next run of the same batch (free them or copy them
+ * before). A run whose inputs no longer give the learned counts (the
+ * resident tables were changed) fails with CJ_ERR_INVALID_ARGUMENT; prepare
+ * the batch again. Plans with host inputs: CJ_ERR_UNSUPPORTED. */
+typedef struct cj_prepared cj_prepared;
+int cj_batch_prepare(cj_context *ctx, const cj_plan_desc *plans,
+                     uint64_t num_plans, uint32_t flags, cj_prepared **out);
+int cj_batch_run(cj_prepared *batch, cj_result **results,
+                 cj_batch_stats *stats);
+void cj_prepared_free(cj_prepared *batch);
+
 /* Hash join of two INT32 key arrays already in device memory, for callers
  * that must not have a library allocate device memory (an engine whose
  * allocator or fixed budget owns all of the GPU's memory). No counterpart

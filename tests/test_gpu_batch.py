@@ -85,3 +85,50 @@ def test_batch_resident_inputs(gpu_ctx):
     want = run_oracle(plan)
     for g in collect(res):
         assert_same(g, want)
+
+
+def _resident(plans, ctx):
+    out, tables = [], []
+    for p in plans:
+        rp = Plan()
+        rp.nodes, rp.root = p.nodes, p.root
+        rp.inputs = [ResidentTable(ctx, t) for t in p.inputs]
+        tables.extend(rp.inputs)
+        out.append(rp)
+    return out, tables
+
+
+@pytest.mark.parametrize("flags", [0, 1])  # host results, device results
+def test_prepared_batch_replays(gpu_ctx, flags):
+    """A batch captured as one CUDA graph: three replays in a row, each
+    result equal to the oracle's (chain plans with nested-loop and hash
+    joins, INT64 keys, VARCHAR outputs, a many-to-many join)."""
+    from calamarijoins_b200 import PreparedBatch
+    rng = np.random.default_rng(14)
+    plans = [chain_plan(int(rng.integers(2, 5)), int(rng.integers(1000, 80000)), rng, max_build=40000,
+                        key_types=[I if rng.random() < 0.6 else L for _ in range(3)], varchar_frac=0.3)
+             for _ in range(12)]
+    plans.append(join2(3000, 30000, seed=7, unique_build=False, build_payload=(V,), probe_payload=(F,)))
+    plans.append(join2(40, 10000, seed=8))  # nested loop
+    want = [run_oracle(p) for p in plans]
+    rplans, tables = _resident(plans, gpu_ctx)
+    pb = PreparedBatch(rplans, gpu_ctx, flags)
+    try:
+        for rep in range(3):
+            res, st = pb.run()
+            assert st["syncs"] == 1
+            for i, r in enumerate(res):
+                got = oa.PagedResult.from_result(r)
+                r.free()
+                assert_same(got, want[i], f"replay {rep} plan {i}")
+    finally:
+        pb.close()
+        for t in tables:
+            t.free()
+
+
+def test_prepared_batch_needs_resident_inputs(gpu_ctx):
+    from calamarijoins_b200 import CJError, PreparedBatch
+    with pytest.raises(CJError) as e:
+        PreparedBatch([join2(100, 1000, seed=1)], gpu_ctx)
+    assert e.value.status == 6  # CJ_ERR_UNSUPPORTED
