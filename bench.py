@@ -481,6 +481,13 @@ def run_ours(args):
     reps = Replicas("nccl", device=f"cuda:{local}")
 
     ctx = cj.Context(local)
+    tuning = None
+    if not args.no_tune:
+        log("autotuning the hash build and probe")
+        t0 = time.perf_counter()
+        ctx.autotune()
+        tuning = {"classes": ctx.tuning(), "seconds": round(time.perf_counter() - t0, 2),
+                  "entry": "(log2 slots per radix partition, radix-pass CTAs/SM, probe CTAs/SM) per size class"}
     log("generating workload")
     plan = gen_workload(True, args.scale)
     log("uploading resident tables")
@@ -601,7 +608,8 @@ def run_ours(args):
                            "inputs": "paged columns resident in HBM (device-resident cj_table)",
                            "l2": "inputs larger than L2 (1.1 GB of pages); no flush",
                            "parallelism": f"replicas x{world}",
-                           "output_rows": st.exec["output_rows"], "output_pages": st.exec["output_pages"]},
+                           "output_rows": st.exec["output_rows"], "output_pages": st.exec["output_pages"],
+                           "tuning": tuning},
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                         "ms_per_step": e2e_s * 1000.0, "step_ms": e2e_steps},
                 "roofline": roof, "cpu_baseline": cpu, "gpu_launches": launches, "parity": parity,
@@ -852,6 +860,7 @@ def main(argv=None):
     ap.add_argument("--scale", type=float, default=1.0, help="row-count scale of the workload")
     ap.add_argument("--cpu-scale", type=float, default=1.0, help="scale of the CPU-baseline sample")
     ap.add_argument("--no-parity", action="store_true", help="skip the oracle fingerprint check")
+    ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (kernel defaults)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-worker", type=int, default=0, help=argparse.SUPPRESS)
     ap.add_argument("--workload", choices=["c2", "c1", "c2s", "c2h", "c3", "c4", "c5"], default="c2",

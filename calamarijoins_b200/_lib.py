@@ -35,6 +35,7 @@ CJ_OPT_CTAS_PER_SM = 5
 CJ_OPT_DENSE_KEYS = 6
 CJ_OPT_BUFFER_CACHE_BYTES = 7
 CJ_OPT_FAIL_ALLOC_AT = 8
+CJ_TUNE_QUICK = 1
 
 
 class ColumnDesc(C.Structure):
@@ -146,6 +147,11 @@ _SIGS = {
     "cj_result_column_device": (C.c_int, [_P, C.c_uint64, C.POINTER(_P)]),
     "cj_result_copy_column": (C.c_int, [_P, C.c_uint64, _P, C.c_uint64]),
     "cj_result_free": (None, [_P]),
+    "cj_autotune": (C.c_int, [_P, C.c_char_p, C.c_uint32]),
+    "cj_tuning_load": (C.c_int, [_P, C.c_char_p]),
+    "cj_tuning_check_file": (C.c_int, [C.c_char_p]),
+    "cj_tuning_entry": (C.c_int, [_P, C.c_uint32, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                                  C.POINTER(C.c_int32)]),
     "cj_batch_prepare": (C.c_int, [_P, _P, C.c_uint64, C.c_uint32, C.POINTER(_P)]),
     "cj_batch_run": (C.c_int, [_P, C.POINTER(_P), C.POINTER(BatchStatsC)]),
     "cj_prepared_free": (None, [_P]),

@@ -314,9 +314,7 @@ void BatchExecutor::run_level(int lvl) {
         BuildPlan bp;
         bp.num_rows = (uint32_t)w.B->rows;
         bp.log2_slots = std::max(11, ceil_log2(w.B->rows));
-        int spp = 11;
-        if (ctx.opt.slots_per_partition > 0) spp = ceil_log2((uint64_t)ctx.opt.slots_per_partition);
-        spp = std::min(spp, bp.log2_slots);
+        const int spp = std::min(build_log2_spp(ctx, w.B->rows), bp.log2_slots);
         bp.log2_parts = std::min(bp.log2_slots - spp, 12);
         if (bp.log2_slots - bp.log2_parts > 14) fail(CJ_ERR_LIMIT, "build side too large for one radix pass");
         w.log2_slots = bp.log2_slots;
@@ -325,7 +323,7 @@ void BatchExecutor::run_level(int lvl) {
         w.dir = ctx.alloc(build_dir_bytes(bp.log2_slots, kb));
         w.tuples = ctx.alloc(w.B->rows * build_tuple_bytes(kb));
         w.part_buf = ctx.alloc(w.B->rows * build_tuple_bytes(kb));
-        BuildGeometry g = build_geometry(L, bp);
+        BuildGeometry g = build_geometry(build_launch(ctx, w.B->rows), bp);
         BuildTask t{};
         t.key = bv;
         t.n = bp.num_rows;

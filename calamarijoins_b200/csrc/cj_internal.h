@@ -153,6 +153,29 @@ struct Launch {
     int num_sms;
     int block_threads; /* 0 = kernel default */
     unsigned int *dev_errors;
+    int ctas_per_sm = 0;      /* persistent probe grids: CTAs per SM (0 = as many as fit) */
+    int part_ctas_per_sm = 0; /* radix histogram / scatter passes: CTAs per SM (0 = 4)     */
+};
+
+/* Tuned launch parameters per size class of a relation's row count (the
+ * autotuner's table). Classes split at 2^12, 2^15, 2^18, 2^21 and 2^24
+ * rows. A zero entry means "the default". */
+constexpr int kTuneClasses = 6;
+inline int tune_class(uint64_t rows) {
+    int c = 0;
+    for (int t : {12, 15, 18, 21, 24})
+        if (rows >= (1ull << t)) ++c;
+    return c;
+}
+struct TuneEntry {
+    int log2_spp = 0;    /* hash directory slots per radix partition (log2) */
+    int part_ctas = 0;   /* radix passes: CTAs per SM                        */
+    int probe_ctas = 0;  /* hash probe: CTAs per SM                          */
+};
+struct Tuning {
+    bool loaded = false;
+    TuneEntry cls[kTuneClasses];
+    const TuneEntry &for_rows(uint64_t rows) const { return cls[tune_class(rows)]; }
 };
 
 /* Scan */

@@ -375,17 +375,16 @@ Relation Executor::exec_join(uint64_t node_idx, int depth, bool is_root, cj_resu
              * counters of one partition fit shared memory); the partition
              * bits are spread over one radix pass, or two above 12 bits
              * (build sides of more than 2^23 rows) */
-            int log2_spp = 11;
-            if (ctx.opt.slots_per_partition > 0) log2_spp = ceil_log2((uint64_t)ctx.opt.slots_per_partition);
-            log2_spp = std::min(std::min(log2_spp, 14), bp.log2_slots);
+            const int log2_spp = std::min(std::min(build_log2_spp(ctx, B.rows), 14), bp.log2_slots);
             bp.log2_parts = bp.log2_slots - log2_spp;
             log2_slots = bp.log2_slots;
             const int kb = bk.type == CJ_INT32 ? 4 : 8;
+            const Launch LB = build_launch(ctx, B.rows);
             dir = ctx.alloc(build_dir_bytes(bp.log2_slots, kb));
             tuples = ctx.alloc(B.rows * build_tuple_bytes(kb));
-            DevPtr tmp = ctx.alloc(build_temp_bytes(L, bp, kb));
+            DevPtr tmp = ctx.alloc(build_temp_bytes(LB, bp, kb));
             KScope k(*this, "build");
-            ck(launch_build(L, bp, bv, ctx.d_bloom, dir->as<uint64_t>(), tuples->ptr, tmp->ptr), "build");
+            ck(launch_build(LB, bp, bv, ctx.d_bloom, dir->as<uint64_t>(), tuples->ptr, tmp->ptr), "build");
         };
         if (nl) {
             stats.num_nested_loop_joins++;
@@ -455,8 +454,9 @@ Relation Executor::exec_join(uint64_t node_idx, int depth, bool is_root, cj_resu
                        "probe_array");
                 } else {
                     KScope k(*this, "probe_hash");
-                    ck(launch_probe_tiles_hash(L, pv, (uint32_t)P.rows, bk.type, dir->as<uint64_t>(), tuples->ptr,
-                                               log2_slots, ctx.d_bloom, mo, sched->ptr),
+                    ck(launch_probe_tiles_hash(probe_launch(ctx, P.rows), pv, (uint32_t)P.rows, bk.type,
+                                               dir->as<uint64_t>(), tuples->ptr, log2_slots, ctx.d_bloom, mo,
+                                               sched->ptr),
                        "probe");
                 }
             }

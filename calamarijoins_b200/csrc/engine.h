@@ -93,6 +93,7 @@ struct Context {
     cudaEvent_t staging_ev[2] = {nullptr, nullptr};
     size_t staging_bytes = 16u << 20;
     Options opt;
+    Tuning tuning; /* autotuned launch parameters (cj_autotune / CJ_TUNING_FILE) */
 
     /* pinned pool: size class -> free blocks */
     std::multimap<size_t, void *> pinned_free;
@@ -160,6 +161,9 @@ void upload_pages(Context &ctx, const cj_column_desc &cd, ColumnPages &out, uint
 /* Creates a context on `device`; with `shared_pool` non-null the context
  * allocates from that pool instead of creating its own. Throws Error. */
 Context *create_context(int device, cudaMemPool_t shared_pool);
+/* Reads a tuning file written by cj_autotune; num_sms > 0 must match the
+ * file's SM count. Throws Error. */
+Tuning load_tuning_file(const char *path, int num_sms);
 /* Creates a device memory pool that keeps freed memory for reuse. */
 cudaMemPool_t create_pool(int device);
 

@@ -18,6 +18,27 @@ inline int ceil_log2(uint64_t x) {
     return l;
 }
 
+/* Hash directory slots per radix partition (log2) for a build of `rows`
+ * rows: the option when set, else the autotuner's entry, else 2^11. */
+inline int build_log2_spp(const Context &ctx, uint64_t rows) {
+    if (ctx.opt.slots_per_partition > 0) return ceil_log2((uint64_t)ctx.opt.slots_per_partition);
+    const int t = ctx.tuning.for_rows(rows).log2_spp;
+    return t > 0 ? t : 11;
+}
+/* Launch parameters of a hash build / a hash probe over `rows` rows: the
+ * CJ_OPT_CTAS_PER_SM option when set, else the autotuner's entry, else the
+ * kernels' defaults. */
+inline Launch build_launch(const Context &ctx, uint64_t rows) {
+    Launch L = ctx.launch();
+    L.part_ctas_per_sm = ctx.opt.ctas_per_sm > 0 ? (int)ctx.opt.ctas_per_sm : ctx.tuning.for_rows(rows).part_ctas;
+    return L;
+}
+inline Launch probe_launch(const Context &ctx, uint64_t rows) {
+    Launch L = ctx.launch();
+    L.ctas_per_sm = ctx.opt.ctas_per_sm > 0 ? (int)ctx.opt.ctas_per_sm : ctx.tuning.for_rows(rows).probe_ctas;
+    return L;
+}
+
 /* A base column decoded into dense device arrays. */
 struct Decoded {
     int32_t type = CJ_INT32;

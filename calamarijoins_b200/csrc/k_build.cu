@@ -378,7 +378,7 @@ PartGeom geometry(const Launch &L, const BuildPlan &bp) {
     g.log2_parts = first_pass_bits(bp.log2_parts);
     g.log2_slots = bp.log2_slots;
     uint64_t chunks = ((uint64_t)bp.num_rows + kPartMinRows - 1) / kPartMinRows;
-    uint64_t grid = (uint64_t)L.num_sms * kPartCtasPerSm;
+    uint64_t grid = (uint64_t)L.num_sms * (L.part_ctas_per_sm > 0 ? L.part_ctas_per_sm : kPartCtasPerSm);
     if (chunks < grid) grid = chunks;
     if (grid == 0) grid = 1;
     g.grid = (uint32_t)grid;

@@ -497,7 +497,8 @@ cudaError_t run_tiles(const Launch &L, const ColView &pkey, uint32_t n, const M 
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_probe_tiles<M>, kProbeThreads, 0);
         return n < 1 ? 1 : n;
     }();
-    uint64_t grid = (uint64_t)L.num_sms * per_sm;
+    const int ctas = L.ctas_per_sm > 0 && L.ctas_per_sm < per_sm ? L.ctas_per_sm : per_sm;
+    uint64_t grid = (uint64_t)L.num_sms * ctas;
     if (grid > ts.num_tiles) grid = ts.num_tiles;
     k_probe_tiles<M><<<(unsigned)grid, kProbeThreads, 0, L.stream>>>(pkey, n, m, out, ts);
     count_launches(1);

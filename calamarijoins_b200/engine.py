@@ -81,6 +81,25 @@ class Context:
     def profile_reset(self):
         check(lib().cj_profile_reset(self.handle))
 
+    def autotune(self, path: Optional[str] = None, quick: bool = False):
+        """Times the hash build and probe per size class and keeps the
+        fastest launch parameters (cj_autotune); writes them to `path`."""
+        check(lib().cj_autotune(self.handle, os.fsencode(path) if path else None,
+                                _lib.CJ_TUNE_QUICK if quick else 0))
+
+    def load_tuning(self, path: str):
+        check(lib().cj_tuning_load(self.handle, os.fsencode(path)))
+
+    def tuning(self) -> list:
+        """Per size class: (log2 slots per partition, radix-pass CTAs per SM,
+        probe CTAs per SM); zeros mean untuned defaults."""
+        out = []
+        for c in range(6):
+            a, b, d = C.c_int32(), C.c_int32(), C.c_int32()
+            check(lib().cj_tuning_entry(self.handle, c, C.byref(a), C.byref(b), C.byref(d)))
+            out.append((a.value, b.value, d.value))
+        return out
+
 
 class ResidentTable:
     """A table whose pages live in device memory (cj_table)."""

@@ -190,13 +190,17 @@ typedef enum cj_option {
                                          kernel is used (reference: 8,
                                          src/execute.cpp:236-238); default 64 */
     CJ_OPT_SLOTS_PER_PARTITION = 1,   /* hash directory slots per radix
-                                         partition (power of two); 0 = auto */
+                                         partition (power of two, at most
+                                         16384); 0 = the autotuner's
+                                         choice, else 2048                  */
     CJ_OPT_PROFILE_KERNELS = 2,       /* 1 = time every kernel with events   */
     CJ_OPT_BLOCK_THREADS = 3,         /* threads per CTA of streaming kernels;
                                          0 = auto                           */
     CJ_OPT_VARCHAR_TILE_ROWS = 4,     /* rows per VARCHAR page-packing tile  */
-    CJ_OPT_CTAS_PER_SM = 5,           /* resident CTAs per SM for persistent
-                                         grids; 0 = auto                    */
+    CJ_OPT_CTAS_PER_SM = 5,           /* CTAs per SM of the hash probe's
+                                         persistent grid and of the radix
+                                         passes; 0 = the autotuner's choice,
+                                         else the kernels' defaults         */
     CJ_OPT_DENSE_KEYS = 6,            /* a build side whose non-NULL keys are
                                          unique and span at most this many
                                          times its row count (and 2^28
@@ -220,6 +224,27 @@ typedef enum cj_option {
 } cj_option;
 int cj_context_set_option(cj_context *ctx, int32_t option, int64_t value);
 int cj_context_get_option(const cj_context *ctx, int32_t option, int64_t *value);
+
+/* Autotuner (no reference counterpart; the reference sizes its radix
+ * partitions from the cache share per thread, include/join_execution/
+ * hashtable.h:172-188): times the unchained hash table's build and probe on
+ * synthetic keys of each size class (row counts split at 2^12, 2^15, 2^18,
+ * 2^21 and 2^24) and keeps, per class, the fastest directory slots per
+ * radix partition, radix-pass CTAs per SM and probe CTAs per SM. The table
+ * goes into the context and, when `path` is not NULL, into that file.
+ * Options CJ_OPT_SLOTS_PER_PARTITION / CJ_OPT_CTAS_PER_SM override it;
+ * results never depend on it. A context created while the environment
+ * variable CJ_TUNING_FILE names a file loads that file (and fails to be
+ * created if the file is malformed or was made for another GPU). */
+#define CJ_TUNE_QUICK 1u /* time only the four smaller classes (the larger
+                            ones take the largest timed class's entry)    */
+int cj_autotune(cj_context *ctx, const char *path, uint32_t flags);
+int cj_tuning_load(cj_context *ctx, const char *path);
+/* Checks a tuning file's format without a GPU. */
+int cj_tuning_check_file(const char *path);
+/* The context's entry for size class `size_class` (0 = untuned default). */
+int cj_tuning_entry(const cj_context *ctx, uint32_t size_class, int32_t *log2_spp,
+                    int32_t *part_ctas, int32_t *probe_ctas);
 
 /* Per-kernel profile (enabled by CJ_OPT_PROFILE_KERNELS): `index`-th kernel
  * name seen since the last reset, its launch count and total device time. */
