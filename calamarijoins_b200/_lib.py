@@ -65,6 +65,16 @@ class PlanDesc(C.Structure):
                 ("resident_inputs", C.POINTER(C.c_void_p)), ("root", C.c_uint64)]
 
 
+class PredNodeC(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("op", C.c_int32), ("column", C.c_uint64), ("left", C.c_uint64),
+                ("right", C.c_uint64), ("literal_type", C.c_int32), ("reserved", C.c_uint32), ("i64", C.c_int64),
+                ("f64", C.c_double), ("str", C.c_char_p), ("str_len", C.c_uint64)]
+
+
+class PredicateC(C.Structure):
+    _fields_ = [("num_nodes", C.c_uint64), ("nodes", C.POINTER(PredNodeC)), ("root", C.c_uint64)]
+
+
 class TimingStatsC(C.Structure):
     _fields_ = [(n, C.c_int64) for n in (
         "hashtable_build_ms", "hash_join_probe_ms", "nested_loop_join_ms", "materialize_ms",
@@ -124,6 +134,9 @@ _SIGS = {
                                        C.POINTER(C.c_uint64), C.POINTER(_P), C.POINTER(_P)]),
     "cj_table_column_pages": (C.c_int, [_P, C.c_uint64, C.POINTER(_P), C.POINTER(C.c_uint64)]),
     "cj_table_free": (None, [_P]),
+    "cj_table_copy_column": (C.c_int, [_P, C.c_uint64, _P, C.c_uint64]),
+    "cj_table_filter": (C.c_int, [_P, _P, C.POINTER(PredicateC), C.c_uint64, C.POINTER(C.c_uint64), C.POINTER(_P),
+                                  C.POINTER(C.c_uint64)]),
     "cj_cache_read_meta": (C.c_int, [C.c_char_p, C.POINTER(CacheMetaC)]),
     "cj_table_write_cache": (C.c_int, [C.POINTER(TableDesc), C.c_char_p]),
     "cj_table_load_cache": (C.c_int, [_P, C.c_char_p, C.POINTER(_P)]),

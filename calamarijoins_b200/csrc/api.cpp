@@ -200,6 +200,20 @@ int cj_table_column_pages(const cj_table *table, uint64_t column, const void **d
     return CJ_OK;
 }
 
+int cj_table_copy_column(const cj_table *table, uint64_t column, void *dst, uint64_t dst_bytes) {
+    if (!table || column >= table->cols.size()) return set_error(CJ_ERR_INVALID_ARGUMENT, "bad column");
+    const uint64_t bytes = table->cols[column].num_pages * CJ_PAGE_SIZE;
+    if (bytes && !dst) return set_error(CJ_ERR_INVALID_ARGUMENT, "null destination");
+    if (dst_bytes < bytes) return set_error(CJ_ERR_INVALID_ARGUMENT, "destination too small");
+    if (!bytes) return CJ_OK;
+    API_BEGIN
+    set_device(table->ctx);
+    cj::check_cuda(cudaMemcpyAsync(dst, table->cols[column].dev, bytes, cudaMemcpyDeviceToHost, table->ctx->stream),
+                   "download");
+    cj::check_cuda(cudaStreamSynchronize(table->ctx->stream), "download");
+    API_END
+}
+
 void cj_table_free(cj_table *table) {
     if (!table) return;
     set_device(table->ctx);

@@ -139,6 +139,32 @@ class ResidentTable:
         check(lib().cj_table_load_cache(ctx.handle, os.fsencode(path), C.byref(h)))
         return cls.from_handle(ctx, h.value, meta["num_rows"], meta["types"])
 
+    def filter(self, predicate=None, columns=None) -> "ResidentTable":
+        """Rows for which `predicate` (a predicate.Statement, or None for
+        all rows) holds, projected to `columns` (default: all), as a new
+        resident table (cj_table_filter): the predicate is evaluated and the
+        pages written on the GPU."""
+        from .predicate import PredicateDesc
+        cols = list(range(len(self.types))) if columns is None else [int(c) for c in columns]
+        arr = (C.c_uint64 * max(len(cols), 1))(*cols)
+        pd = PredicateDesc(predicate) if predicate is not None else None
+        h, n = C.c_void_p(), C.c_uint64()
+        check(lib().cj_table_filter(self.ctx.handle, self.handle, C.byref(pd.desc) if pd else None, len(cols), arr,
+                                    C.byref(h), C.byref(n)))
+        return ResidentTable.from_handle(self.ctx, h.value, n.value, [self.types[c] for c in cols])
+
+    def download(self) -> ColumnarTable:
+        """The table's pages copied back to the host."""
+        cols = []
+        for c, t in enumerate(self.types):
+            p, np_ = C.c_void_p(), C.c_uint64()
+            check(lib().cj_table_column_pages(self.handle, c, C.byref(p), C.byref(np_)))
+            host = np.zeros((np_.value, PAGE_SIZE), np.uint8)
+            if np_.value:
+                check(lib().cj_table_copy_column(self.handle, c, host.ctypes.data, host.nbytes))
+            cols.append(Column(DataType(t), host))
+        return ColumnarTable(self.num_rows, cols)
+
     def free(self):
         if getattr(self, "handle", None):
             if getattr(self, "_owned", True):

@@ -282,7 +282,84 @@ int cj_table_from_device(cj_context *ctx, uint64_t num_rows,
 int cj_table_column_pages(const cj_table *table, uint64_t column,
                           const void **device_pages, uint64_t *num_pages);
 
+/* Copies a resident column's pages to caller memory (dst_bytes >=
+ * pages * 8192). */
+int cj_table_copy_column(const cj_table *table, uint64_t column, void *dst,
+                         uint64_t dst_bytes);
+
 void cj_table_free(cj_table *table);
+
+/* Scan-side filters on resident tables. A predicate is a tree of nodes in
+ * the form of the reference's Statement (include/data_model/statement.h):
+ * comparisons of one column with a literal (Comparison, statement.h:54-64)
+ * combined by AND / OR / NOT (LogicalOperation). Evaluation follows the
+ * reference's column-wise Comparison::eval / LogicalOperation::eval
+ * (src/statement.cpp:47-241, include/data_model/inner_column.h):
+ *   - a comparison is false on a NULL row; IS_NULL / IS_NOT_NULL test the
+ *     validity bit; NOT flips the bit of every row (NOT (x < 5) holds on the
+ *     rows where x is NULL);
+ *   - INT32 columns compare with the INT64 literal cast to int32 (its low 32
+ *     bits), INT64 columns with the INT64 literal, FP64 columns with the
+ *     FP64 literal (an INT64 literal given for an FP64 column is converted);
+ *   - VARCHAR columns compare bytewise, a shorter prefix first, like
+ *     std::string_view; LIKE / NOT LIKE match the whole string, '%' any run
+ *     of characters and '_' one character (a UTF-8 code point), neither of
+ *     them a newline (the RE2 pattern that Comparison::like_match builds,
+ *     statement.h:119-158); NOT LIKE is false on NULL rows.
+ * Comparisons of mismatched types (a VARCHAR literal for a numeric column, a
+ * numeric literal for VARCHAR, LIKE on a numeric column) are
+ * CJ_ERR_INVALID_PLAN. */
+typedef enum cj_pred_kind {
+    CJ_PRED_CMP = 0,
+    CJ_PRED_AND = 1,
+    CJ_PRED_OR = 2,
+    CJ_PRED_NOT = 3
+} cj_pred_kind;
+
+/* Values equal Comparison::Op's enumerators (statement.h:57). */
+typedef enum cj_cmp_op {
+    CJ_CMP_EQ = 0,
+    CJ_CMP_NEQ = 1,
+    CJ_CMP_LT = 2,
+    CJ_CMP_GT = 3,
+    CJ_CMP_LEQ = 4,
+    CJ_CMP_GEQ = 5,
+    CJ_CMP_LIKE = 6,
+    CJ_CMP_NOT_LIKE = 7,
+    CJ_CMP_IS_NULL = 8,
+    CJ_CMP_IS_NOT_NULL = 9
+} cj_cmp_op;
+
+typedef struct cj_pred_node {
+    int32_t kind;           /* cj_pred_kind                                  */
+    int32_t op;             /* cj_cmp_op (CJ_PRED_CMP)                       */
+    uint64_t column;        /* column of the input table (CJ_PRED_CMP)        */
+    uint64_t left, right;   /* children (AND / OR: both; NOT: left)           */
+    int32_t literal_type;   /* CJ_INT64, CJ_FP64 or CJ_VARCHAR (Literal)      */
+    uint32_t reserved;
+    int64_t i64;
+    double f64;
+    const char *str;        /* VARCHAR literal bytes (str_len of them)        */
+    uint64_t str_len;
+} cj_pred_node;
+
+typedef struct cj_predicate {
+    uint64_t num_nodes;
+    const cj_pred_node *nodes;
+    uint64_t root;
+} cj_predicate;
+
+/* Rows of the resident table `in` for which `pred` holds (all rows when
+ * pred is NULL), projected to `columns` (num_columns indices into in's
+ * columns, in that order), as a new resident table whose pages are written
+ * as ColumnInserter<T> writes pages (include/data_model/plan.h:187-366);
+ * row order is kept. `*num_rows` (may be NULL) receives its row count.
+ * The GPU form of the loader's filter pass before execute()
+ * (src/build_table.cpp:201-367). */
+int cj_table_filter(cj_context *ctx, const cj_table *in,
+                    const cj_predicate *pred, uint64_t num_columns,
+                    const uint64_t *columns, cj_table **out,
+                    uint64_t *num_rows);
 
 /* The reference's `.tbl` table cache (written by DumpTable::dump,
  * include/data_access/table.h:136-221; read by Table::from_cache,

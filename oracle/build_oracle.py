@@ -92,6 +92,30 @@ def build_reference(threads=DEFAULT_THREADS, force: bool = False) -> list[str]:
     return built
 
 
+def build_reference_filter(force: bool = False) -> str | None:
+    """oracle/_ref/libcj_ref_filter.so: the reference's scan-filter
+    evaluation (src/statement.cpp with include/data_model/inner_column.h)
+    behind oracle/ref_filter_bridge.cpp; RE2 is the shim's subset matcher."""
+    ref = reference_dir()
+    if ref is None:
+        return None
+    try:
+        import torch  # only for the bundled header-only fmt
+        fmt_inc = os.path.join(os.path.dirname(torch.__file__), "include")
+    except Exception:  # pragma: no cover
+        return None
+    outdir = os.path.join(HERE, "_ref")
+    os.makedirs(outdir, exist_ok=True)
+    shim = os.path.join(HERE, "ref_shim")
+    sources = [os.path.join(ref, "src", "statement.cpp"), os.path.join(HERE, "ref_filter_bridge.cpp")]
+    out = os.path.join(outdir, "libcj_ref_filter.so")
+    if force or not _newer(out, sources + [os.path.join(shim, "re2", "re2.h")]):
+        _run(["g++", "-std=c++17", "-O2", "-fpermissive", "-w", "-fno-gnu-unique", "-Wl,-Bsymbolic",
+              "-DFMT_HEADER_ONLY", "-I", shim, "-I", os.path.join(ref, "include"), "-I", fmt_inc,
+              "-shared", "-fPIC", *sources, "-o", out, "-lpthread"])
+    return out
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--threads", default=",".join(str(t) for t in DEFAULT_THREADS))
@@ -100,6 +124,7 @@ def main(argv=None) -> int:
     print(build_oracle(a.force))
     for p in build_reference(tuple(int(x) for x in a.threads.split(",")), a.force):
         print(p)
+    print(build_reference_filter(a.force))
     return 0
 
 

@@ -1294,3 +1294,184 @@ int cjo_paged_table_fingerprint(uint64_t ncols, const int32_t *types, uint64_t r
     *fp = s + rows;
     return CJ_OK;
 }
+
+
+/* ------------------------------------------------------------------------ */
+/* Scan-side filters (the loader's predicate pass, src/build_table.cpp:      */
+/* 318-366; src/statement.cpp:47-241; include/data_model/inner_column.h)     */
+/* ------------------------------------------------------------------------ */
+
+static uint64_t cp_len_o(uint8_t b) {
+    if (b < 0x80) return 1;
+    if ((b & 0xE0) == 0xC0) return 2;
+    if ((b & 0xF0) == 0xE0) return 3;
+    if ((b & 0xF8) == 0xF0) return 4;
+    return 1;
+}
+
+/* Exact matcher by dynamic programming over (text byte, pattern byte):
+ * ok[i][j] = pattern[j..] matches text[i..]. The translated RE2 pattern
+ * (statement.h:125-147) is '%' -> ".*", '_' -> ".", every other byte
+ * literal; RE2's '.' is one UTF-8 code point other than a newline. */
+int cjo_like(const char *s, uint64_t n, const char *pat, uint64_t m) {
+    const uint8_t *t = (const uint8_t *)s;
+    const uint8_t *p = (const uint8_t *)pat;
+    uint8_t *ok = (uint8_t *)calloc((n + 1) * (m + 1), 1);
+    if (!ok) return -1;
+#define OK(i, j) ok[(uint64_t)(i) * (m + 1) + (j)]
+    OK(n, m) = 1;
+    for (uint64_t ii = n + 1; ii-- > 0;) {
+        for (uint64_t jj = m + 1; jj-- > 0;) {
+            if (jj == m) { OK(ii, jj) = ii == n; continue; }
+            uint8_t r = 0;
+            if (p[jj] == '%') {
+                r = OK(ii, jj + 1);
+                if (!r && ii < n && t[ii] != '\n') {
+                    uint64_t nx = ii + cp_len_o(t[ii]);
+                    r = nx <= n && OK(nx, jj);
+                }
+            } else if (p[jj] == '_') {
+                if (ii < n && t[ii] != '\n') {
+                    uint64_t nx = ii + cp_len_o(t[ii]);
+                    r = nx <= n && OK(nx, jj + 1);
+                }
+            } else {
+                r = ii < n && t[ii] == p[jj] && OK(ii + 1, jj + 1);
+            }
+            OK(ii, jj) = r;
+        }
+    }
+    int res = OK(0, 0);
+#undef OK
+    free(ok);
+    return res;
+}
+
+static int cmp_i(int op, int64_t a, int64_t b) {
+    switch (op) {
+    case CJ_CMP_EQ: return a == b;
+    case CJ_CMP_NEQ: return a != b;
+    case CJ_CMP_LT: return a < b;
+    case CJ_CMP_GT: return a > b;
+    case CJ_CMP_LEQ: return a <= b;
+    case CJ_CMP_GEQ: return a >= b;
+    default: return 0;
+    }
+}
+
+static int cmp_f(int op, double a, double b) {
+    switch (op) {
+    case CJ_CMP_EQ: return a == b;
+    case CJ_CMP_NEQ: return a != b;
+    case CJ_CMP_LT: return a < b;
+    case CJ_CMP_GT: return a > b;
+    case CJ_CMP_LEQ: return a <= b;
+    case CJ_CMP_GEQ: return a >= b;
+    default: return 0;
+    }
+}
+
+/* std::string_view ordering: bytes as unsigned char, then length. */
+static int str_cmp3(const char *a, uint64_t la, const char *b, uint64_t lb) {
+    uint64_t m = la < lb ? la : lb;
+    int c = m ? memcmp(a, b, m) : 0;
+    if (c) return c < 0 ? -1 : 1;
+    return la < lb ? -1 : (la > lb ? 1 : 0);
+}
+
+/* One row of one comparison, as InnerColumn<T>::equal / less / ... /
+ * like / not_like write it: false on a NULL row (inner_column.h:240-313,
+ * 387-588); IS_NULL / IS_NOT_NULL read the bitmap (statement.cpp:49-53). */
+static int eval_cmp_row(const cj_pred_node *nd, const cjo_column *c, uint64_t r) {
+    int valid = c->valid[r] != 0;
+    if (nd->op == CJ_CMP_IS_NULL) return !valid;
+    if (nd->op == CJ_CMP_IS_NOT_NULL) return valid;
+    if (!valid) return 0;
+    switch (c->type) {
+    case CJ_INT32: /* static_cast<int32_t>(std::get<int64_t>(value)), statement.cpp:54 */
+        return cmp_i(nd->op, c->i32[r], (int32_t)nd->i64);
+    case CJ_INT64: return cmp_i(nd->op, c->i64[r], nd->i64);
+    case CJ_FP64: return cmp_f(nd->op, c->f64[r], nd->literal_type == CJ_INT64 ? (double)nd->i64 : nd->f64);
+    default: {
+        const char *sv = c->chars + c->str_off[r];
+        uint64_t len = c->str_off[r + 1] - c->str_off[r];
+        if (nd->op == CJ_CMP_LIKE) return cjo_like(sv, len, nd->str, nd->str_len) == 1;
+        if (nd->op == CJ_CMP_NOT_LIKE) return cjo_like(sv, len, nd->str, nd->str_len) == 0;
+        int d = str_cmp3(sv, len, nd->str, nd->str_len);
+        return cmp_i(nd->op, d, 0);
+    }
+    }
+}
+
+/* LogicalOperation: AND / OR of the children's bitmaps, NOT flips every
+ * row's bit (statement.cpp:222-241). */
+static int eval_pred_row(const cj_predicate *pr, uint64_t node, const cjo_column *cols, uint64_t r, int depth) {
+    const cj_pred_node *nd = &pr->nodes[node];
+    if (depth > (int)pr->num_nodes) return 0;
+    switch (nd->kind) {
+    case CJ_PRED_CMP: return eval_cmp_row(nd, &cols[nd->column], r);
+    case CJ_PRED_AND:
+        return eval_pred_row(pr, nd->left, cols, r, depth + 1) & eval_pred_row(pr, nd->right, cols, r, depth + 1);
+    case CJ_PRED_OR:
+        return eval_pred_row(pr, nd->left, cols, r, depth + 1) | eval_pred_row(pr, nd->right, cols, r, depth + 1);
+    default: return !eval_pred_row(pr, nd->left, cols, r, depth + 1);
+    }
+}
+
+int cjo_filter(const cj_table_desc *table, const cj_predicate *pred, uint64_t ncols, const uint64_t *cols,
+               cjo_result **out, uint8_t *selected) {
+    *out = NULL;
+    uint64_t nc = table->num_columns, rows = table->num_rows;
+    cjo_column *dec = (cjo_column *)xcalloc(nc ? nc : 1, sizeof(cjo_column));
+    if (!dec) return CJ_ERR_OUT_OF_MEMORY;
+    int rc = CJ_OK;
+    for (uint64_t c = 0; c < nc && rc == CJ_OK; ++c) {
+        const cj_column_desc *cd = &table->columns[c];
+        rc = cjo_decode_column(cd->type, cd->pages, cd->num_pages, rows, &dec[c]);
+    }
+    uint32_t *sel = rc == CJ_OK ? (uint32_t *)xcalloc(rows ? rows : 1, 4) : NULL;
+    uint64_t n = 0;
+    if (rc == CJ_OK && !sel) rc = CJ_ERR_OUT_OF_MEMORY;
+    for (uint64_t r = 0; rc == CJ_OK && r < rows; ++r) {
+        int keep = pred ? eval_pred_row(pred, pred->root, dec, r, 0) : 1;
+        if (selected) selected[r] = (uint8_t)keep;
+        if (keep) sel[n++] = (uint32_t)r;
+    }
+    cjo_result *res = rc == CJ_OK ? new_result(ncols) : NULL;
+    if (rc == CJ_OK && !res) rc = CJ_ERR_OUT_OF_MEMORY;
+    if (res) res->num_rows = n;
+    for (uint64_t k = 0; rc == CJ_OK && k < ncols; ++k) {
+        const cjo_column *c = &dec[cols[k]];
+        res->types[k] = c->type;
+        inserter *in = (inserter *)malloc(sizeof(inserter));
+        if (!in) { rc = CJ_ERR_OUT_OF_MEMORY; break; }
+        ins_init(in, c->type, &res->cols[k]);
+        for (uint64_t i = 0; i < n && !in->oom; ++i) {
+            uint64_t r = sel[i];
+            if (!c->valid[r]) {
+                if (c->type == CJ_VARCHAR) ins_insert_null_varchar(in);
+                else ins_insert_null_fixed(in);
+            } else if (c->type == CJ_INT32) {
+                ins_insert_fixed(in, &c->i32[r]);
+            } else if (c->type == CJ_INT64) {
+                ins_insert_fixed(in, &c->i64[r]);
+            } else if (c->type == CJ_FP64) {
+                ins_insert_fixed(in, &c->f64[r]);
+            } else {
+                ins_insert_varchar(in, c->chars + c->str_off[r], c->str_off[r + 1] - c->str_off[r]);
+            }
+        }
+        ins_finalize(in);
+        if (in->oom) rc = CJ_ERR_OUT_OF_MEMORY;
+        free(in);
+    }
+    for (uint64_t c = 0; c < nc; ++c) cjo_column_free(&dec[c]);
+    free(dec);
+    free(sel);
+    if (rc != CJ_OK) {
+        cjo_result_free(res);
+        return rc;
+    }
+    *out = res;
+    return CJ_OK;
+}

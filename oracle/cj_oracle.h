@@ -95,6 +95,19 @@ int cjo_paged_tables_equal(uint64_t ncols, const int32_t *types,
 
 /* Order-insensitive 64-bit fingerprint of a paged table's row multiset
  * (sum over rows of a row hash); used for full-size property checks. */
+/* Scan-side filter: rows of the host table for which `pred` holds (all
+ * rows when pred is NULL), projected to `cols`, encoded as ColumnInserter
+ * would, plus the selection as one byte per row in `selected` (may be
+ * NULL; table->num_rows bytes). Follows the reference's column-wise
+ * Comparison::eval / LogicalOperation::eval (src/statement.cpp:47-241,
+ * include/data_model/inner_column.h) row by row. */
+int cjo_filter(const cj_table_desc *table, const cj_predicate *pred, uint64_t ncols, const uint64_t *cols,
+               cjo_result **out, uint8_t *selected);
+
+/* Comparison::like_match's matching (statement.h:119-158): the whole
+ * string, '%' any run and '_' one UTF-8 code point, neither a newline. */
+int cjo_like(const char *s, uint64_t n, const char *pat, uint64_t m);
+
 int cjo_paged_table_fingerprint(uint64_t ncols, const int32_t *types,
                                 uint64_t rows, const uint64_t *num_pages,
                                 const void *const *pages, uint64_t *fp);

@@ -50,6 +50,8 @@ def oracle_lib() -> C.CDLL:
                                                  C.c_char_p, C.c_uint64]),
             "cjo_paged_table_fingerprint": (C.c_int, [C.c_uint64, _P, C.c_uint64, _P, _P,
                                                       C.POINTER(C.c_uint64)]),
+            "cjo_filter": (C.c_int, [_P, _P, C.c_uint64, _P, C.POINTER(_P), _P]),
+            "cjo_like": (C.c_int, [C.c_char_p, C.c_uint64, C.c_char_p, C.c_uint64]),
         }
         for n, (r, a) in sigs.items():
             f = getattr(h, n)
@@ -233,3 +235,94 @@ def encode(dtype: int, values, valid=None, offsets=None) -> np.ndarray:
         if rc:
             raise RuntimeError(f"encode failed {rc}")
     return out
+
+
+def _table_desc(table):
+    """A cj_table_desc over a ColumnarTable's host pages (kept alive by the
+    returned tuple)."""
+    from calamarijoins_b200._lib import ColumnDesc, TableDesc
+    keep = []
+    cols = (ColumnDesc * max(len(table.columns), 1))()
+    for c, col in enumerate(table.columns):
+        ptrs = col.page_pointers()
+        keep.append(ptrs)
+        cols[c].type = int(col.type)
+        cols[c].num_pages = col.num_pages
+        cols[c].pages = C.cast(ptrs, C.POINTER(C.c_void_p))
+    return TableDesc(table.num_rows, len(table.columns), cols), keep, cols
+
+
+def oracle_filter(table, predicate, columns=None):
+    """The oracle's scan filter (cjo_filter): (PagedResult of the selected
+    rows projected to `columns`, selected flags as a bool array)."""
+    from calamarijoins_b200.predicate import PredicateDesc
+    L = oracle_lib()
+    td, keep, cols_arr = _table_desc(table)
+    cols = list(range(len(table.columns))) if columns is None else list(columns)
+    ca = (C.c_uint64 * max(len(cols), 1))(*cols)
+    pd = PredicateDesc(predicate) if predicate is not None else None
+    sel = np.zeros(max(table.num_rows, 1), np.uint8)
+    h = C.c_void_p()
+    rc = L.cjo_filter(C.byref(td), C.byref(pd.desc) if pd else None, len(cols), ca, C.byref(h), sel.ctypes.data)
+    if rc != 0:
+        raise RuntimeError(f"oracle filter failed with status {rc}")
+    try:
+        res = _copy_paged(L.cjo_result_num_rows, L.cjo_result_num_columns, L.cjo_result_column, h.value)
+    finally:
+        L.cjo_result_free(h.value)
+    return res, sel[:table.num_rows].astype(bool)
+
+
+def oracle_like(s: bytes, pattern: bytes) -> bool:
+    return oracle_lib().cjo_like(s, len(s), pattern, len(pattern)) == 1
+
+
+REF_FILTER_SO = os.path.join(REF_DIR, "libcj_ref_filter.so")
+_ref_filter = None
+
+
+def ref_filter_available() -> bool:
+    return os.path.exists(REF_FILTER_SO)
+
+
+def ref_filter(table, predicate):
+    """The reference's own column-wise Statement::eval (src/statement.cpp,
+    compiled into oracle/_ref/libcj_ref_filter.so) on the table's rows:
+    the selected flags as a bool array."""
+    global _ref_filter
+    from calamarijoins_b200 import DataType, decode_column
+    from calamarijoins_b200._lib import PredicateC
+    from calamarijoins_b200.predicate import PredicateDesc
+    if _ref_filter is None:
+        _ref_filter = C.CDLL(REF_FILTER_SO)
+        _ref_filter.cjref_filter.restype = C.c_int
+        _ref_filter.cjref_filter.argtypes = [C.c_uint64, _P, C.c_uint64, _P, _P, _P, C.POINTER(PredicateC), _P]
+    n = table.num_rows
+    keep = []
+    nc = len(table.columns)
+    types = np.array([int(c.type) for c in table.columns], np.int32)
+    valid_p, values_p, offs_p = (C.c_void_p * max(nc, 1))(), (C.c_void_p * max(nc, 1))(), (C.c_void_p * max(nc, 1))()
+    for c, col in enumerate(table.columns):
+        vals, valid = decode_column(col)
+        if col.type == DataType.VARCHAR:
+            valid = np.array([v is not None for v in vals], np.uint8)
+            parts = [v or b"" for v in vals]
+            offs = np.zeros(n + 1, np.uint64)
+            offs[1:] = np.cumsum([len(x) for x in parts])
+            chars = np.frombuffer(b"".join(parts) or b"\0", np.uint8).copy()
+            keep += [offs, chars]
+            values_p[c], offs_p[c] = chars.ctypes.data, offs.ctypes.data
+        else:
+            vals = np.ascontiguousarray(vals)
+            keep.append(vals)
+            values_p[c] = vals.ctypes.data
+        valid = np.ascontiguousarray(valid, np.uint8)
+        keep.append(valid)
+        valid_p[c] = valid.ctypes.data
+    pd = PredicateDesc(predicate)
+    sel = np.zeros(max(n, 1), np.uint8)
+    rc = _ref_filter.cjref_filter(nc, types.ctypes.data, n, valid_p, values_p, offs_p, C.byref(pd.desc),
+                                  sel.ctypes.data)
+    if rc != 0:
+        raise RuntimeError("reference filter failed")
+    return sel[:n].astype(bool)
