@@ -81,6 +81,12 @@ CJ_DEV void put_key(const MatchOut &out, unsigned long long pos, int64_t key) {
 template <typename KB> struct HashMatcher {
     static constexpr bool kAtMostOne = false;
     static constexpr bool kInline = sizeof(KB) == 4;
+    /* A probe row whose slot holds more tuples than this is counted and
+     * written by its whole warp (warp_count / warp_write), 32 tuples a
+     * step, instead of by its own lane alone: a heavy-hitter key with
+     * 10^5 build rows costs its warp 10^5 / 32 steps, not one lane 10^5. */
+    static constexpr bool kHeavy = true;
+    static constexpr uint32_t kHeavyRun = 64;
     static constexpr int kMinBlocks = CJ_HASH_MIN_BLOCKS;
     static constexpr int kItems = kProbeItems;
     CJ_DEV HashMatcher resolved() const { return *this; }
@@ -122,8 +128,14 @@ template <typename KB> struct HashMatcher {
         }
         return en;
     }
-    CJ_DEV uint32_t count(const Shared &sh, int64_t key, uint32_t &first) const {
+    /* heavy: the slot is longer than kHeavyRun; the count is left to
+     * warp_count (0 returned). */
+    CJ_DEV uint32_t count(const Shared &sh, int64_t key, uint32_t &first, bool &heavy) const {
         const Entry en = entry(sh, key);
+        if (en.n > kHeavyRun) {
+            heavy = true;
+            return 0;
+        }
         uint32_t c = 0, j = 0;
         if (kInline && en.n) { /* tuple 0 came with the entry */
             if ((int64_t)en.key0 == key) {
@@ -155,6 +167,39 @@ template <typename KB> struct HashMatcher {
             ++pos;
         }
     }
+    /* Warp-wide (every lane calls it with the same key): the key's matches
+     * among its slot's tuples, each lane taking every 32nd tuple. */
+    CJ_DEV uint32_t warp_count(const Shared &sh, int64_t key) const {
+        const Entry en = entry(sh, key);
+        uint32_t c = 0;
+        for (uint32_t j = lane_id(); j < en.n; j += 32) c += (int64_t)ht.tuples[en.s + j].key == key ? 1u : 0u;
+        return warp_sum(c);
+    }
+    /* Warp-wide: the key's matches written from `pos` on, in slot order,
+     * 32 tuples a step (a ballot places each step's matches). */
+    CJ_DEV void warp_write(const Shared &sh, int64_t key, unsigned long long pos, uint32_t prow,
+                           const MatchOut &out) const {
+        const Entry en = entry(sh, key);
+        for (uint32_t j0 = 0; j0 < en.n; j0 += 32) {
+            const uint32_t j = j0 + lane_id();
+            Tuple<KB> t{};
+            bool hit = false;
+            if (j < en.n) {
+                t = ht.tuples[en.s + j];
+                hit = (int64_t)t.key == key;
+            }
+            const uint32_t b = __ballot_sync(0xffffffffu, hit);
+            if (hit) {
+                const unsigned long long p = pos + __popc(b & lanemask_lt());
+                if (p < out.capacity) {
+                    if (out.build_rids) out.build_rids[p] = t.rid;
+                    if (out.probe_rids) out.probe_rids[p] = prow;
+                    put_key(out, p, key);
+                }
+            }
+            pos += __popc(b);
+        }
+    }
 };
 
 /* Direct-mapped table: slots[key - lo] holds the build row of `key`, or
@@ -163,6 +208,7 @@ template <typename KB> struct HashMatcher {
  * caller then builds the hash table instead). */
 struct ArrayMatcher {
     static constexpr bool kAtMostOne = true; /* unique keys: 0 or 1 match per row */
+    static constexpr bool kHeavy = false;
     static constexpr int kMinBlocks = kProbeMinBlocks;
     static constexpr int kItems = 4;         /* one light chain per row: 4 rows per thread
                                                 fit 32 registers (387 us vs 434 us for 2
@@ -204,6 +250,7 @@ struct ArrayMatcher {
  * slots from the key's hash until the key or an empty slot. */
 struct OpenMatcher {
     static constexpr bool kAtMostOne = true; /* unique keys */
+    static constexpr bool kHeavy = false;
     static constexpr int kItems = 4;
     static constexpr int kMinBlocks = kProbeMinBlocks;
     const unsigned long long *slots;
@@ -242,6 +289,7 @@ struct OpenMatcher {
 
 struct LoopMatcher {
     static constexpr bool kAtMostOne = false;
+    static constexpr bool kHeavy = false;
     static constexpr int kMinBlocks = kProbeMinBlocks;
     static constexpr int kItems = kProbeItems;
     CJ_DEV LoopMatcher resolved() const { return *this; }
@@ -312,10 +360,24 @@ CJ_DEV void probe_tile(const ColView &pkey, uint32_t n, const M &m, const typena
     for (int it = 0; it < kItems; ++it) {
         const uint64_t i = row0 + (uint64_t)it * 32 + lane;
         const uint32_t si = warp * 32 * kItems + it * 32 + lane;
-        int64_t key;
+        int64_t key = 0;
         uint32_t c = 0, first = 0;
-        if (i < n && load_key_stream(pkey, (uint32_t)i, &key)) c = m.count(sh, key, first);
-        kinds |= (c == 0 ? 0u : (c == 1 ? 1u : 2u)) << (2 * it);
+        bool heavy = false;
+        if (i < n && load_key_stream(pkey, (uint32_t)i, &key)) {
+            if constexpr (M::kHeavy) c = m.count(sh, key, first, heavy);
+            else c = m.count(sh, key, first);
+        }
+        if constexpr (M::kHeavy) {
+            /* the warp counts each heavy row's slot together */
+            uint32_t hb = __ballot_sync(0xffffffffu, heavy);
+            while (hb) {
+                const int L = __ffs(hb) - 1;
+                hb &= hb - 1;
+                const uint32_t cnt = m.warp_count(sh, (int64_t)__shfl_sync(0xffffffffu, (long long)key, L));
+                if ((int)lane == L) c = cnt;
+            }
+        }
+        kinds |= (c == 0 ? 0u : (heavy ? 3u : (c == 1 ? 1u : 2u))) << (2 * it);
         ps.first[si] = first;
         if (wants_key(out) && c == 1) ps.key[si] = key;
         if (M::kAtMostOne) {
@@ -343,7 +405,6 @@ CJ_DEV void probe_tile(const ColView &pkey, uint32_t n, const M &m, const typena
 #pragma unroll
     for (int it = 0; it < kItems; ++it) {
         const uint32_t k = (kinds >> (2 * it)) & 3u;
-        if (!k) continue;
         const uint32_t prow = (uint32_t)(row0 + (uint64_t)it * 32 + lane);
         const uint32_t si = warp * 32 * kItems + it * 32 + lane;
         const unsigned long long pos = base + ps.pre[si];
@@ -353,10 +414,23 @@ CJ_DEV void probe_tile(const ColView &pkey, uint32_t n, const M &m, const typena
                 if (out.probe_rids) out.probe_rids[pos] = prow;
                 if (wants_key(out)) put_key(out, pos, ps.key[si]);
             }
-        } else {
+        } else if (k == 2) {
             int64_t key;
             load_key(pkey, prow, &key);
             m.write_all(sh, key, pos, prow, out);
+        }
+        if constexpr (M::kHeavy) {
+            /* heavy rows: the warp writes each one's matches together */
+            uint32_t hb = __ballot_sync(0xffffffffu, k == 3u);
+            while (hb) {
+                const int L = __ffs(hb) - 1;
+                hb &= hb - 1;
+                const uint32_t prow_l = __shfl_sync(0xffffffffu, prow, L);
+                const unsigned long long pos_l = __shfl_sync(0xffffffffu, pos, L);
+                int64_t key_l = 0;
+                load_key(pkey, prow_l, &key_l);
+                m.warp_write(sh, key_l, pos_l, prow_l, out);
+            }
         }
     }
     __syncthreads();

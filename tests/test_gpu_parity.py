@@ -508,3 +508,41 @@ def test_radix_passes_any_partition_size(gpu_ctx, spp):
     finally:
         gpu_ctx.set_option(_lib.CJ_OPT_SLOTS_PER_PARTITION, 0)
         gpu_ctx.set_option(_lib.CJ_OPT_DENSE_KEYS, 8)
+
+
+@pytest.mark.parametrize("key_type", [I, L])
+def test_heavy_slots_written_by_the_warp(gpu_ctx, key_type):
+    """Slots longer than 64 tuples are counted and written by the whole
+    warp: a key repeated 5,000 times on the build side (and a second one 70
+    times, just past the limit) against probe rows holding them, alone and
+    inside a batch."""
+    from calamarijoins_b200 import execute_batch
+    rng = np.random.default_rng(66)
+    nb, npr = 20_000, 60_000
+    bk = rng.permutation(nb).astype(np.int64) + 100
+    bk[:5000] = 7
+    bk[5000:5070] = 8
+    rng.shuffle(bk)
+    pk = rng.integers(0, nb + 200, npr)
+    pk[rng.choice(npr, 300, replace=False)] = 7
+    pk[rng.choice(npr, 300, replace=False)] = 8
+    npt = np.int32 if key_type == I else np.int64
+    pvalid = (rng.random(npr) > 0.03).astype(np.uint8)
+    plan = Plan()
+    plan.inputs.append(ColumnarTable(nb, [encode_column(key_type, bk.astype(npt)),
+                                          encode_column(I, rng.integers(0, 1 << 30, nb).astype(np.int32))]))
+    plan.inputs.append(ColumnarTable(npr, [encode_column(key_type, pk.astype(npt), pvalid),
+                                           encode_column(F, rng.standard_normal(npr))]))
+    plan.new_scan_node(0, [(0, key_type), (1, I)])
+    plan.new_scan_node(1, [(0, key_type), (1, F)])
+    plan.new_join_node(True, 0, 1, 0, 0, [(0, key_type), (1, I), (3, F)])
+    plan.root = 2
+    want = run_oracle(plan)
+    assert want.num_rows > 1_000_000
+    got, _ = run_product(plan, gpu_ctx)
+    assert_same(got, want, "alone")
+    res, sts, _ = execute_batch([plan, join2(100, 1000, seed=3)], gpu_ctx)
+    got = oa.PagedResult.from_result(res[0])
+    for r in res:
+        r.free()
+    assert_same(got, want, "batched")
