@@ -4,6 +4,8 @@
  */
 #include <cstdlib>
 #include <cstring>
+#include <thread>
+#include <vector>
 #include <string>
 
 #include "engine.h"
@@ -303,6 +305,27 @@ int cj_result_column_device(const cj_result *r, uint64_t c, const void **device_
     return CJ_OK;
 }
 
+/* Host-to-host copy split over up to 8 threads for large blocks (one core
+ * copies, and first-touches fresh destination pages, at a fraction of the
+ * host's memory bandwidth). */
+static void parallel_copy(void *dst, const void *src, uint64_t bytes) {
+    const uint64_t kMinPerThread = 32ull << 20;
+    unsigned nt = (unsigned)std::min<uint64_t>(8, bytes / kMinPerThread);
+    if (nt < 2) {
+        std::memcpy(dst, src, bytes);
+        return;
+    }
+    const uint64_t per = (bytes / nt + 4095) & ~uint64_t(4095);
+    std::vector<std::thread> ts;
+    for (unsigned t = 0; t < nt; ++t) {
+        const uint64_t b = t * per;
+        if (b >= bytes) break;
+        const uint64_t n = std::min(per, bytes - b);
+        ts.emplace_back([=] { std::memcpy(static_cast<uint8_t *>(dst) + b, static_cast<const uint8_t *>(src) + b, n); });
+    }
+    for (auto &t : ts) t.join();
+}
+
 int cj_result_copy_column(const cj_result *r, uint64_t c, void *dst, uint64_t dst_bytes) {
     if (!r || c >= r->types.size() || (!dst && r->num_pages[c]))
         return set_error(CJ_ERR_INVALID_ARGUMENT, "bad argument");
@@ -312,7 +335,7 @@ int cj_result_copy_column(const cj_result *r, uint64_t c, void *dst, uint64_t ds
     API_BEGIN
     set_device(r->ctx);
     if (!r->host_cols.empty() && r->host_cols[c]) {
-        std::memcpy(dst, r->host_cols[c], bytes);
+        parallel_copy(dst, r->host_cols[c], bytes);
     } else {
         cj::check_cuda(cudaMemcpyAsync(dst, r->dev_pages[c]->ptr, bytes, cudaMemcpyDeviceToHost, r->ctx->stream),
                        "download");
