@@ -277,8 +277,10 @@ def algorithmic_bytes(kernel: str, st: dict, plan_info: dict):
     slots = plan_info["slots"]
     if kernel == "probe_hash":
         # probe keys (4 B + 1 validity bit per row), one pass over the hash
-        # table (8 B tuples + 8 B directory slots), 2 x 4 B row ids per match
-        return npr * (4 + 1 / 8) + nb * 8 + slots * 8 + m * 8
+        # table (8 B tuples + 16 B directory entries for INT32 keys), per
+        # match 2 x 4 B row ids and the 4 B key the probe emits for the
+        # root's key columns
+        return npr * (4 + 1 / 8) + nb * 8 + slots * 16 + m * 12
     if kernel == "probe_array":
         # probe keys (4 B + validity bit), the direct-mapped table (4 B per
         # slot; the C2 build keys are a permutation of [0, rows), so slots =
@@ -300,7 +302,10 @@ def algorithmic_bytes(kernel: str, st: dict, plan_info: dict):
     if kernel == "decode_int32":
         return plan_info["int32_pages"] * 8192 / plan_info["int32_cols"] + 0  # per launch: one column
     if kernel == "build":
-        return nb * (4 + 4 + 8 + 8 + 8 + 8) + slots * 8
+        # keys read twice (histogram, scatter: 4 B + validity bit), tuples
+        # written once by the scatter, read twice and written once by the
+        # per-partition build; 16 B directory entries
+        return nb * (2 * (4 + 1 / 8) + 8 + 16 + 8) + slots * 16
     return None
 
 
@@ -585,8 +590,15 @@ def run_ours(args):
                 "traffic": (tr.get("bytes_per_launch") if tr else None), "peak_source": peak_kind,
                 "launches_timed": nl, "avg_launch_us": avg_us, "algorithmic_bytes_per_launch": ab}
 
-    kernels = {k: {"launches": v[0], "total_us": v[1], "share": v[1] / max(sum(x[1] for x in prof.values()), 1e-9)}
-               for k, v in sorted(prof.items(), key=lambda kv: -kv[1][1])}
+    kernels = {}
+    total_prof = max(sum(x[1] for x in prof.values()), 1e-9)
+    for k, v in sorted(prof.items(), key=lambda kv: -kv[1][1]):
+        e = {"launches": v[0], "total_us": v[1], "share": v[1] / total_prof}
+        ab = algorithmic_bytes(k, st.exec, info)
+        if ab:
+            gbs = ab / (v[1] / max(v[0], 1) * 1e-6) / 1e9
+            e.update({"algorithmic_bytes_per_launch": ab, "achieved_gbs": gbs, "frac_of_peak": gbs / peak})
+        kernels[k] = e
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -276,8 +276,10 @@ class Filter {
             count_launches(1);
             check_cuda(cudaGetLastError(), "popc");
             check_cuda(scan_u32_to_u64(L, cnt->as<uint32_t>(), off->as<uint64_t>(), words, tmp->ptr), "scan");
-            check_cuda(cudaMemcpyAsync(&ctx.h_status->aux[7], off->as<uint64_t>() + words, 8, cudaMemcpyDeviceToHost,
-                                       ctx.stream),
+            /* the count goes back with the status block (sync_status copies
+             * all of it to the host) */
+            check_cuda(cudaMemcpyAsync(&ctx.d_status->aux[7], off->as<uint64_t>() + words, 8,
+                                       cudaMemcpyDeviceToDevice, ctx.stream),
                        "copy");
             ctx.sync_status();
             count = ctx.h_status->aux[7];
@@ -308,10 +310,7 @@ class Filter {
                     check_cuda(launch_varchar_plan(L, v, count, TR, temp->ptr,
                                                    reinterpret_cast<unsigned long long *>(&ctx.d_status->aux[7])),
                                "varchar_plan");
-                    check_cuda(cudaMemcpyAsync(&ctx.h_status->aux[7], &ctx.d_status->aux[7], 8,
-                                               cudaMemcpyDeviceToHost, ctx.stream),
-                               "copy");
-                    ctx.sync_status();
+                    ctx.sync_status(); /* brings the page count back in aux[7] */
                     cp.num_pages = ctx.h_status->aux[7];
                     cp.owner = ctx.alloc(cp.num_pages * kPageSize);
                     check_cuda(launch_varchar_write(L, v, count, TR, temp->ptr, cp.owner->as<uint8_t>()),
