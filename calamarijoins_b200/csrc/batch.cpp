@@ -58,7 +58,8 @@ struct JoinWork {
         RelCol col;
     };
     std::vector<Out> outs;
-    DevPtr dir, tuples, part_buf, nlk, nlr, nlc, mb, mp, status;
+    DevPtr dir, tuples, part_buf, nlk, nlr, nlc, mb, mp, status, slots;
+    unsigned long long *params = nullptr; /* direct-mapped table's parameters (device) */
     int log2_slots = 0, log2_parts = 0;
     uint64_t M = 0;
 };
@@ -344,8 +345,48 @@ void BatchExecutor::run_level(int lvl) {
         max_slots = std::max(max_slots, 1u << (bp.log2_slots - bp.log2_parts));
         btasks.push_back(t);
     }
+    /* Unique keys spread over at most dense_keys x rows values also get a
+     * direct-mapped table (built beside the hash table, which stays the
+     * fallback): the device decides per join whether it is usable, and the
+     * probe takes it when it is (one random access per probe row). */
+    std::vector<DirectTask> dtasks;
+    std::vector<size_t> didx;
+    uint32_t key_blocks = 0, fill_blocks = 0;
+    for (size_t k = 0; k < work.size(); ++k) {
+        auto &w = work[k];
+        if (w.nl || !w.B->rows || !w.P->rows || ctx.opt.dense_keys <= 0) continue;
+        const uint64_t max_span = std::min<uint64_t>((uint64_t)ctx.opt.dense_keys * w.B->rows, 1ull << 28);
+        w.slots = ctx.alloc(max_span * 4);
+        DirectTask t{};
+        t.key = view(w.plan, *w.B, w.bk, nullptr);
+        t.n = (uint32_t)w.B->rows;
+        t.key_blocks = (uint32_t)((w.B->rows + kDirectBlockRows - 1) / kDirectBlockRows);
+        t.key_base = key_blocks;
+        t.fill_blocks = (uint32_t)((max_span + kDirectFillSlots - 1) / kDirectFillSlots);
+        t.fill_base = fill_blocks;
+        t.max_span = max_span;
+        t.slots = w.slots->as<uint32_t>();
+        key_blocks += t.key_blocks;
+        fill_blocks += t.fill_blocks;
+        dtasks.push_back(t);
+        didx.push_back(k);
+    }
+    DevPtr dparams;
+    if (!dtasks.empty()) {
+        std::vector<unsigned long long> init(dtasks.size() * kDirectParams, 0ull);
+        for (size_t j = 0; j < dtasks.size(); ++j) init[j * kDirectParams] = ~0ull;
+        dparams = upload_tasks(init);
+        for (size_t j = 0; j < dtasks.size(); ++j) {
+            dtasks[j].params = dparams->as<unsigned long long>() + j * kDirectParams;
+            work[didx[j]].params = dtasks[j].params;
+        }
+        keep_checks.push_back(dparams);
+    }
     stats.num_hash_joins += btasks.size();
     stats.num_nested_loop_joins += ntasks.size();
+    DevPtr dt = upload_tasks(dtasks);
+    ck(launch_direct_build_grouped(L, dt->as<DirectTask>(), (uint32_t)dtasks.size(), key_blocks, fill_blocks),
+       "direct_build_grouped");
     DevPtr bt = upload_tasks(btasks), nt = upload_tasks(ntasks);
     DevPtr btmp = ctx.alloc(build_grouped_temp_bytes(cells));
     ck(launch_build_grouped(L, bt->as<BuildTask>(), (uint32_t)btasks.size(), chunks, parts, cells, max_parts, max_slots,
@@ -389,7 +430,9 @@ void BatchExecutor::run_level(int lvl) {
             ProbeTask t{};
             t.pkey = view(w.plan, *w.P, w.pk, nullptr);
             t.n_probe = (uint32_t)w.P->rows;
-            t.kind = w.nl ? 1 : 0;
+            t.kind = w.nl ? 1 : (w.params ? 2 : 0);
+            t.slots = w.slots ? w.slots->as<uint32_t>() : nullptr;
+            t.params = w.params;
             t.build_key_type = w.bk.type;
             t.log2_slots = w.log2_slots;
             t.dir = w.dir ? w.dir->as<uint64_t>() : nullptr;
@@ -443,6 +486,7 @@ void BatchExecutor::run_level(int lvl) {
         w.dir.reset();
         w.tuples.reset();
         w.part_buf.reset();
+        w.slots.reset();
         stats.probe_rows += w.P->rows;
         stats.matches += w.M;
     }

@@ -321,7 +321,8 @@ cudaError_t launch_nl_probe_tiles(const Launch &L, const ColView &pkey, uint32_t
 struct ProbeTask {
     ColView pkey;
     uint32_t n_probe;
-    int32_t kind;           /* 0 hash, 1 nested loop                       */
+    int32_t kind;           /* 0 hash, 1 nested loop, 2 direct-mapped table
+                               when usable (params[3] == 0), else hash     */
     int32_t build_key_type; /* hash: CJ_INT32 / CJ_INT64 tuples            */
     int32_t log2_slots;
     const uint64_t *dir;
@@ -329,10 +330,30 @@ struct ProbeTask {
     const int64_t *nl_keys;
     const uint32_t *nl_rids;
     const uint32_t *nl_count;
+    const uint32_t *slots;              /* kind 2: direct-mapped table      */
+    const unsigned long long *params;   /* kind 2: its kDirectParams words  */
     MatchOut out;               /* out.counter zeroed before launch         */
     uint32_t num_tiles;
     uint32_t tile_base;         /* first global tile of this task           */
 };
+/* Grouped direct-mapped builds (launch_direct_build for every task): task k
+ * owns blocks [block_base, block_base + blocks) of each pass; params hold
+ * kDirectParams words per task, set to {~0, 0, 0, 0, 0, 0} before. */
+struct DirectTask {
+    ColView key;
+    uint32_t n;
+    uint32_t key_blocks;   /* blocks over the keys                         */
+    uint32_t key_base;
+    uint32_t fill_blocks;  /* blocks over max_span slots                   */
+    uint32_t fill_base;
+    uint64_t max_span;
+    uint32_t *slots;
+    unsigned long long *params;
+};
+cudaError_t launch_direct_build_grouped(const Launch &L, const DirectTask *tasks_dev, uint32_t ntasks,
+                                        uint32_t total_key_blocks, uint32_t total_fill_blocks);
+constexpr uint32_t kDirectBlockRows = 256 * 8; /* key rows per block of the grouped passes */
+constexpr uint32_t kDirectFillSlots = 256 * 16; /* slots per block of the grouped fill     */
 uint32_t probe_tiles(uint32_t n_probe);
 /* `ticket` must be zeroed, and each task's counter. */
 cudaError_t launch_probe_grouped(const Launch &L, const ProbeTask *tasks_dev, uint32_t ntasks,

@@ -460,13 +460,15 @@ CJ_DEV unsigned long long warp_max_u64(unsigned long long v) {
     return v;
 }
 
-__global__ void __launch_bounds__(kBuildThreads)
-    k_key_range(ColView key, uint32_t n, unsigned long long *range) {
+/* Block-wide min / max / count of the non-NULL keys of rows i0, i0 +
+ * stride, ... below i1, folded into range[0..2] by atomics. */
+CJ_DEV void key_range_rows(const ColView &key, uint64_t i0, uint64_t i1, uint64_t stride,
+                           unsigned long long *range) {
     __shared__ unsigned long long s_min[kBuildThreads / 32], s_max[kBuildThreads / 32];
     __shared__ unsigned int s_cnt[kBuildThreads / 32];
     unsigned long long mn = ~0ull, mx = 0ull;
     unsigned int cnt = 0;
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    for (uint64_t i = i0; i < i1; i += stride) {
         int64_t k;
         if (load_key(key, (uint32_t)i, &k)) {
             const unsigned long long b = (unsigned long long)k ^ (1ull << 63);
@@ -499,6 +501,12 @@ __global__ void __launch_bounds__(kBuildThreads)
     }
 }
 
+__global__ void __launch_bounds__(kBuildThreads)
+    k_key_range(ColView key, uint32_t n, unsigned long long *range) {
+    key_range_rows(key, (uint64_t)blockIdx.x * blockDim.x + threadIdx.x, n, (uint64_t)gridDim.x * blockDim.x,
+                   range);
+}
+
 /* params: [0] min ^ 2^63, [1] max ^ 2^63, [2] count (from k_key_range),
  * [3] unusable (1: span too wide, 2: a key repeats), [4] lo, [5] span. */
 __global__ void k_array_prep(unsigned long long *p, uint64_t max_span) {
@@ -527,6 +535,74 @@ __global__ void k_array_build(ColView key, uint32_t n, uint32_t *__restrict__ sl
         const uint64_t off = (uint64_t)k - lo;
         if (off >= span) continue; /* cannot happen: lo and span come from these keys */
         if (atomicCAS(slots + off, kArrayEmpty, (uint32_t)i) != kArrayEmpty) p[3] = 2ull; /* a key repeats */
+    }
+}
+
+/* ---- grouped direct-mapped builds (every candidate join of a batch level) ---- */
+CJ_DEV uint32_t find_direct_task(const DirectTask *tasks, uint32_t ntasks, uint32_t block, bool fill) {
+    uint32_t lo = 0, hi = ntasks;
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if ((fill ? tasks[mid].fill_base : tasks[mid].key_base) <= block) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+__global__ void __launch_bounds__(kBuildThreads)
+    k_key_range_grouped(const DirectTask *__restrict__ tasks, uint32_t ntasks) {
+    __shared__ uint32_t s_task;
+    if (threadIdx.x == 0) s_task = find_direct_task(tasks, ntasks, blockIdx.x, false);
+    __syncthreads();
+    const DirectTask &T = tasks[s_task];
+    const uint64_t r0 = (uint64_t)(blockIdx.x - T.key_base) * kDirectBlockRows;
+    const uint64_t r1 = min((uint64_t)T.n, r0 + kDirectBlockRows);
+    key_range_rows(T.key, r0 + threadIdx.x, r1, blockDim.x, T.params);
+}
+
+__global__ void k_array_prep_grouped(const DirectTask *__restrict__ tasks, uint32_t ntasks) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ntasks) return;
+    unsigned long long *p = tasks[t].params;
+    if (p[2] == 0) return;
+    const unsigned long long width = p[1] - p[0];
+    if (width >= tasks[t].max_span) {
+        p[3] = 1ull;
+        return;
+    }
+    p[4] = p[0] ^ (1ull << 63);
+    p[5] = width + 1;
+}
+
+__global__ void __launch_bounds__(kBuildThreads)
+    k_array_fill_grouped(const DirectTask *__restrict__ tasks, uint32_t ntasks) {
+    __shared__ uint32_t s_task;
+    if (threadIdx.x == 0) s_task = find_direct_task(tasks, ntasks, blockIdx.x, true);
+    __syncthreads();
+    const DirectTask &T = tasks[s_task];
+    const uint64_t span = T.params[3] ? 0ull : T.params[5];
+    const uint64_t i0 = (uint64_t)(blockIdx.x - T.fill_base) * kDirectFillSlots;
+    const uint64_t i1 = min(span, i0 + kDirectFillSlots);
+    for (uint64_t i = i0 + threadIdx.x; i < i1; i += blockDim.x) T.slots[i] = kArrayEmpty;
+}
+
+__global__ void __launch_bounds__(kBuildThreads)
+    k_array_build_grouped(const DirectTask *__restrict__ tasks, uint32_t ntasks) {
+    __shared__ uint32_t s_task;
+    if (threadIdx.x == 0) s_task = find_direct_task(tasks, ntasks, blockIdx.x, false);
+    __syncthreads();
+    const DirectTask &T = tasks[s_task];
+    unsigned long long *p = T.params;
+    if (p[3]) return;
+    const uint64_t lo = p[4], span = p[5];
+    const uint64_t r0 = (uint64_t)(blockIdx.x - T.key_base) * kDirectBlockRows;
+    const uint64_t r1 = min((uint64_t)T.n, r0 + kDirectBlockRows);
+    for (uint64_t i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+        int64_t k;
+        if (!load_key(T.key, (uint32_t)i, &k)) continue;
+        const uint64_t off = (uint64_t)k - lo;
+        if (off >= span) continue;
+        if (atomicCAS(T.slots + off, kArrayEmpty, (uint32_t)i) != kArrayEmpty) p[3] = 2ull;
     }
 }
 
@@ -661,6 +737,17 @@ cudaError_t launch_direct_build(const Launch &L, const ColView &key, uint32_t n,
     k_array_fill<<<(unsigned)g, 256, 0, L.stream>>>(slots, params);
     g = std::min<uint64_t>(((uint64_t)n + 255) / 256, (uint64_t)L.num_sms * 8);
     k_array_build<<<(unsigned)g, 256, 0, L.stream>>>(key, n, slots, params);
+    count_launches(4);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_direct_build_grouped(const Launch &L, const DirectTask *tasks_dev, uint32_t ntasks,
+                                        uint32_t total_key_blocks, uint32_t total_fill_blocks) {
+    if (!ntasks) return cudaSuccess;
+    if (total_key_blocks) k_key_range_grouped<<<total_key_blocks, kBuildThreads, 0, L.stream>>>(tasks_dev, ntasks);
+    k_array_prep_grouped<<<(ntasks + 127) / 128, 128, 0, L.stream>>>(tasks_dev, ntasks);
+    if (total_fill_blocks) k_array_fill_grouped<<<total_fill_blocks, kBuildThreads, 0, L.stream>>>(tasks_dev, ntasks);
+    if (total_key_blocks) k_array_build_grouped<<<total_key_blocks, kBuildThreads, 0, L.stream>>>(tasks_dev, ntasks);
     count_launches(4);
     return cudaGetLastError();
 }

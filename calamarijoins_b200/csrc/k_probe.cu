@@ -206,13 +206,11 @@ template <typename KB> struct HashMatcher {
  * kArrayEmpty. Unique build keys only: a duplicate found while building
  * sets *dup, and a probe launched over such a table does nothing (the
  * caller then builds the hash table instead). */
-struct ArrayMatcher {
+template <int kItemsT> struct ArrayMatcherT {
     static constexpr bool kAtMostOne = true; /* unique keys: 0 or 1 match per row */
     static constexpr bool kHeavy = false;
     static constexpr int kMinBlocks = kProbeMinBlocks;
-    static constexpr int kItems = 4;         /* one light chain per row: 4 rows per thread
-                                                fit 32 registers (387 us vs 434 us for 2
-                                                on 64M probe rows) */
+    static constexpr int kItems = kItemsT;
     const uint32_t *slots;
     const unsigned long long *params; /* [3] unusable, [4] lo, [5] span */
     uint64_t lo = 0, span = 0;        /* read from params by resolved() */
@@ -220,8 +218,8 @@ struct ArrayMatcher {
         uint32_t unused;
     };
     CJ_DEV bool skip() const { return params[3] != 0ull; }
-    CJ_DEV ArrayMatcher resolved() const {
-        ArrayMatcher m = *this;
+    CJ_DEV ArrayMatcherT resolved() const {
+        ArrayMatcherT m = *this;
         m.lo = params[4];
         m.span = params[5];
         return m;
@@ -245,6 +243,11 @@ struct ArrayMatcher {
         }
     }
 };
+
+/* One light chain per row: 4 rows per thread fit 32 registers (387 us vs
+ * 434 us for 2 on 64M probe rows). The grouped kernel's tiles are 2 rows
+ * per thread for every matcher (ArrayMatcherT<kProbeItems>). */
+using ArrayMatcher = ArrayMatcherT<4>;
 
 /* Open-addressing table of unique INT32 keys (launch_open_build): walk the
  * slots from the key's hash until the key or an empty slot. */
@@ -493,7 +496,13 @@ __global__ void __launch_bounds__(kProbeThreads, CJ_GROUPED_MIN_BLOCKS)
         if (gt >= total_tiles) break;
         const ProbeTask &T = tasks[ps.task];
         const uint32_t tile = gt - T.tile_base;
-        if (T.kind == 1) {
+        if (T.kind == 2 && T.params[3] == 0ull) {
+            /* a direct-mapped table the build found usable (unique keys
+             * over a dense range); otherwise the task's hash table below */
+            const ArrayMatcherT<kProbeItems> m = ArrayMatcherT<kProbeItems>{T.slots, T.params}.resolved();
+            ArrayMatcherT<kProbeItems>::Shared none;
+            probe_tile(T.pkey, T.n_probe, m, none, T.out, tile, ps);
+        } else if (T.kind == 1) {
             LoopMatcher m{T.nl_keys, T.nl_rids, T.nl_count};
             if (loaded_task != ps.task) {
                 __syncthreads();
