@@ -156,9 +156,12 @@ class BatchExecutor {
     void check_counts(const unsigned long long *counts, const std::vector<uint64_t> &want) {
         std::vector<unsigned long long> w(want.begin(), want.end());
         DevPtr d = upload_tasks(w);
-        ck(launch_check_counts(L, counts, d->as<unsigned long long>(), (uint32_t)w.size()), "check_counts");
+        ck(launch_check_counts(L, counts, d->as<unsigned long long>(), (uint32_t)w.size(), ctx.d_status->stale,
+                               num_checks++),
+           "check_counts");
         keep_checks.push_back(d);
     }
+    uint32_t num_checks = 0; /* checks captured so far (levels, then VARCHAR totals) */
     std::vector<DevPtr> keep_checks;
     int levels(PlanState &p, uint64_t node, int depth);
     void decode_all();
@@ -733,6 +736,19 @@ cj_prepared *prepare_batch(Context &ctx, const cj_plan_desc *plans, size_t n, ui
         for (uint64_t t = 0; t < plans[i].num_inputs; ++t)
             if (!resident_input(plans[i], t))
                 fail(CJ_ERR_UNSUPPORTED, "a prepared batch needs device-resident inputs (cj_table)");
+    /* A VARCHAR column's page count depends on the order of its rows (the
+     * writer packs each tile's strings greedily), and a probe's output
+     * order differs from run to run (tiles reserve their output as they
+     * finish): a graph cannot size such pages from a learned count.
+     * Fixed-width pages (ceil(rows / rows per page)) do not depend on it. */
+    for (size_t i = 0; i < n; ++i) {
+        if (plans[i].root >= plans[i].num_nodes || !plans[i].nodes) continue; /* the learn run reports it */
+        const cj_plan_node &root = plans[i].nodes[plans[i].root];
+        for (uint64_t a = 0; a < root.num_output_attrs; ++a)
+            if (root.output_attrs && root.output_attrs[a].type == CJ_VARCHAR)
+                fail(CJ_ERR_UNSUPPORTED, "a prepared batch writes fixed-width results only (plan " + std::to_string(i) +
+                                             " outputs VARCHAR, whose page count depends on the row order)");
+    }
     auto prep = std::make_unique<cj_prepared>();
     prep->ctx = &ctx;
     prep->plans.assign(plans, plans + n);

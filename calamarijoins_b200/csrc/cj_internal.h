@@ -70,6 +70,8 @@ struct StatusBlock {
     unsigned long long aux[8];    /* [0, kDirectParams): direct-mapped table
                                      parameters; [kOpenDup]: a repeated key
                                      in the open-addressing table          */
+    unsigned long long stale[3];  /* DEV_ERR_STALE: check index, count found,
+                                     count recorded (one of the mismatches) */
 };
 
 /* How a kernel reads one column of a relation: row i of the relation is
@@ -369,7 +371,8 @@ cudaError_t launch_nl_collect_grouped(const Launch &L, const NlCollectTask *task
 
 /* Raises DEV_ERR_STALE unless counts[i] == expected[i] for every i < n. */
 cudaError_t launch_check_counts(const Launch &L, const unsigned long long *counts,
-                                const unsigned long long *expected, uint32_t n);
+                                const unsigned long long *expected, uint32_t n,
+                                unsigned long long *detail, uint32_t check_id);
 
 /* Headers (n_rows = n_values), zero gaps and all-ones bitmaps of the
  * ceil(rows / R) pages of a NULL-free fixed-width column whose values are

@@ -177,7 +177,11 @@ void Context::sync_status() {
         if (err & DEV_ERR_BAD_PAGE_KIND) what += " special page in fixed-width column;";
         if (err & DEV_ERR_ROW_COUNT) what += " pages hold a row count other than the table's;";
         if (err & DEV_ERR_INTERNAL) what += " internal;";
-        if (err & DEV_ERR_STALE) what += " match counts differ from the prepared batch's (inputs changed);";
+        if (err & DEV_ERR_STALE)
+            what += " match counts differ from the prepared batch's (inputs changed): check " +
+                    std::to_string(h_status->stale[0] >> 32) + " entry " + std::to_string(h_status->stale[0] & 0xFFFFFFFFu) +
+                    " counted " + std::to_string(h_status->stale[1]) + ", recorded " + std::to_string(h_status->stale[2]) +
+                    ";";
         int code = (err & DEV_ERR_INTERNAL) ? CJ_ERR_INTERNAL
                    : (err & DEV_ERR_STALE)  ? CJ_ERR_INVALID_ARGUMENT
                                             : CJ_ERR_MALFORMED_PAGE;

@@ -516,6 +516,10 @@ __global__ void k_array_prep(unsigned long long *p, uint64_t max_span) {
         p[3] = 1ull;
         return;
     }
+    if (p[2] > width + 1) { /* more keys than values in their range: one repeats */
+        p[3] = 2ull;
+        return;
+    }
     p[4] = p[0] ^ (1ull << 63);
     p[5] = width + 1;
 }
@@ -568,6 +572,10 @@ __global__ void k_array_prep_grouped(const DirectTask *__restrict__ tasks, uint3
     const unsigned long long width = p[1] - p[0];
     if (width >= tasks[t].max_span) {
         p[3] = 1ull;
+        return;
+    }
+    if (p[2] > width + 1) { /* more keys than values in their range: one repeats */
+        p[3] = 2ull;
         return;
     }
     p[4] = p[0] ^ (1ull << 63);

@@ -651,16 +651,25 @@ cudaError_t launch_probe_grouped(const Launch &L, const ProbeTask *tasks_dev, ui
 
 namespace {
 __global__ void k_check_counts(const unsigned long long *__restrict__ counts,
-                               const unsigned long long *__restrict__ expected, uint32_t n, unsigned int *errors) {
+                               const unsigned long long *__restrict__ expected, uint32_t n, unsigned int *errors,
+                               unsigned long long *detail, uint32_t check_id) {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-        if (counts[i] != expected[i]) atomicOr(errors, (unsigned int)DEV_ERR_STALE);
+        if (counts[i] != expected[i]) {
+            /* the first mismatch found records where (check, entry) and
+             * the two counts */
+            if (!(atomicOr(errors, (unsigned int)DEV_ERR_STALE) & DEV_ERR_STALE) && detail) {
+                detail[0] = ((unsigned long long)check_id << 32) | i;
+                detail[1] = counts[i];
+                detail[2] = expected[i];
+            }
+        }
 }
 } // namespace
 
 cudaError_t launch_check_counts(const Launch &L, const unsigned long long *counts, const unsigned long long *expected,
-                                uint32_t n) {
+                                uint32_t n, unsigned long long *detail, uint32_t check_id) {
     if (!n) return cudaSuccess;
-    k_check_counts<<<(n + 255) / 256, 256, 0, L.stream>>>(counts, expected, n, L.dev_errors);
+    k_check_counts<<<(n + 255) / 256, 256, 0, L.stream>>>(counts, expected, n, L.dev_errors, detail, check_id);
     count_launches(1);
     return cudaGetLastError();
 }

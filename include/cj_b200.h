@@ -450,7 +450,9 @@ int cj_execute_batch(cj_context *ctx, const cj_plan_desc *plans,
  * overwritten by the next run of the same batch (free them or copy them
  * before). A run whose inputs no longer give the learned counts (the
  * resident tables were changed) fails with CJ_ERR_INVALID_ARGUMENT; prepare
- * the batch again. Plans with host inputs: CJ_ERR_UNSUPPORTED. */
+ * the batch again. Plans with host inputs, or with VARCHAR result columns
+ * (their page count depends on the order of the rows, which differs from
+ * run to run), are refused with CJ_ERR_UNSUPPORTED. */
 typedef struct cj_prepared cj_prepared;
 int cj_batch_prepare(cj_context *ctx, const cj_plan_desc *plans,
                      uint64_t num_plans, uint32_t flags, cj_prepared **out);

@@ -101,14 +101,14 @@ def _resident(plans, ctx):
 @pytest.mark.parametrize("flags", [0, 1])  # host results, device results
 def test_prepared_batch_replays(gpu_ctx, flags):
     """A batch captured as one CUDA graph: three replays in a row, each
-    result equal to the oracle's (chain plans with nested-loop and hash
-    joins, INT64 keys, VARCHAR outputs, a many-to-many join)."""
+    result equal to the oracle's (chain plans with nested-loop, direct and
+    hash joins, INT64 keys, a many-to-many join)."""
     from calamarijoins_b200 import PreparedBatch
     rng = np.random.default_rng(14)
     plans = [chain_plan(int(rng.integers(2, 5)), int(rng.integers(1000, 80000)), rng, max_build=40000,
-                        key_types=[I if rng.random() < 0.6 else L for _ in range(3)], varchar_frac=0.3)
+                        key_types=[I if rng.random() < 0.6 else L for _ in range(3)])
              for _ in range(12)]
-    plans.append(join2(3000, 30000, seed=7, unique_build=False, build_payload=(V,), probe_payload=(F,)))
+    plans.append(join2(3000, 30000, seed=7, unique_build=False, build_payload=(L,), probe_payload=(F,)))
     plans.append(join2(40, 10000, seed=8))  # nested loop
     want = [run_oracle(p) for p in plans]
     rplans, tables = _resident(plans, gpu_ctx)
@@ -132,3 +132,17 @@ def test_prepared_batch_needs_resident_inputs(gpu_ctx):
     with pytest.raises(CJError) as e:
         PreparedBatch([join2(100, 1000, seed=1)], gpu_ctx)
     assert e.value.status == 6  # CJ_ERR_UNSUPPORTED
+
+
+def test_prepared_batch_refuses_varchar_results(gpu_ctx):
+    """A VARCHAR result's page count depends on the order of its rows,
+    which differs between runs: a prepared batch refuses such plans."""
+    from calamarijoins_b200 import CJError, PreparedBatch
+    rplans, tables = _resident([join2(100, 1000, seed=1, build_payload=(V,))], gpu_ctx)
+    try:
+        with pytest.raises(CJError) as e:
+            PreparedBatch(rplans, gpu_ctx)
+        assert e.value.status == 6 and "VARCHAR" in str(e.value)
+    finally:
+        for t in tables:
+            t.free()
