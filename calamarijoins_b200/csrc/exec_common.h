@@ -127,8 +127,11 @@ inline void validate_plan(const Context &ctx, const cj_plan_desc &plan) {
     for (uint64_t t = 0; t < plan.num_inputs; ++t) {
         const cj_table *r = resident_input(plan, t);
         if (!r && !plan.inputs) fail(CJ_ERR_INVALID_PLAN, "input " + std::to_string(t) + " missing");
-        if (r && r->ctx != &ctx && r->ctx->pool != ctx.pool)
-            fail(CJ_ERR_INVALID_ARGUMENT, "resident table from another context");
+        /* a resident table is complete when it is handed out (its upload
+         * or filter synchronises), so any context of the same device may
+         * read it; its owner must outlive the plans that do */
+        if (r && r->ctx != &ctx && r->ctx->device != ctx.device)
+            fail(CJ_ERR_INVALID_ARGUMENT, "resident table of another device");
         if (!r) {
             const cj_table_desc &td = plan.inputs[t];
             if (td.num_columns && !td.columns) fail(CJ_ERR_INVALID_PLAN, "table without column array");

@@ -459,8 +459,8 @@ extern "C" int cj_table_filter(cj_context *ctx, const cj_table *in, const cj_pre
                                const uint64_t *columns, cj_table **out, uint64_t *num_rows) {
     if (!ctx || !in || !out) return cj::set_last_error(CJ_ERR_INVALID_ARGUMENT, "null argument");
     *out = nullptr;
-    if (in->ctx != ctx && in->ctx->pool != ctx->pool)
-        return cj::set_last_error(CJ_ERR_INVALID_ARGUMENT, "table of another context");
+    if (in->ctx != ctx && in->ctx->device != ctx->device)
+        return cj::set_last_error(CJ_ERR_INVALID_ARGUMENT, "table of another device");
     cudaSetDevice(ctx->device);
     try {
         *out = cj::filter_table(*ctx, *in, pred, num_columns, columns, num_rows);

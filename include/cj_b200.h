@@ -266,7 +266,9 @@ int cj_context_memory(const cj_context *ctx, uint64_t *used_bytes,
 /* Resident tables: pages uploaded once and kept in HBM                      */
 /* ------------------------------------------------------------------------ */
 
-/* Uploads every column of `table` into device memory. */
+/* Uploads every column of `table` into device memory. A resident table
+ * may be used by every context (and server) of the same device; free it
+ * after the last plan that reads it. */
 int cj_table_upload(cj_context *ctx, const cj_table_desc *table,
                     cj_table **out);
 
