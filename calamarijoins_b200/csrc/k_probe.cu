@@ -130,7 +130,7 @@ template <typename KB> struct HashMatcher {
     }
     /* heavy: the slot is longer than kHeavyRun; the count is left to
      * warp_count (0 returned). */
-    CJ_DEV uint32_t count(const Shared &sh, int64_t key, uint32_t &first, bool &heavy) const {
+    CJ_DEV uint32_t count(const Shared &sh, int64_t key, uint32_t &first, uint32_t &second, bool &heavy) const {
         const Entry en = entry(sh, key);
         if (en.n > kHeavyRun) {
             heavy = true;
@@ -148,6 +148,7 @@ template <typename KB> struct HashMatcher {
             const Tuple<KB> t = ht.tuples[en.s + j];
             if ((int64_t)t.key == key) {
                 if (!c) first = t.rid;
+                else if (c == 1) second = t.rid;
                 ++c;
             }
         }
@@ -313,11 +314,12 @@ struct LoopMatcher {
             sh.rids[b] = g_rids[b];
         }
     }
-    CJ_DEV uint32_t count(const Shared &sh, int64_t key, uint32_t &first) const {
+    CJ_DEV uint32_t count(const Shared &sh, int64_t key, uint32_t &first, uint32_t &second) const {
         uint32_t c = 0;
         for (uint32_t b = 0; b < sh.n; ++b)
             if (sh.keys[b] == key) {
                 if (!c) first = sh.rids[b];
+                else if (c == 1) second = sh.rids[b];
                 ++c;
             }
         return c;
@@ -340,7 +342,8 @@ struct LoopMatcher {
  * memory, not registers, so the kernel fits 32 registers (8 CTAs per SM). */
 template <int kItemsT> struct ProbeSmemT {
     static constexpr uint32_t kRows = kProbeThreads * kItemsT;
-    uint32_t first[kRows]; /* first matching build row (one-match rows) */
+    uint32_t first[kRows]; /* first matching build row (one- and two-match rows) */
+    uint32_t second[kRows]; /* second matching build row (two-match rows)        */
     int64_t key[kRows];    /* the row's key, when the matches carry it   */
     uint32_t pre[kRows];   /* row's match offset within its warp        */
     uint32_t warp[kProbeThreads / 32 + 1];
@@ -357,17 +360,21 @@ CJ_DEV void probe_tile(const ColView &pkey, uint32_t n, const M &m, const typena
     constexpr uint32_t kRows = ProbeSmemT<M::kItems>::kRows;
     const uint32_t warp = threadIdx.x >> 5, lane = lane_id();
     const uint64_t row0 = (uint64_t)tile * kRows + (uint64_t)warp * 32 * kItems;
-    uint32_t kinds = 0; /* 2 bits per item: 0 none, 1 one match, 2 more */
+    /* 3 bits per item: 0 no match, 1 one, 2 two (both build rows kept), 3
+     * more (the write pass walks the slot again), 4 heavy slot (the warp
+     * writes it) */
+    uint32_t kinds = 0;
     uint32_t wrun = 0;
 #pragma unroll
     for (int it = 0; it < kItems; ++it) {
         const uint64_t i = row0 + (uint64_t)it * 32 + lane;
         const uint32_t si = warp * 32 * kItems + it * 32 + lane;
         int64_t key = 0;
-        uint32_t c = 0, first = 0;
+        uint32_t c = 0, first = 0, second = 0;
         bool heavy = false;
         if (i < n && load_key_stream(pkey, (uint32_t)i, &key)) {
-            if constexpr (M::kHeavy) c = m.count(sh, key, first, heavy);
+            if constexpr (M::kHeavy) c = m.count(sh, key, first, second, heavy);
+            else if constexpr (!M::kAtMostOne) c = m.count(sh, key, first, second);
             else c = m.count(sh, key, first);
         }
         if constexpr (M::kHeavy) {
@@ -380,9 +387,11 @@ CJ_DEV void probe_tile(const ColView &pkey, uint32_t n, const M &m, const typena
                 if ((int)lane == L) c = cnt;
             }
         }
-        kinds |= (c == 0 ? 0u : (heavy ? 3u : (c == 1 ? 1u : 2u))) << (2 * it);
+        const uint32_t kind = c == 0 ? 0u : (heavy ? 4u : (c <= 2 ? c : 3u));
+        kinds |= kind << (3 * it);
         ps.first[si] = first;
-        if (wants_key(out) && c == 1) ps.key[si] = key;
+        if (!M::kAtMostOne) ps.second[si] = second;
+        if (wants_key(out) && (kind == 1u || kind == 2u)) ps.key[si] = key;
         if (M::kAtMostOne) {
             const uint32_t ball = __ballot_sync(0xffffffffu, c != 0);
             ps.pre[si] = wrun + __popc(ball & lanemask_lt());
@@ -407,24 +416,29 @@ CJ_DEV void probe_tile(const ColView &pkey, uint32_t n, const M &m, const typena
     const unsigned long long base = ps.base + ps.warp[warp];
 #pragma unroll
     for (int it = 0; it < kItems; ++it) {
-        const uint32_t k = (kinds >> (2 * it)) & 3u;
+        const uint32_t k = (kinds >> (3 * it)) & 7u;
         const uint32_t prow = (uint32_t)(row0 + (uint64_t)it * 32 + lane);
         const uint32_t si = warp * 32 * kItems + it * 32 + lane;
         const unsigned long long pos = base + ps.pre[si];
-        if (k == 1) {
+        if (k == 1 || k == 2) {
             if (pos < out.capacity) {
                 if (out.build_rids) out.build_rids[pos] = ps.first[si];
                 if (out.probe_rids) out.probe_rids[pos] = prow;
                 if (wants_key(out)) put_key(out, pos, ps.key[si]);
             }
-        } else if (k == 2) {
+            if (!M::kAtMostOne && k == 2 && pos + 1 < out.capacity) {
+                if (out.build_rids) out.build_rids[pos + 1] = ps.second[si];
+                if (out.probe_rids) out.probe_rids[pos + 1] = prow;
+                if (wants_key(out)) put_key(out, pos + 1, ps.key[si]);
+            }
+        } else if (k == 3) {
             int64_t key;
             load_key(pkey, prow, &key);
             m.write_all(sh, key, pos, prow, out);
         }
         if constexpr (M::kHeavy) {
             /* heavy rows: the warp writes each one's matches together */
-            uint32_t hb = __ballot_sync(0xffffffffu, k == 3u);
+            uint32_t hb = __ballot_sync(0xffffffffu, k == 4u);
             while (hb) {
                 const int L = __ffs(hb) - 1;
                 hb &= hb - 1;
