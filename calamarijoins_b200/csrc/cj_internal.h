@@ -233,12 +233,15 @@ struct BuildPlan {
     int log2_parts;      /* radix partition bits in all: one pass up to 12
                             bits, two passes above (launch_build)         */
     uint32_t num_rows;   /* rows of the build relation                    */
+    bool inline_first = true; /* INT32 keys: 16-byte entries holding the
+                                 slot's first tuple (DirEntry32), else the
+                                 8-byte word alone                        */
 };
 /* Directory entry word: start (63..32) | count (31..16, saturated) | tags
  * (15..0); INT32 keys add the first tuple (DirEntry32); one sentinel entry
  * after the last slot. */
-inline size_t build_dir_bytes(int log2_slots, int key_bytes) {
-    return ((1ull << log2_slots) + 1) * (key_bytes == 4 ? sizeof(DirEntry32) : sizeof(uint64_t));
+inline size_t build_dir_bytes(int log2_slots, int key_bytes, bool inline_first = true) {
+    return ((1ull << log2_slots) + 1) * (key_bytes == 4 && inline_first ? sizeof(DirEntry32) : sizeof(uint64_t));
 }
 size_t build_temp_bytes(const Launch &L, const BuildPlan &bp, int key_bytes);
 size_t build_tuple_bytes(int key_bytes);
@@ -306,10 +309,12 @@ cudaError_t launch_probe_tiles_open(const Launch &L, const ColView &pkey, uint32
 /* Probe and nested loop share one tiled kernel; `sched` is scratch of
  * probe_sched_bytes(n_probe) bytes (the tile ticket). */
 size_t probe_sched_bytes(uint32_t n_probe);
+/* inline_dir: the table was built with BuildPlan::inline_first (INT32
+ * keys only; ignored for INT64). */
 cudaError_t launch_probe_tiles_hash(const Launch &L, const ColView &pkey, uint32_t n_probe,
                                     int32_t build_key_type, const uint64_t *dir,
                                     const void *tuples, int log2_slots, const uint16_t *bloom,
-                                    const MatchOut &out, void *sched);
+                                    const MatchOut &out, void *sched, bool inline_dir = true);
 
 /* Nested loop (build side <= 64 rows) */
 constexpr uint32_t kNestedLoopMax = 64;

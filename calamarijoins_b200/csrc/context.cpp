@@ -296,6 +296,7 @@ Context *create_context(int device, cudaMemPool_t shared_pool) {
     c->opt.ctas_per_sm = env_opt("CJ_CTAS_PER_SM", c->opt.ctas_per_sm);
     c->opt.dense_keys = std::max<int64_t>(0, std::min<int64_t>(64, env_opt("CJ_DENSE_KEYS", c->opt.dense_keys)));
     c->opt.buffer_cache_bytes = std::max<int64_t>(0, env_opt("CJ_BUFFER_CACHE_BYTES", c->opt.buffer_cache_bytes));
+    c->opt.inline_dir_max_bytes = std::max<int64_t>(0, env_opt("CJ_INLINE_DIR_MAX_BYTES", c->opt.inline_dir_max_bytes));
     if (shared_pool) c->opt.buffer_cache_bytes = 0; /* contexts sharing a pool share through it */
     if (const char *tf = std::getenv("CJ_TUNING_FILE"); tf && *tf) c->tuning = load_tuning_file(tf, c->num_sms);
     return c.release();

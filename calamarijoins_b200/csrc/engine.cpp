@@ -346,6 +346,7 @@ Relation Executor::exec_join(uint64_t node_idx, int depth, bool is_root, cj_resu
         const bool nl = B.rows <= nl_max;
         DevPtr dir, tuples, nlk, nlr, nlc, slots;
         int log2_slots = 0;
+        bool inline_dir = true;
         unsigned long long *d_params = &ctx.d_status->aux[0];
         bool direct = false; /* direct-mapped table tried (the device decides) */
         bool open = false;   /* open-addressing table tried (the device decides) */
@@ -380,7 +381,10 @@ Relation Executor::exec_join(uint64_t node_idx, int depth, bool is_root, cj_resu
             log2_slots = bp.log2_slots;
             const int kb = bk.type == CJ_INT32 ? 4 : 8;
             const Launch LB = build_launch(ctx, B.rows);
-            dir = ctx.alloc(build_dir_bytes(bp.log2_slots, kb));
+            bp.inline_first = kb == 4 && build_dir_bytes(bp.log2_slots, 4, true) + B.rows * build_tuple_bytes(4) <=
+                                             (uint64_t)ctx.opt.inline_dir_max_bytes;
+            inline_dir = bp.inline_first;
+            dir = ctx.alloc(build_dir_bytes(bp.log2_slots, kb, bp.inline_first));
             tuples = ctx.alloc(B.rows * build_tuple_bytes(kb));
             DevPtr tmp = ctx.alloc(build_temp_bytes(LB, bp, kb));
             KScope k(*this, "build");
@@ -456,7 +460,7 @@ Relation Executor::exec_join(uint64_t node_idx, int depth, bool is_root, cj_resu
                     KScope k(*this, "probe_hash");
                     ck(launch_probe_tiles_hash(probe_launch(ctx, P.rows), pv, (uint32_t)P.rows, bk.type,
                                                dir->as<uint64_t>(), tuples->ptr, log2_slots, ctx.d_bloom, mo,
-                                               sched->ptr),
+                                               sched->ptr, inline_dir),
                        "probe");
                 }
             }

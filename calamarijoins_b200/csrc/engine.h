@@ -47,6 +47,11 @@ struct Options {
     int64_t dense_keys = 8; /* max key span / build rows for a direct-mapped table; 0 = off */
     int64_t buffer_cache_bytes = 16ll << 30; /* freed device buffers kept for reuse */
     int64_t fail_alloc_at = 0; /* injected failure of the N-th device allocation from now; 0 = off */
+    /* INT32-key hash tables whose directory (16-byte entries) and tuples
+     * together stay within this many bytes keep each slot's first tuple in
+     * its entry; larger ones use 8-byte entries, so that more of the table
+     * stays in L2 (environment CJ_INLINE_DIR_MAX_BYTES) */
+    int64_t inline_dir_max_bytes = 64ll << 20;
 };
 
 struct Context;

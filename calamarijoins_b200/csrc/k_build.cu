@@ -143,7 +143,7 @@ template <typename K>
 CJ_DEV void build_partition(const Tuple<K> *__restrict__ in, const uint64_t *__restrict__ offsets, uint64_t off_base,
                             uint32_t grid_hist, int log2_parts, int log2_slots, uint32_t p, const uint16_t *s_bloom,
                             uint64_t *__restrict__ dir, Tuple<K> *__restrict__ out, uint32_t *s_cnt, uint32_t *s_tag,
-                            uint32_t *wbuf) {
+                            uint32_t *wbuf, bool inline_first) {
     const uint32_t S = 1u << (log2_slots - log2_parts);
     for (uint32_t s = threadIdx.x; s < S; s += blockDim.x) {
         s_cnt[s] = 0;
@@ -167,7 +167,7 @@ CJ_DEV void build_partition(const Tuple<K> *__restrict__ in, const uint64_t *__r
         if (s0 + k < S) sum += s_cnt[s0 + k];
     uint32_t tot;
     uint32_t pre = block_exclusive_scan<uint32_t>(sum, wbuf, &tot);
-    constexpr bool kInline = sizeof(K) == 4; /* DirEntry32: first tuple in the entry */
+    const bool kInline = sizeof(K) == 4 && inline_first; /* DirEntry32: first tuple in the entry */
     DirEntry32 *dir16 = reinterpret_cast<DirEntry32 *>(dir);
     for (uint32_t k = 0; k < per; ++k) {
         uint32_t s = s0 + k;
@@ -285,7 +285,7 @@ template <typename K>
 __global__ void __launch_bounds__(kBuildThreads)
     k_part_build(const Tuple<K> *__restrict__ in, const uint64_t *__restrict__ offsets, uint32_t grid_hist,
                  int log2_parts, int log2_slots, const uint16_t *__restrict__ g_bloom, uint64_t *__restrict__ dir,
-                 Tuple<K> *__restrict__ out) {
+                 Tuple<K> *__restrict__ out, int inline_first) {
     extern __shared__ uint32_t smem[];
     __shared__ uint16_t s_bloom[2048];
     __shared__ uint32_t wbuf[kBuildThreads / 32 + 1];
@@ -294,7 +294,7 @@ __global__ void __launch_bounds__(kBuildThreads)
     load_bloom(s_bloom, g_bloom);
     for (uint32_t p = blockIdx.x; p < P; p += gridDim.x)
         build_partition<K>(in, offsets, 0, grid_hist, log2_parts, log2_slots, p, s_bloom, dir, out, smem, smem + S,
-                           wbuf);
+                           wbuf, inline_first != 0);
 }
 
 /* ---- grouped kernels: every hash join of a batch level ---- */
@@ -364,11 +364,11 @@ __global__ void __launch_bounds__(kBuildThreads)
         if (T.key.type == CJ_INT32)
             build_partition<int32_t>(reinterpret_cast<const Tuple<int32_t> *>(T.part_buf), off, off[0], T.grid,
                                      T.log2_parts, T.log2_slots, u - T.part_base, s_bloom, T.dir,
-                                     reinterpret_cast<Tuple<int32_t> *>(T.tuples), smem, smem + S, wbuf);
+                                     reinterpret_cast<Tuple<int32_t> *>(T.tuples), smem, smem + S, wbuf, true);
         else
             build_partition<int64_t>(reinterpret_cast<const Tuple<int64_t> *>(T.part_buf), off, off[0], T.grid,
                                      T.log2_parts, T.log2_slots, u - T.part_base, s_bloom, T.dir,
-                                     reinterpret_cast<Tuple<int64_t> *>(T.tuples), smem, smem + S, wbuf);
+                                     reinterpret_cast<Tuple<int64_t> *>(T.tuples), smem, smem + S, wbuf, true);
     }
 }
 
@@ -443,7 +443,7 @@ cudaError_t build_impl(const Launch &L, const BuildPlan &bp, const ColView &key,
     const size_t build_smem = 2 * S * sizeof(uint32_t);
     unsigned grid_b = (unsigned)(P < (uint64_t)L.num_sms * 16 ? P : (uint64_t)L.num_sms * 16);
     k_part_build<K><<<grid_b, kBuildThreads, build_smem, L.stream>>>(
-        parts, bounds, bounds_stride, bp.log2_parts, bp.log2_slots, bloom, dir, tuples);
+        parts, bounds, bounds_stride, bp.log2_parts, bp.log2_slots, bloom, dir, tuples, bp.inline_first ? 1 : 0);
     count_launches(1);
     return cudaGetLastError();
 }

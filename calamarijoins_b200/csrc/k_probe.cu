@@ -78,9 +78,9 @@ CJ_DEV void put_key(const MatchOut &out, unsigned long long pos, int64_t key) {
  * them) and the OR of their Bloom tags (15..0). INT32-key tables hold the
  * slot's first tuple in the entry too (DirEntry32, 16 bytes, one sector):
  * a row whose slot has one tuple is answered by that one random load. */
-template <typename KB> struct HashMatcher {
+template <typename KB, bool kInlineDir = (sizeof(KB) == 4)> struct HashMatcher {
     static constexpr bool kAtMostOne = false;
-    static constexpr bool kInline = sizeof(KB) == 4;
+    static constexpr bool kInline = kInlineDir && sizeof(KB) == 4;
     /* A probe row whose slot holds more tuples than this is counted and
      * written by its whole warp (warp_count / warp_write), 32 tuples a
      * step, instead of by its own lane alone: a heavy-hitter key with
@@ -610,9 +610,13 @@ uint32_t probe_tiles(uint32_t n_probe) { return (n_probe + kTileRows - 1) / kTil
 
 cudaError_t launch_probe_tiles_hash(const Launch &L, const ColView &pkey, uint32_t n_probe, int32_t build_key_type,
                                     const uint64_t *dir, const void *tuples, int log2_slots, const uint16_t *bloom,
-                                    const MatchOut &out, void *sched_mem) {
+                                    const MatchOut &out, void *sched_mem, bool inline_dir) {
+    if (build_key_type == CJ_INT32 && inline_dir) {
+        HashMatcher<int32_t, true> m{{dir, reinterpret_cast<const Tuple<int32_t> *>(tuples), log2_slots}, bloom};
+        return run_tiles(L, pkey, n_probe, m, out, sched_mem);
+    }
     if (build_key_type == CJ_INT32) {
-        HashMatcher<int32_t> m{{dir, reinterpret_cast<const Tuple<int32_t> *>(tuples), log2_slots}, bloom};
+        HashMatcher<int32_t, false> m{{dir, reinterpret_cast<const Tuple<int32_t> *>(tuples), log2_slots}, bloom};
         return run_tiles(L, pkey, n_probe, m, out, sched_mem);
     }
     HashMatcher<int64_t> m{{dir, reinterpret_cast<const Tuple<int64_t> *>(tuples), log2_slots}, bloom};
