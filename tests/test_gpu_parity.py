@@ -546,3 +546,25 @@ def test_heavy_slots_written_by_the_warp(gpu_ctx, key_type):
     for r in res:
         r.free()
     assert_same(got, want, "batched")
+
+
+@pytest.mark.parametrize("budget", [0, 1 << 40])
+def test_hash_directory_layouts(budget):
+    """INT32-key hash tables with 8-byte directory entries (budget 0) and
+    with the slot's first tuple inline (16-byte entries): the same results."""
+    import os
+    from calamarijoins_b200 import Context
+    os.environ["CJ_INLINE_DIR_MAX_BYTES"] = str(budget)
+    try:
+        ctx = Context(0)
+    finally:
+        del os.environ["CJ_INLINE_DIR_MAX_BYTES"]
+    try:
+        ctx.set_option(_lib.CJ_OPT_DENSE_KEYS, 0)
+        for plan in (join2(200_000, 1_000_000, seed=51, unique_build=False, zipf=0.8, probe_null=0.05),
+                     join2(300_000, 1_000_000, seed=52, zipf=0.9, outside=0.3),
+                     join2(5_000, 100_000, seed=53, unique_build=False, zipf=1.2)):
+            got, _ = run_product(plan, ctx)
+            assert_same(got, run_oracle(plan), f"budget {budget}")
+    finally:
+        ctx.close()
