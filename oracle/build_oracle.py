@@ -116,6 +116,35 @@ def build_reference_filter(force: bool = False) -> str | None:
     return out
 
 
+def build_reference_cache(force: bool = False) -> str | None:
+    """oracle/_ref/libcj_ref_cache.so: the reference's `.tbl` cache reader
+    (Table::from_cache, src/build_table.cpp) and writer (DumpTable,
+    include/data_access/table.h) behind oracle/ref_cache_bridge.cpp. The
+    reference's table.h needs range-v3, absent here: compiled as C++23 with
+    oracle/ref_shim_tbl's stand-in over std::ranges, and with the reference's
+    own headers ahead of oracle/ref_shim (only its re2 stand-in is used)."""
+    ref = reference_dir()
+    if ref is None:
+        return None
+    try:
+        import torch  # only for the bundled header-only fmt
+        fmt_inc = os.path.join(os.path.dirname(torch.__file__), "include")
+    except Exception:  # pragma: no cover
+        return None
+    outdir = os.path.join(HERE, "_ref")
+    os.makedirs(outdir, exist_ok=True)
+    sources = [os.path.join(ref, "src", f) for f in ("build_table.cpp", "csv_parser.cpp", "statement.cpp")]
+    sources.append(os.path.join(HERE, "ref_cache_bridge.cpp"))
+    out = os.path.join(outdir, "libcj_ref_cache.so")
+    deps = sources + [os.path.join(HERE, "ref_shim_tbl", "range", "v3", "all.hpp")]
+    if force or not _newer(out, deps):
+        _run(["g++", "-std=c++23", "-O2", "-fpermissive", "-w", "-fno-gnu-unique", "-Wl,-Bsymbolic",
+              "-DFMT_HEADER_ONLY", "-I", os.path.join(HERE, "ref_shim_tbl"), "-I", os.path.join(ref, "include"),
+              "-I", os.path.join(HERE, "ref_shim"), "-I", fmt_inc,
+              "-shared", "-fPIC", *sources, "-o", out, "-lpthread"])
+    return out
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--threads", default=",".join(str(t) for t in DEFAULT_THREADS))
@@ -125,6 +154,7 @@ def main(argv=None) -> int:
     for p in build_reference(tuple(int(x) for x in a.threads.split(",")), a.force):
         print(p)
     print(build_reference_filter(a.force))
+    print(build_reference_cache(a.force))
     return 0
 
 

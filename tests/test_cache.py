@@ -3,8 +3,12 @@ DumpTable format and cj_cache_read_meta checks it, without a GPU; on the
 GPU, a cache file loaded into a resident table (directly or through a
 catalog) gives the same join results as the host pages it came from.
 
-The format is restated here from the reference's sources, which cannot be
-compiled in this environment (table.h needs range-v3): TableMeta
+The format is checked two ways. Against the reference's own code: its
+Table::from_cache (src/build_table.cpp:140-197) reads the files the library
+writes, and the library reads the files its DumpTable::dump
+(include/data_access/table.h:136-221) writes (oracle/_ref/
+libcj_ref_cache.so, compiled here with a std::ranges stand-in for range-v3).
+And restated from the sources: TableMeta
 (include/data_access/table.h:30-35) = u64 num_rows, u64 num_cols,
 16 x 4-byte DataType, 16 x u64 page counts (208 bytes) at the start of an
 8 KiB header page filled with zeros (FILLER_SIZE, table.h:37, 210-214),
@@ -129,3 +133,79 @@ def test_cache_to_resident_tables_and_catalog(gpu_ctx, tmp_path):
             cat.load("t0", str(tmp_path / "t0.tbl"))  # the name is taken
     finally:
         cat.close()
+
+
+# ---- against the reference's own reader and writer ----
+
+import ctypes as C
+
+REF_CACHE_SO = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle", "_ref",
+                            "libcj_ref_cache.so")
+need_ref_cache = pytest.mark.skipif(not os.path.exists(REF_CACHE_SO), reason="reference cache code not compiled")
+
+
+def ref_cache_lib():
+    h = C.CDLL(REF_CACHE_SO)
+    P = C.c_void_p
+    from calamarijoins_b200._lib import TableDesc
+    sigs = {"cjref_cache_read": (C.c_int, [C.c_char_p, C.POINTER(P)]), "cjref_cache_num_rows": (C.c_uint64, [P]),
+            "cjref_cache_num_columns": (C.c_uint64, [P]),
+            "cjref_cache_column": (C.c_int, [P, C.c_uint64, C.POINTER(C.c_int32), C.POINTER(C.c_uint64),
+                                             C.POINTER(P), C.c_uint64]),
+            "cjref_cache_free": (None, [P]), "cjref_cache_write": (C.c_int, [C.POINTER(TableDesc), C.c_char_p])}
+    for n, (r, a) in sigs.items():
+        f = getattr(h, n)
+        f.restype, f.argtypes = r, a
+    return h
+
+
+def read_with_reference(path):
+    """Table::from_cache(path) -> (num_rows, [(type, pages as (n, 8192) uint8)])."""
+    L = ref_cache_lib()
+    h = C.c_void_p()
+    assert L.cjref_cache_read(path.encode(), C.byref(h)) == 0
+    try:
+        out = []
+        for c in range(L.cjref_cache_num_columns(h)):
+            t, n = C.c_int32(), C.c_uint64()
+            L.cjref_cache_column(h, c, C.byref(t), C.byref(n), None, 0)
+            ptrs = (C.c_void_p * max(n.value, 1))()
+            L.cjref_cache_column(h, c, C.byref(t), C.byref(n), ptrs, n.value)
+            pages = np.zeros((n.value, 8192), np.uint8)
+            for k in range(n.value):
+                pages[k] = np.frombuffer((C.c_uint8 * 8192).from_address(ptrs[k]), np.uint8)
+            out.append((t.value, pages))
+        return L.cjref_cache_num_rows(h), out
+    finally:
+        L.cjref_cache_free(h)
+
+
+@need_ref_cache
+@pytest.mark.parametrize("n", [0, 1, 20_000])
+def test_reference_reads_what_the_library_writes(tmp_path, n):
+    t = sample_table(n=max(n, 1)) if n else ColumnarTable(0, [encode_column(I, np.zeros(0, np.int32)),
+                                                               encode_column(V, [])])
+    path = str(tmp_path / "lib.tbl")
+    write_cache(t, path)
+    rows, cols = read_with_reference(path)
+    assert rows == t.num_rows
+    assert [c for c, _ in cols] == [int(c.type) for c in t.columns]
+    for (_, pages), col in zip(cols, t.columns):
+        assert np.array_equal(pages, col.pages.reshape(-1, 8192))
+
+
+@need_ref_cache
+def test_library_reads_what_the_reference_writes(tmp_path):
+    from oracle.oracle_api import _table_desc
+    t = sample_table(seed=3, n=30_000)
+    path = str(tmp_path / "ref.tbl")
+    td, keep, cols = _table_desc(t)
+    assert ref_cache_lib().cjref_cache_write(C.byref(td), path.encode()) == 0
+    m = read_cache_meta(path)
+    assert m["num_rows"] == t.num_rows
+    assert m["types"] == [c.type for c in t.columns]
+    assert m["num_pages"] == [c.num_pages for c in t.columns]
+    # and the library's writer produces the very same file
+    mine = str(tmp_path / "lib.tbl")
+    write_cache(t, mine)
+    assert open(mine, "rb").read() == open(path, "rb").read()
