@@ -815,9 +815,10 @@ def run_serve(args):
         return {"plans_per_s": st["plans_per_s"], "p50_ms": st["p50_us"] / 1e3, "p99_ms": st["p99_us"] / 1e3,
                 "mean_ms": st["mean_us"] / 1e3, "max_ms": st["max_us"] / 1e3, "failed": st["failed"],
                 "rejected": st["rejected"], "peak_admitted_gb": st["peak_admitted_bytes"] / 1e9,
-                "batches": st["batches"], "mean_batch": st["mean_batch"], "skipped_ahead": st["skipped_ahead"]}
+                "batches": st["batches"], "mean_batch": st["mean_batch"], "skipped_ahead": st["skipped_ahead"],
+                "batch_fallbacks": st["batch_fallbacks"]}
 
-    def plain(ctx, arrivals, order):
+    def plain(ctx, arrivals, order, flags):
         lat = []
         t0 = time.perf_counter()
         last = t0
@@ -825,7 +826,7 @@ def run_serve(args):
             d = at - (time.perf_counter() - t0)
             if d > 0:
                 time.sleep(d)
-            r, _ = cj.execute_raw(pool[k], ctx, 0, descs[k])
+            r, _ = cj.execute_raw(pool[k], ctx, flags, descs[k])
             r.free()
             last = time.perf_counter()
             lat.append((last - t0) - at)
@@ -833,32 +834,52 @@ def run_serve(args):
         return {"plans_per_s": len(lat) / wall, "p50_ms": pct(lat, 0.5) * 1e3, "p99_ms": pct(lat, 0.99) * 1e3,
                 "mean_ms": statistics.mean(lat) * 1e3, "max_ms": max(lat) * 1e3}
 
-    srv = cj.Server(device=0, slots=4, memory_budget=150 << 30)
+    from calamarijoins_b200 import _lib
+    modes = {"host": 0, "device": _lib.CJ_EXEC_RESULT_ON_DEVICE}
+    per_mode = {}
+    result_bytes = []
     try:
-        log("warm-up")
-        for d in descs:
-            r, _ = srv.wait(srv.submit(d))
-            r.free()
-        srv.stats(reset=True)
-        for p, d in zip(pool, descs):
-            r, _ = cj.execute_raw(p, ctx, 0, d)
-            r.free()
-        per_rate = []
-        for lam in C5_RATES:
-            arrivals, order = trace(lam)
-            log(f"rate {lam}/s: {len(order)} plans, served")
-            sv = served(srv, arrivals, order)
-            log(f"rate {lam}/s: plain")
-            pl = plain(ctx, arrivals, order)
-            per_rate.append({"rate": lam, "plans": len(order), "served": sv, "plain": pl,
-                             "served_over_plain": sv["plans_per_s"] / pl["plans_per_s"]})
+        for mode, flags in modes.items():
+            srv = cj.Server(device=0, slots=4, memory_budget=150 << 30, flags=flags)
+            try:
+                log(f"{mode} results: warm-up")
+                for _ in range(2):  # every worker sees plans of every size: pinned and pool blocks exist
+                    ts = [srv.submit(d) for d in descs for _ in range(2)]
+                    for t in ts:
+                        r, _ = srv.wait(t)
+                        r.free()
+                srv.stats(reset=True)
+                for i, (p, d) in enumerate(zip(pool, descs)):
+                    r, _ = cj.execute_raw(p, ctx, flags, d)
+                    if mode == "host":
+                        result_bytes.append(sum(r.column_info(c)[1] for c in range(r.num_columns)) * 8192)
+                    r.free()
+                per_rate = []
+                for lam in C5_RATES:
+                    arrivals, order = trace(lam)
+                    log(f"{mode} results, rate {lam}/s: {len(order)} plans, served")
+                    sv = served(srv, arrivals, order)
+                    log(f"{mode} results, rate {lam}/s: plain")
+                    pl = plain(ctx, arrivals, order, flags)
+                    per_rate.append({"rate": lam, "plans": len(order), "served": sv, "plain": pl,
+                                     "served_over_plain": sv["plans_per_s"] / pl["plans_per_s"]})
+                per_mode[mode] = per_rate
+            finally:
+                srv.close()
     finally:
-        srv.close()
         for t in tables:
             t.free()
         ctx.close()
+    per_rate = per_mode["host"]
+    mean_mb = statistics.mean(result_bytes) / 1e6
     best = max(per_rate, key=lambda x: x["served"]["plans_per_s"])
     plain_best = max(x["plain"]["plans_per_s"] for x in per_rate)
+
+    def summary(rates):
+        b = max(rates, key=lambda x: x["served"]["plans_per_s"])
+        pb = max(x["plain"]["plans_per_s"] for x in rates)
+        return {"served_best_plans_per_s": b["served"]["plans_per_s"], "plain_best_plans_per_s": pb,
+                "served_over_plain_at_saturation": b["served"]["plans_per_s"] / pb}
     line = {"metric": "served plans/s (Poisson arrivals), p50 / p99 latency", "value": best["served"]["plans_per_s"],
             "unit": "plans/s", "n_gpus": 1, "steps": len(C5_RATES), "warmup": 1, "ms_per_step": None,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32/int64",
@@ -873,6 +894,11 @@ def run_serve(args):
             "rates": per_rate,
             "plain_best_plans_per_s": plain_best,
             "served_over_plain_at_saturation": best["served"]["plans_per_s"] / plain_best,
+            "result_mb_per_plan": mean_mb,
+            "result_download_gbs_at_best": mean_mb * best["served"]["plans_per_s"] / 1e3,
+            "device_results": {"rates": per_mode["device"], **summary(per_mode["device"]),
+                               "note": "the same trace with results left in HBM (CJ_EXEC_RESULT_ON_DEVICE) in "
+                                       "both arms: no result download"},
             "cpu_baseline": {"unavailable": "the reference joins INT32 keys only (30 % of the pool has INT64 keys) "
                                             "and has no serving front end"}}
     print(json.dumps(line))

@@ -67,9 +67,13 @@ void Context::trim_buffers() {
 }
 
 PinnedBlock::~PinnedBlock() {
-    if (!ptr || !ctx) return;
-    std::lock_guard<std::mutex> g(ctx->pinned_mu);
-    ctx->pinned_free.emplace(bytes, ptr);
+    if (!ptr || !pool) return;
+    std::lock_guard<std::mutex> g(pool->mu);
+    pool->free.emplace(bytes, ptr);
+}
+
+PinnedPool::~PinnedPool() {
+    for (auto &kv : free) cudaFreeHost(kv.second);
 }
 
 DevPtr Context::alloc(size_t bytes) {
@@ -124,16 +128,16 @@ static size_t pinned_class(size_t bytes) {
 
 PinnedPtr Context::alloc_pinned(size_t bytes) {
     auto b = std::make_shared<PinnedBlock>();
-    b->ctx = this;
+    b->pool = pinned;
     if (bytes == 0) return b;
     size_t cls = pinned_class(bytes);
     {
-        std::lock_guard<std::mutex> g(pinned_mu);
-        auto it = pinned_free.find(cls);
-        if (it != pinned_free.end()) {
+        std::lock_guard<std::mutex> g(pinned->mu);
+        auto it = pinned->free.find(cls);
+        if (it != pinned->free.end()) {
             b->ptr = it->second;
             b->bytes = cls;
-            pinned_free.erase(it);
+            pinned->free.erase(it);
             return b;
         }
     }
@@ -217,7 +221,6 @@ Context::~Context() {
         if (staging_ev[i]) cudaEventDestroy(staging_ev[i]);
         if (staging[i]) cudaFreeHost(staging[i]);
     }
-    for (auto &kv : pinned_free) cudaFreeHost(kv.second);
     if (h_status) cudaFreeHost(h_status);
     if (d_status) cudaFree(d_status);
     if (d_bloom) cudaFree(d_bloom);
@@ -254,7 +257,7 @@ cudaMemPool_t create_pool(int device) {
     return pool;
 }
 
-Context *create_context(int device, cudaMemPool_t shared_pool) {
+Context *create_context(int device, cudaMemPool_t shared_pool, std::shared_ptr<PinnedPool> shared_pinned) {
     int n = 0;
     cudaError_t e = cudaGetDeviceCount(&n);
     if (e != cudaSuccess || n == 0) {
@@ -266,6 +269,7 @@ Context *create_context(int device, cudaMemPool_t shared_pool) {
     check_cuda(cudaSetDevice(device), "cudaSetDevice");
     std::unique_ptr<Context> c(new cj_context());
     c->device = device;
+    c->pinned = shared_pinned ? shared_pinned : std::make_shared<PinnedPool>();
     check_cuda(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device), "attr");
     check_cuda(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "stream");
     check_cuda(cudaStreamCreateWithFlags(&c->h2d_stream, cudaStreamNonBlocking), "stream");

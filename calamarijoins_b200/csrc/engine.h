@@ -51,7 +51,7 @@ struct Options {
      * together stay within this many bytes keep each slot's first tuple in
      * its entry; larger ones use 8-byte entries, so that more of the table
      * stays in L2 (environment CJ_INLINE_DIR_MAX_BYTES) */
-    int64_t inline_dir_max_bytes = 64ll << 20;
+    int64_t inline_dir_max_bytes = 256ll << 20;
 };
 
 struct Context;
@@ -68,9 +68,19 @@ struct DevBuf {
 };
 using DevPtr = std::shared_ptr<DevBuf>;
 
-/* Page-locked host block from the context's pinned pool. */
+/* Cache of page-locked host blocks by size class (cudaHostAlloc is slow:
+ * freed blocks are kept for reuse). A context has its own; the worker
+ * contexts of a server share one, so that no worker pays for allocating
+ * blocks another has already made. */
+struct PinnedPool {
+    std::multimap<size_t, void *> free;
+    std::mutex mu;
+    ~PinnedPool();
+};
+
+/* Page-locked host block from a pinned pool. */
 struct PinnedBlock {
-    Context *ctx = nullptr;
+    std::shared_ptr<PinnedPool> pool;
     void *ptr = nullptr;
     size_t bytes = 0;
     ~PinnedBlock();
@@ -100,9 +110,7 @@ struct Context {
     Options opt;
     Tuning tuning; /* autotuned launch parameters (cj_autotune / CJ_TUNING_FILE) */
 
-    /* pinned pool: size class -> free blocks */
-    std::multimap<size_t, void *> pinned_free;
-    std::mutex pinned_mu;
+    std::shared_ptr<PinnedPool> pinned; /* pinned host blocks by size class */
 
     /* Freed device buffers by size class. Every use of a context buffer is
      * ordered on the kernel stream (copy streams wait on it and it waits on
@@ -165,7 +173,8 @@ void upload_pages(Context &ctx, const cj_column_desc &cd, ColumnPages &out, uint
 
 /* Creates a context on `device`; with `shared_pool` non-null the context
  * allocates from that pool instead of creating its own. Throws Error. */
-Context *create_context(int device, cudaMemPool_t shared_pool);
+Context *create_context(int device, cudaMemPool_t shared_pool,
+                        std::shared_ptr<PinnedPool> shared_pinned = nullptr);
 /* Reads a tuning file written by cj_autotune; num_sms > 0 must match the
  * file's SM count. Throws Error. */
 Tuning load_tuning_file(const char *path, int num_sms);

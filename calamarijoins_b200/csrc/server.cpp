@@ -143,7 +143,7 @@ struct cj_server {
     uint64_t admitted = 0, peak_admitted = 0;
     uint32_t running = 0;      /* plans running                       */
     uint32_t busy_workers = 0; /* workers running a plan or a batch   */
-    uint64_t batches = 0, batched_plans = 0, skipped_ahead = 0;
+    uint64_t batches = 0, batched_plans = 0, skipped_ahead = 0, batch_fallbacks = 0;
     bool stop = false;
     /* statistics */
     uint64_t submitted = 0, completed = 0, failed = 0, rejected = 0, cancelled = 0;
@@ -270,6 +270,8 @@ struct cj_server {
                     }
                     cudaStreamSynchronize(ctx.stream);
                     cudaGetLastError();
+                    std::lock_guard<std::mutex> lk(mu);
+                    ++batch_fallbacks;
                 }
             }
             if (!done)
@@ -315,7 +317,8 @@ int cj_server_create(const cj_server_config *cfg, cj_server **out) {
         cj::check_cuda(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo");
         s->budget = cfg->memory_budget ? cfg->memory_budget : (uint64_t)(free_b * 0.85);
         const uint32_t slots = cfg->slots ? cfg->slots : 4;
-        for (uint32_t w = 0; w < slots; ++w) s->workers.emplace_back(cj::create_context(dev, s->pool));
+        auto pinned = std::make_shared<cj::PinnedPool>(); /* one cache of result blocks for all workers */
+        for (uint32_t w = 0; w < slots; ++w) s->workers.emplace_back(cj::create_context(dev, s->pool, pinned));
     } catch (const cj::Error &e) {
         for (auto &w : s->workers) w.reset();
         if (s->pool) cudaMemPoolDestroy(s->pool);
@@ -415,11 +418,12 @@ int cj_server_get_stats(cj_server *s, cj_server_stats *out, int reset) {
     st.batches = s->batches;
     st.skipped_ahead = s->skipped_ahead;
     st.mean_batch = s->batches ? (double)s->batched_plans / s->batches : 0;
+    st.batch_fallbacks = s->batch_fallbacks;
     *out = st;
     if (reset) {
         s->latencies.clear();
         s->completed = s->failed = s->rejected = s->cancelled = s->submitted = 0;
-        s->batches = s->batched_plans = s->skipped_ahead = 0;
+        s->batches = s->batched_plans = s->skipped_ahead = s->batch_fallbacks = 0;
         s->t_first = s->t_last = 0;
         s->peak_admitted = s->admitted;
     }

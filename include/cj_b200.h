@@ -544,6 +544,9 @@ typedef struct cj_server_stats {
     uint64_t skipped_ahead;                 /* plans admitted ahead of an
                                                earlier one that did not fit */
     double mean_batch;                      /* plans per execution          */
+    uint64_t batch_fallbacks;               /* grouped executions that failed
+                                               as a whole, their plans then
+                                               run one by one               */
 } cj_server_stats;
 
 int cj_server_create(const cj_server_config *config, cj_server **out);
