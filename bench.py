@@ -262,11 +262,12 @@ def measured_peaks():
         return 6650.0, "fallback"
 
 
-def traffic_table():
-    """Per-launch DRAM traffic of kernels from committed ncu summaries."""
+def traffic_table(workload: str):
+    """Per-launch DRAM traffic of this workload's kernels, from the committed
+    ncu summaries (keyed by workload, then by kernel)."""
     try:
         with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
-            return json.load(f)
+            return json.load(f).get(workload, {})
     except Exception:
         return {}
 
@@ -283,6 +284,8 @@ def algorithmic_bytes(kernel: str, st: dict, plan_info: dict):
         # root's key columns
         return npr * (4 + 1 / 8) + nb * 8 + slots * 16 + m * 12
     if kernel == "probe_array":
+        if not st.get("num_direct_joins"):
+            return None  # the launch found the table unusable and returned at once
         # probe keys (4 B + validity bit), the direct-mapped table (4 B per
         # slot; the C2 build keys are a permutation of [0, rows), so slots =
         # build rows) once; per match 2 x 4 B row ids and the 4 B key the
@@ -584,7 +587,7 @@ def run_ours(args):
         name, (nl, tot_us) = dom
         avg_us = tot_us / max(nl, 1)
         ab = algorithmic_bytes(name, st.exec, info)
-        tr = traffic_table().get(name)
+        tr = traffic_table(WL["name"]).get(name)
         achieved = (ab / (avg_us * 1e-6) / 1e9) if ab else None
         roof = {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": (achieved / peak) if achieved else None,
@@ -816,7 +819,8 @@ def run_serve(args):
                 "mean_ms": st["mean_us"] / 1e3, "max_ms": st["max_us"] / 1e3, "failed": st["failed"],
                 "rejected": st["rejected"], "peak_admitted_gb": st["peak_admitted_bytes"] / 1e9,
                 "batches": st["batches"], "mean_batch": st["mean_batch"], "skipped_ahead": st["skipped_ahead"],
-                "batch_fallbacks": st["batch_fallbacks"]}
+                "batch_fallbacks": st["batch_fallbacks"], "pinned_allocs": st["pinned_allocs"],
+                "pinned_alloc_mb": st["pinned_alloc_bytes"] / 1e6}
 
     def plain(ctx, arrivals, order, flags):
         lat = []
@@ -844,9 +848,12 @@ def run_serve(args):
             try:
                 log(f"{mode} results: warm-up")
                 for _ in range(2):  # every worker sees plans of every size: pinned and pool blocks exist
-                    ts = [srv.submit(d) for d in descs for _ in range(2)]
+                    ts = [srv.submit(d) for d in descs for _ in range(2)]  # grouped executions
                     for t in ts:
                         r, _ = srv.wait(t)
+                        r.free()
+                    for d in descs:  # one plan at a time
+                        r, _ = srv.wait(srv.submit(d))
                         r.free()
                 srv.stats(reset=True)
                 for i, (p, d) in enumerate(zip(pool, descs)):

@@ -114,7 +114,7 @@ class ServerStatsC(C.Structure):
         "peak_admitted_bytes", "memory_budget")]
         + [(n, C.c_double) for n in ("p50_us", "p99_us", "mean_us", "max_us", "wall_s", "plans_per_s")]
         + [("batches", C.c_uint64), ("skipped_ahead", C.c_uint64), ("mean_batch", C.c_double),
-           ("batch_fallbacks", C.c_uint64)])
+           ("batch_fallbacks", C.c_uint64), ("pinned_allocs", C.c_uint64), ("pinned_alloc_bytes", C.c_uint64)])
 
 
 # every function of include/cj_b200.h: name -> (restype, argtypes)

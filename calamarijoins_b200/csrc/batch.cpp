@@ -615,16 +615,16 @@ void BatchExecutor::materialize_roots() {
         }
     }
     if (flags & CJ_EXEC_RESULT_ON_DEVICE) return;
-    uint64_t total = 0;
-    for (auto &p : ps)
-        if (p.result)
-            for (uint64_t np : p.result->num_pages) total += np;
-    if (!total) return;
-    PinnedPtr host = ctx.alloc_pinned(total * kPageSize);
-    uint8_t *h = static_cast<uint8_t *>(host->ptr);
     for (auto &p : ps) {
         if (!p.result) continue;
-        p.result->host = host; /* shared block, released with the last result */
+        uint64_t total = 0;
+        for (uint64_t np : p.result->num_pages) total += np;
+        if (!total) continue;
+        /* one block per plan, of the size a plan run alone takes, so that
+         * blocks go back to the pool as their results are freed and serve
+         * single-plan and grouped executions alike */
+        p.result->host = ctx.alloc_pinned(total * kPageSize);
+        uint8_t *h = static_cast<uint8_t *>(p.result->host->ptr);
         for (size_t c = 0; c < p.result->num_pages.size(); ++c) {
             p.result->host_cols[c] = h;
             const size_t bytes = p.result->num_pages[c] * kPageSize;

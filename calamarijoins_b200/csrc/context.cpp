@@ -132,11 +132,13 @@ PinnedPtr Context::alloc_pinned(size_t bytes) {
     if (bytes == 0) return b;
     size_t cls = pinned_class(bytes);
     {
+        /* best fit: the smallest cached block of this class or up to two
+         * classes larger (a block of 4x the request at most) */
         std::lock_guard<std::mutex> g(pinned->mu);
-        auto it = pinned->free.find(cls);
-        if (it != pinned->free.end()) {
+        auto it = pinned->free.lower_bound(cls);
+        if (it != pinned->free.end() && it->first <= 4 * cls) {
             b->ptr = it->second;
-            b->bytes = cls;
+            b->bytes = it->first;
             pinned->free.erase(it);
             return b;
         }
@@ -147,6 +149,8 @@ PinnedPtr Context::alloc_pinned(size_t bytes) {
         cudaGetLastError();
         fail(CJ_ERR_OUT_OF_MEMORY, "pinned allocation of " + std::to_string(cls) + " bytes failed");
     }
+    pinned->host_allocs.fetch_add(1, std::memory_order_relaxed);
+    pinned->host_alloc_bytes.fetch_add(cls, std::memory_order_relaxed);
     b->ptr = p;
     b->bytes = cls;
     return b;

@@ -13,6 +13,7 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 #include <map>
 #include <memory>
@@ -75,6 +76,7 @@ using DevPtr = std::shared_ptr<DevBuf>;
 struct PinnedPool {
     std::multimap<size_t, void *> free;
     std::mutex mu;
+    std::atomic<uint64_t> host_allocs{0}, host_alloc_bytes{0}; /* cudaHostAlloc calls made */
     ~PinnedPool();
 };
 

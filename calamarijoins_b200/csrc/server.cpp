@@ -144,6 +144,8 @@ struct cj_server {
     uint32_t running = 0;      /* plans running                       */
     uint32_t busy_workers = 0; /* workers running a plan or a batch   */
     uint64_t batches = 0, batched_plans = 0, skipped_ahead = 0, batch_fallbacks = 0;
+    std::shared_ptr<cj::PinnedPool> pinned; /* the workers' shared result blocks */
+    uint64_t pinned_allocs0 = 0, pinned_bytes0 = 0;
     bool stop = false;
     /* statistics */
     uint64_t submitted = 0, completed = 0, failed = 0, rejected = 0, cancelled = 0;
@@ -317,8 +319,8 @@ int cj_server_create(const cj_server_config *cfg, cj_server **out) {
         cj::check_cuda(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo");
         s->budget = cfg->memory_budget ? cfg->memory_budget : (uint64_t)(free_b * 0.85);
         const uint32_t slots = cfg->slots ? cfg->slots : 4;
-        auto pinned = std::make_shared<cj::PinnedPool>(); /* one cache of result blocks for all workers */
-        for (uint32_t w = 0; w < slots; ++w) s->workers.emplace_back(cj::create_context(dev, s->pool, pinned));
+        s->pinned = std::make_shared<cj::PinnedPool>(); /* one cache of result blocks for all workers */
+        for (uint32_t w = 0; w < slots; ++w) s->workers.emplace_back(cj::create_context(dev, s->pool, s->pinned));
     } catch (const cj::Error &e) {
         for (auto &w : s->workers) w.reset();
         if (s->pool) cudaMemPoolDestroy(s->pool);
@@ -419,8 +421,13 @@ int cj_server_get_stats(cj_server *s, cj_server_stats *out, int reset) {
     st.skipped_ahead = s->skipped_ahead;
     st.mean_batch = s->batches ? (double)s->batched_plans / s->batches : 0;
     st.batch_fallbacks = s->batch_fallbacks;
+    const cj::PinnedPool &pp = *s->pinned;
+    st.pinned_allocs = pp.host_allocs.load() - s->pinned_allocs0;
+    st.pinned_alloc_bytes = pp.host_alloc_bytes.load() - s->pinned_bytes0;
     *out = st;
     if (reset) {
+        s->pinned_allocs0 = pp.host_allocs.load();
+        s->pinned_bytes0 = pp.host_alloc_bytes.load();
         s->latencies.clear();
         s->completed = s->failed = s->rejected = s->cancelled = s->submitted = 0;
         s->batches = s->batched_plans = s->skipped_ahead = s->batch_fallbacks = 0;

@@ -547,6 +547,10 @@ typedef struct cj_server_stats {
     uint64_t batch_fallbacks;               /* grouped executions that failed
                                                as a whole, their plans then
                                                run one by one               */
+    uint64_t pinned_allocs;                 /* page-locked host blocks
+                                               allocated for results (the
+                                               rest came from the cache)    */
+    uint64_t pinned_alloc_bytes;
 } cj_server_stats;
 
 int cj_server_create(const cj_server_config *config, cj_server **out);
