@@ -273,7 +273,10 @@ def traffic_table(workload: str):
 
 
 def algorithmic_bytes(kernel: str, st: dict, plan_info: dict):
-    """Algorithmic HBM bytes of ONE launch of `kernel` in this workload."""
+    """Algorithmic HBM bytes of ONE launch of `kernel` in this workload
+    (two-table workloads; None for the multi-join C3)."""
+    if WL["name"] == "c3":
+        return None
     nb, npr = plan_info["build_rows"], plan_info["probe_rows"]
     m = st["matches"]
     slots = plan_info["slots"]
@@ -844,7 +847,8 @@ def run_serve(args):
     result_bytes = []
     try:
         for mode, flags in modes.items():
-            srv = cj.Server(device=0, slots=4, memory_budget=150 << 30, flags=flags)
+            srv = cj.Server(device=0, slots=4, memory_budget=150 << 30, flags=flags,
+                            host_cache_bytes=(8 << 30) if mode == "host" else 0)
             try:
                 log(f"{mode} results: warm-up")
                 for _ in range(2):  # every worker sees plans of every size: pinned and pool blocks exist
@@ -895,7 +899,8 @@ def run_serve(args):
                                     "10 % VARCHAR outputs, probes log-uniform 1e4-1e7 rows, dimensions 10-1e6 rows, "
                                     "base tables resident in HBM, results to host memory; Poisson arrivals, each "
                                     "plan drawn from the pool; served: "
-                                    "4 worker streams, 150 GB admission budget, continuous batching; plain: "
+                                    "4 worker streams, 150 GB admission budget, continuous batching, 8 GB "
+                                    "page-locked result cache reserved at creation; plain: "
                                     "cj_execute one plan at a time in arrival order"), "scale": args.scale,
                        "probe_rows": {"min": min(probe_rows), "max": max(probe_rows)}},
             "rates": per_rate,

@@ -88,7 +88,7 @@ class ExecStatsC(C.Structure):
         + [(n, C.c_uint64) for n in (
             "h2d_bytes", "d2h_bytes", "num_joins", "num_hash_joins", "num_nested_loop_joins",
             "probe_rows", "matches", "probe_reruns", "output_rows", "output_pages",
-            "kernel_launches", "num_direct_joins", "num_open_joins")])
+            "kernel_launches", "num_direct_joins", "num_open_joins", "host_syncs")])
 
 
 class CacheMetaC(C.Structure):
@@ -105,7 +105,8 @@ class BatchStatsC(C.Structure):
 
 class ServerConfigC(C.Structure):
     _fields_ = [("device", C.c_int32), ("slots", C.c_uint32), ("memory_budget", C.c_uint64),
-                ("exec_flags", C.c_uint32), ("max_batch", C.c_uint32), ("age_limit_us", C.c_uint64)]
+                ("exec_flags", C.c_uint32), ("max_batch", C.c_uint32), ("age_limit_us", C.c_uint64),
+                ("host_cache_bytes", C.c_uint64)]
 
 
 class ServerStatsC(C.Structure):

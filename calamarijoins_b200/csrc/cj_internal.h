@@ -382,7 +382,12 @@ cudaError_t launch_check_counts(const Launch &L, const unsigned long long *count
 /* Headers (n_rows = n_values), zero gaps and all-ones bitmaps of the
  * ceil(rows / R) pages of a NULL-free fixed-width column whose values are
  * already in place (R by type, as rows_per_page_fixed). */
-cudaError_t launch_finish_dense_pages(const Launch &L, uint8_t *pages, uint64_t rows, int32_t type);
+/* The page writers below take `rows` as the rows to write, or, with
+ * `rows_dev` set, as the capacity the pages were sized for while the count
+ * itself is read on the device from *rows_dev (a match counter the host has
+ * not read yet). */
+cudaError_t launch_finish_dense_pages(const Launch &L, uint8_t *pages, uint64_t rows, int32_t type,
+                                      const unsigned long long *rows_dev = nullptr);
 
 /* Intermediates: out[i] = src[idx[i]] */
 cudaError_t launch_gather_u32(const Launch &L, const uint32_t *src,
@@ -412,7 +417,8 @@ cudaError_t launch_write_fixed_grouped(const Launch &L, const PageTask *tasks_de
 /* Output pages */
 uint32_t rows_per_page_fixed(int32_t type);
 cudaError_t launch_write_fixed_pages(const Launch &L, const ColView &col,
-                                     uint64_t rows, uint8_t *out_pages);
+                                     uint64_t rows, uint8_t *out_pages,
+                                     const unsigned long long *rows_dev = nullptr);
 size_t varchar_temp_bytes(uint64_t rows, uint32_t tile_rows);
 /* Pass 1: page count per tile; total pages into *total_pages_dev. */
 cudaError_t launch_varchar_plan(const Launch &L, const ColView &col, uint64_t rows,

@@ -69,11 +69,59 @@ void Context::trim_buffers() {
 PinnedBlock::~PinnedBlock() {
     if (!ptr || !pool) return;
     std::lock_guard<std::mutex> g(pool->mu);
-    pool->free.emplace(bytes, ptr);
+    if (in_arena) pool->arena_give(ptr, bytes);
+    else pool->free.emplace(bytes, ptr);
 }
 
 PinnedPool::~PinnedPool() {
     for (auto &kv : free) cudaFreeHost(kv.second);
+    if (arena) cudaFreeHost(arena);
+}
+
+constexpr size_t kArenaAlign = 64u << 10; /* arena blocks start and end on 64 KB */
+
+void PinnedPool::reserve(size_t bytes) {
+    std::lock_guard<std::mutex> g(mu);
+    if (arena || !bytes) return;
+    bytes = (bytes + kArenaAlign - 1) & ~(kArenaAlign - 1);
+    void *p = nullptr;
+    if (cudaHostAlloc(&p, bytes, cudaHostAllocDefault) != cudaSuccess) {
+        cudaGetLastError();
+        fail(CJ_ERR_OUT_OF_MEMORY, "page-locked host cache of " + std::to_string(bytes) + " bytes failed");
+    }
+    host_allocs.fetch_add(1, std::memory_order_relaxed);
+    host_alloc_bytes.fetch_add(bytes, std::memory_order_relaxed);
+    arena = static_cast<uint8_t *>(p);
+    arena_bytes = bytes;
+    arena_free.emplace(0, bytes);
+}
+
+void *PinnedPool::arena_take(size_t bytes) {
+    for (auto it = arena_free.begin(); it != arena_free.end(); ++it) {
+        if (it->second < bytes) continue;
+        const size_t off = it->first, left = it->second - bytes;
+        arena_free.erase(it);
+        if (left) arena_free.emplace(off + bytes, left);
+        return arena + off;
+    }
+    return nullptr;
+}
+
+void PinnedPool::arena_give(void *p, size_t bytes) {
+    size_t off = static_cast<uint8_t *>(p) - arena;
+    auto next = arena_free.lower_bound(off);
+    if (next != arena_free.end() && off + bytes == next->first) {
+        bytes += next->second;
+        next = arena_free.erase(next);
+    }
+    if (next != arena_free.begin()) {
+        auto prev = std::prev(next);
+        if (prev->first + prev->second == off) {
+            prev->second += bytes;
+            return;
+        }
+    }
+    arena_free.emplace(off, bytes);
 }
 
 DevPtr Context::alloc(size_t bytes) {
@@ -132,9 +180,18 @@ PinnedPtr Context::alloc_pinned(size_t bytes) {
     if (bytes == 0) return b;
     size_t cls = pinned_class(bytes);
     {
+        std::lock_guard<std::mutex> g(pinned->mu);
+        if (pinned->arena) {
+            const size_t need = (bytes + kArenaAlign - 1) & ~(kArenaAlign - 1);
+            if (void *p = pinned->arena_take(need)) {
+                b->ptr = p;
+                b->bytes = need;
+                b->in_arena = true;
+                return b;
+            }
+        }
         /* best fit: the smallest cached block of this class or up to two
          * classes larger (a block of 4x the request at most) */
-        std::lock_guard<std::mutex> g(pinned->mu);
         auto it = pinned->free.lower_bound(cls);
         if (it != pinned->free.end() && it->first <= 4 * cls) {
             b->ptr = it->second;
@@ -305,6 +362,7 @@ Context *create_context(int device, cudaMemPool_t shared_pool, std::shared_ptr<P
     c->opt.dense_keys = std::max<int64_t>(0, std::min<int64_t>(64, env_opt("CJ_DENSE_KEYS", c->opt.dense_keys)));
     c->opt.buffer_cache_bytes = std::max<int64_t>(0, env_opt("CJ_BUFFER_CACHE_BYTES", c->opt.buffer_cache_bytes));
     c->opt.inline_dir_max_bytes = std::max<int64_t>(0, env_opt("CJ_INLINE_DIR_MAX_BYTES", c->opt.inline_dir_max_bytes));
+    c->opt.defer_count = env_opt("CJ_DEFER_COUNT", c->opt.defer_count);
     if (shared_pool) c->opt.buffer_cache_bytes = 0; /* contexts sharing a pool share through it */
     if (const char *tf = std::getenv("CJ_TUNING_FILE"); tf && *tf) c->tuning = load_tuning_file(tf, c->num_sms);
     return c.release();

@@ -120,6 +120,26 @@ class Executor {
     std::map<std::pair<uint64_t, uint64_t>, Prefetched> prefetched;
     std::vector<PhaseEv> phase_events;
     cj_exec_stats stats{};
+    bool synced_last = false; /* the last thing enqueued was a synchronisation */
+    /* Brings the status block to the host, counting the synchronisation. */
+    void sync() {
+        ctx.sync_status();
+        stats.host_syncs++;
+    }
+    /* A result written with a device-side row count (materialize with
+     * rows_dev): its rows and pages once the count is known. */
+    void finish_counted(cj_result &r, uint64_t rows) {
+        r.num_rows = rows;
+        uint64_t pages = 0;
+        for (size_t c = 0; c < r.types.size(); ++c) {
+            const uint32_t R = rows_per_page_fixed(r.types[c]);
+            r.num_pages[c] = (rows + R - 1) / R;
+            if (!rows) r.dev_pages[c].reset();
+            pages += r.num_pages[c];
+        }
+        stats.output_rows = rows;
+        stats.output_pages = pages;
+    }
 
     const cj_table *resident(uint64_t t) const { return resident_input(plan, t); }
     uint64_t table_rows(uint64_t t) const { return input_rows(plan, t); }
@@ -140,8 +160,8 @@ class Executor {
         DevPtr pages; /* result pages written by the probe (no NULL) */
     };
     ColView out_view(const OutCol &oc) { return view(*oc.rel, oc.col, oc.rid_a); }
-    cj_result *materialize(const std::vector<OutCol> &cols, const std::vector<int32_t> &types,
-                           uint64_t rows);
+    cj_result *materialize(const std::vector<OutCol> &cols, const std::vector<int32_t> &types, uint64_t rows,
+                           const unsigned long long *rows_dev = nullptr);
     void ck(cudaError_t e, const char *what) { check_cuda(e, what); }
 };
 
@@ -329,6 +349,21 @@ Relation Executor::exec_join(uint64_t node_idx, int depth, bool is_root, cj_resu
     const bool collect = need_b || need_p || emit_keys;
     const int32_t key_bytes = pk.type == CJ_INT32 ? 4 : 8;
     DevPtr mb, mp, mk;
+    /* The root's result columns: the pages the probe wrote the keys into, or
+     * a relation column and the match row ids that select its rows. */
+    auto root_columns = [&](std::vector<OutCol> &cols, std::vector<int32_t> &types) {
+        for (auto &o : outs) {
+            OutCol oc{o.rel, o.col, nullptr, nullptr};
+            if (o.from_keys) {
+                oc.rel = nullptr;
+                oc.pages = mk; /* o.col.type == the probe key's type */
+            } else {
+                oc.rid_a = o.from_build ? (mb ? mb->as<uint32_t>() : nullptr) : (mp ? mp->as<uint32_t>() : nullptr);
+            }
+            cols.push_back(oc);
+            types.push_back(o.col.type);
+        }
+    };
     if (B.rows && P.rows) {
         const ColView bv = view(B, bk, nullptr);
         const ColView pv = view(P, pk, nullptr);
@@ -424,8 +459,9 @@ Relation Executor::exec_join(uint64_t node_idx, int depth, bool is_root, cj_resu
             }
             if (!direct) build_hash();
         }
-        uint64_t cap = P.rows;
-        for (;;) {
+        /* Allocates the match outputs for `cap` pairs and launches the probe
+         * of the table built above. */
+        auto launch_probe = [&](uint64_t cap) {
             mb = need_b ? ctx.alloc(cap * 4) : nullptr;
             mp = need_p ? ctx.alloc(cap * 4) : nullptr;
             /* the key columns' result pages, sized for the capacity */
@@ -464,17 +500,50 @@ Relation Executor::exec_join(uint64_t node_idx, int depth, bool is_root, cj_resu
                        "probe");
                 }
             }
-            ctx.sync_status();
+        };
+        /* keys too spread out (aux[3] = 1) or a key repeats (2): the
+         * direct-mapped table is unusable (its probe did nothing); an
+         * open-addressing table for spread-out keys, else the hash table */
+        auto replace_direct = [&]() {
+            direct = false;
+            slots.reset();
+            PhaseScope ph(*this, PH_BUILD);
+            open = ctx.h_status->aux[3] == 1 && build_open();
+            if (!open) build_hash();
+        };
+        uint64_t cap = P.rows;
+        bool all_fixed = true;
+        for (const auto &o : outs) all_fixed &= o.col.type != CJ_VARCHAR;
+        if (is_root && direct && collect && all_fixed && (flags & CJ_EXEC_RESULT_ON_DEVICE) && ctx.opt.defer_count) {
+            /* Unique build keys at the root, result left in HBM, no VARCHAR
+             * output: at most one match per probe row, so the result is sized
+             * for P.rows and its pages are written with the match count read
+             * on the device. The execution's one host synchronisation comes
+             * last; only if the device refused the direct-mapped table does
+             * the join go on as below. */
+            launch_probe(cap);
+            std::vector<OutCol> cols;
+            std::vector<int32_t> types;
+            root_columns(cols, types);
+            std::unique_ptr<cj_result> r(materialize(cols, types, cap, &ctx.d_status->counter));
+            sync();
+            if (!ctx.h_status->aux[3]) {
+                M = ctx.h_status->counter;
+                finish_counted(*r, M);
+                stats.num_direct_joins++;
+                stats.matches += M;
+                synced_last = true;
+                *out = r.release();
+                return Relation{};
+            }
+            r.reset();
+            replace_direct();
+        }
+        for (;;) {
+            launch_probe(cap);
+            sync();
             if (direct && ctx.h_status->aux[3]) {
-                /* keys too spread out (1) or a key repeats (2): the
-                 * direct-mapped table is unusable (the probe did nothing);
-                 * an open-addressing table for spread-out keys, else the
-                 * hash table */
-                direct = false;
-                slots.reset();
-                PhaseScope ph(*this, PH_BUILD);
-                open = ctx.h_status->aux[3] == 1 && build_open();
-                if (!open) build_hash();
+                replace_direct();
                 continue;
             }
             if (open && ctx.h_status->aux[kOpenDup]) {
@@ -500,17 +569,7 @@ Relation Executor::exec_join(uint64_t node_idx, int depth, bool is_root, cj_resu
     if (is_root) {
         std::vector<OutCol> cols;
         std::vector<int32_t> types;
-        for (auto &o : outs) {
-            OutCol oc{o.rel, o.col, nullptr, nullptr};
-            if (o.from_keys) {
-                oc.rel = nullptr;
-                oc.pages = mk; /* o.col.type == the probe key's type */
-            } else {
-                oc.rid_a = o.from_build ? (mb ? mb->as<uint32_t>() : nullptr) : (mp ? mp->as<uint32_t>() : nullptr);
-            }
-            cols.push_back(oc);
-            types.push_back(o.col.type);
-        }
+        root_columns(cols, types);
         *out = materialize(cols, types, M);
         return Relation{};
     }
@@ -554,7 +613,7 @@ Relation Executor::exec_join(uint64_t node_idx, int depth, bool is_root, cj_resu
  * go down on the context's download stream as soon as its writer is done,
  * so the copy of one column overlaps the writing of the next. */
 cj_result *Executor::materialize(const std::vector<OutCol> &cols, const std::vector<int32_t> &types,
-                                 uint64_t rows) {
+                                 uint64_t rows, const unsigned long long *rows_dev) {
     auto *res = new cj_result;
     std::unique_ptr<cj_result> guard(res);
     res->ctx = &ctx;
@@ -565,6 +624,14 @@ cj_result *Executor::materialize(const std::vector<OutCol> &cols, const std::vec
     res->dev_pages.resize(nc);
     res->host_cols.assign(nc, nullptr);
     const bool to_host = !(flags & CJ_EXEC_RESULT_ON_DEVICE);
+    if (rows_dev) {
+        /* rows is a capacity and the count is on the device: fixed-width
+         * columns left in HBM only (their pages do not depend on the count
+         * beyond the last one) */
+        for (int32_t t : types)
+            if (t == CJ_VARCHAR) fail(CJ_ERR_INTERNAL, "device-counted result with a VARCHAR column");
+        if (to_host) fail(CJ_ERR_INTERNAL, "device-counted result for the host");
+    }
     /* Orders the kernel stream (and so every later free) after the copies
      * issued so far, also when an error leaves this scope early. */
     struct DownloadJoin {
@@ -607,7 +674,7 @@ cj_result *Executor::materialize(const std::vector<OutCol> &cols, const std::vec
             }
             std::vector<unsigned long long> host(nvar);
             ck(cudaMemcpyAsync(host.data(), totals->ptr, nvar * 8, cudaMemcpyDeviceToHost, ctx.stream), "copy");
-            ctx.sync_status();
+            sync();
             k = 0;
             for (size_t c = 0; c < nc; ++c)
                 if (types[c] == CJ_VARCHAR) res->num_pages[c] = host[k++];
@@ -651,7 +718,8 @@ cj_result *Executor::materialize(const std::vector<OutCol> &cols, const std::vec
                 res->dev_pages[c] = cols[c].pages;
                 if (alias[c] < 0) {
                     KScope ks(*this, "finish_pages");
-                    ck(launch_finish_dense_pages(L, cols[c].pages->as<uint8_t>(), rows, types[c]), "finish_pages");
+                    ck(launch_finish_dense_pages(L, cols[c].pages->as<uint8_t>(), rows, types[c], rows_dev),
+                       "finish_pages");
                 }
             } else {
                 /* decoded here, not before the loop: the kernel stream waits
@@ -660,7 +728,8 @@ cj_result *Executor::materialize(const std::vector<OutCol> &cols, const std::vec
                 res->dev_pages[c] = ctx.alloc(res->num_pages[c] * kPageSize);
                 if (types[c] != CJ_VARCHAR) {
                     KScope ks(*this, types[c] == CJ_INT32 ? "write_pages_int32" : "write_pages_8byte");
-                    ck(launch_write_fixed_pages(L, cv, rows, res->dev_pages[c]->as<uint8_t>()), "write_fixed");
+                    ck(launch_write_fixed_pages(L, cv, rows, res->dev_pages[c]->as<uint8_t>(), rows_dev),
+                       "write_fixed");
                 } else {
                     KScope ks(*this, "varchar_write");
                     ck(launch_varchar_write(L, cv, rows, TR, vtemp[c]->ptr, res->dev_pages[c]->as<uint8_t>()),
@@ -716,7 +785,7 @@ cj_result *Executor::run(cj_exec_stats *st) {
         exec_join(plan.root, 0, true, &res);
     }
     std::unique_ptr<cj_result> guard(res);
-    ctx.sync_status();
+    if (!synced_last) sync();
     double ph_us[PH_COUNT] = {0};
     for (auto &pe : phase_events) {
         float ms = 0;

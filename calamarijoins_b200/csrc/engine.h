@@ -53,6 +53,10 @@ struct Options {
      * its entry; larger ones use 8-byte entries, so that more of the table
      * stays in L2 (environment CJ_INLINE_DIR_MAX_BYTES) */
     int64_t inline_dir_max_bytes = 256ll << 20;
+    /* a root over unique build keys with its result left in HBM writes the
+     * result with the match count read on the device, without a host
+     * synchronisation after the probe (environment CJ_DEFER_COUNT=0: off) */
+    int64_t defer_count = 1;
 };
 
 struct Context;
@@ -77,6 +81,16 @@ struct PinnedPool {
     std::multimap<size_t, void *> free;
     std::mutex mu;
     std::atomic<uint64_t> host_allocs{0}, host_alloc_bytes{0}; /* cudaHostAlloc calls made */
+    /* Optional arena reserved up front (a server's host_cache_bytes):
+     * blocks are carved from it first fit, and freed ranges merge with
+     * their neighbours, so any mix of sizes is served without allocating
+     * while it has room. */
+    uint8_t *arena = nullptr;
+    size_t arena_bytes = 0;
+    std::map<size_t, size_t> arena_free; /* offset -> length */
+    void reserve(size_t bytes);          /* throws Error */
+    void *arena_take(size_t bytes);      /* mu held; nullptr when no range fits */
+    void arena_give(void *p, size_t bytes); /* mu held */
     ~PinnedPool();
 };
 
@@ -85,6 +99,7 @@ struct PinnedBlock {
     std::shared_ptr<PinnedPool> pool;
     void *ptr = nullptr;
     size_t bytes = 0;
+    bool in_arena = false;
     ~PinnedBlock();
 };
 using PinnedPtr = std::shared_ptr<PinnedBlock>;

@@ -198,10 +198,22 @@ CJ_DEV void zero_page(PageSmem &sm) {
     __syncthreads();
 }
 
+/* Rows to write: `rows`, or, when `rows_dev` is set, the count it holds
+ * (at most `rows`, the capacity the pages were sized for). */
+CJ_DEV uint64_t live_rows(uint64_t rows, const unsigned long long *rows_dev) {
+    if (!rows_dev) return rows;
+    const uint64_t n = *rows_dev;
+    return n < rows ? n : rows;
+}
+
 template <typename T>
 __global__ void __launch_bounds__(kMatThreads, kMatMinBlocks)
-    k_write_fixed(ColView col, uint64_t rows, uint32_t R, uint64_t num_pages, uint8_t *__restrict__ out) {
+    k_write_fixed(ColView col, uint64_t rows, const unsigned long long *rows_dev, uint32_t R,
+                  uint8_t *__restrict__ out) {
     __shared__ PageSmem sm;
+    rows = live_rows(rows, rows_dev);
+    const uint64_t num_pages = (rows + R - 1) / R;
+    if (blockIdx.x >= num_pages) return;
     zero_page(sm);
     for (uint64_t pg = blockIdx.x; pg < num_pages; pg += gridDim.x) write_fixed_page<T>(col, rows, R, pg, out, sm);
 }
@@ -209,9 +221,11 @@ __global__ void __launch_bounds__(kMatThreads, kMatMinBlocks)
 /* Finishes pages whose values are in place (a NULL-free column written by
  * the probe): header, zero gap after the values, bitmap of nr ones. */
 template <typename T>
-__global__ void k_finish_dense_pages(uint8_t *__restrict__ pages, uint64_t rows, uint64_t num_pages) {
+__global__ void k_finish_dense_pages(uint8_t *__restrict__ pages, uint64_t rows, const unsigned long long *rows_dev) {
     constexpr uint32_t R = sizeof(T) == 4 ? kRowsPerPageInt32 : kRowsPerPage8B;
     constexpr uint32_t DB = sizeof(T) == 4 ? 4u : 8u;
+    rows = live_rows(rows, rows_dev);
+    const uint64_t num_pages = (rows + R - 1) / R;
     for (uint64_t pg = blockIdx.x; pg < num_pages; pg += gridDim.x) {
         uint8_t *dst = pages + pg * kPageSize;
         const uint32_t nr = (uint32_t)min((uint64_t)R, rows - pg * R);
@@ -530,29 +544,30 @@ uint32_t rows_per_page_fixed(int32_t type) {
 }
 
 cudaError_t launch_write_fixed_pages(const Launch &L, const ColView &col, uint64_t rows,
-                                     uint8_t *out) {
+                                     uint8_t *out, const unsigned long long *rows_dev) {
     if (rows == 0) return cudaSuccess;
     const uint32_t R = rows_per_page_fixed(col.type);
     const uint64_t np = (rows + R - 1) / R;
     uint64_t g = np, cap = (uint64_t)L.num_sms * kMatMinBlocks;
     if (g > cap) g = cap;
     if (col.type == CJ_INT32) {
-        k_write_fixed<int32_t><<<(unsigned)g, kMatThreads, 0, L.stream>>>(col, rows, R, np, out);
+        k_write_fixed<int32_t><<<(unsigned)g, kMatThreads, 0, L.stream>>>(col, rows, rows_dev, R, out);
         count_launches(1);
     } else {
-        k_write_fixed<long long><<<(unsigned)g, kMatThreads, 0, L.stream>>>(col, rows, R, np, out);
+        k_write_fixed<long long><<<(unsigned)g, kMatThreads, 0, L.stream>>>(col, rows, rows_dev, R, out);
         count_launches(1);
     }
     return cudaGetLastError();
 }
 
-cudaError_t launch_finish_dense_pages(const Launch &L, uint8_t *pages, uint64_t rows, int32_t type) {
+cudaError_t launch_finish_dense_pages(const Launch &L, uint8_t *pages, uint64_t rows, int32_t type,
+                                      const unsigned long long *rows_dev) {
     if (rows == 0) return cudaSuccess;
     const uint32_t R = rows_per_page_fixed(type);
     const uint64_t np = (rows + R - 1) / R;
     const unsigned g = (unsigned)std::min<uint64_t>(np, (uint64_t)L.num_sms * 8);
-    if (type == CJ_INT32) k_finish_dense_pages<int32_t><<<g, 128, 0, L.stream>>>(pages, rows, np);
-    else k_finish_dense_pages<long long><<<g, 128, 0, L.stream>>>(pages, rows, np);
+    if (type == CJ_INT32) k_finish_dense_pages<int32_t><<<g, 128, 0, L.stream>>>(pages, rows, rows_dev);
+    else k_finish_dense_pages<long long><<<g, 128, 0, L.stream>>>(pages, rows, rows_dev);
     count_launches(1);
     return cudaGetLastError();
 }

@@ -320,6 +320,7 @@ int cj_server_create(const cj_server_config *cfg, cj_server **out) {
         s->budget = cfg->memory_budget ? cfg->memory_budget : (uint64_t)(free_b * 0.85);
         const uint32_t slots = cfg->slots ? cfg->slots : 4;
         s->pinned = std::make_shared<cj::PinnedPool>(); /* one cache of result blocks for all workers */
+        if (cfg->host_cache_bytes) s->pinned->reserve(cfg->host_cache_bytes);
         for (uint32_t w = 0; w < slots; ++w) s->workers.emplace_back(cj::create_context(dev, s->pool, s->pinned));
     } catch (const cj::Error &e) {
         for (auto &w : s->workers) w.reset();

@@ -168,6 +168,12 @@ typedef struct cj_exec_stats {
     uint64_t num_open_joins;   /* hash joins served by an open-addressing
                                   table (unique INT32 keys too spread out for
                                   a direct-mapped one); within num_hash_joins */
+    uint64_t host_syncs;       /* times the host waited for the device: one
+                                  per join (its match count), one per VARCHAR
+                                  result (its page counts) and the last; a
+                                  root over unique build keys whose result
+                                  stays in HBM (CJ_EXEC_RESULT_ON_DEVICE, no
+                                  VARCHAR column) needs only the last */
 } cj_exec_stats;
 
 /* ------------------------------------------------------------------------ */
@@ -530,6 +536,11 @@ typedef struct cj_server_config {
                                 admit later plans that do, for at most this
                                 long after its submission; then it goes
                                 first; 0 = 20,000                            */
+    uint64_t host_cache_bytes; /* page-locked host memory reserved at creation
+                                for host results, which are carved from it
+                                (any mix of sizes, no allocation while it has
+                                room); 0 = none: blocks are allocated as
+                                needed and cached by size for reuse          */
 } cj_server_config;
 
 typedef struct cj_server_stats {

@@ -384,6 +384,38 @@ def test_result_on_device(gpu_ctx):
     assert_same(r, run_oracle(plan))
 
 
+@pytest.mark.parametrize("case", ["direct", "empty", "varchar", "dups", "probe_side_only"])
+def test_device_counted_result(gpu_ctx, case):
+    """A root over unique build keys whose result stays in HBM is written
+    with the match count read on the device (result sized for the probe
+    rows): one host synchronisation in the whole execution. A VARCHAR output
+    or a table the device refuses (a repeated key) takes the counted path.
+    Both give the oracle's result, with host and with device results."""
+    kw = dict(build_payload=(L, F), probe_payload=(F, I), outside=0.3, probe_null=0.05)
+    if case == "empty":
+        kw["outside"] = 1.0
+    if case == "varchar":
+        kw["probe_payload"] = (F, V)
+    if case == "dups":
+        kw["unique_build"] = False
+    if case == "probe_side_only":
+        kw["output"] = [3, 4]  # probe key and probe FP64: no build row ids
+    plan = join2(40_000, 250_000, seed=17, **kw)
+    want = run_oracle(plan)
+    if case == "empty":
+        assert want.num_rows == 0
+    for flags in (0, _lib.CJ_EXEC_RESULT_ON_DEVICE):
+        got, st = run_product(plan, gpu_ctx, flags)
+        assert_same(got, want, f"{case} flags={flags}")
+        assert st.exec["output_rows"] == want.num_rows
+        deferred = flags and case in ("direct", "empty", "probe_side_only")
+        assert st.exec["num_direct_joins"] == (0 if case == "dups" else 1)
+        if deferred:
+            assert st.exec["host_syncs"] == 1
+        else:
+            assert st.exec["host_syncs"] >= 2
+
+
 def test_malformed_pages_rejected(gpu_ctx):
     plan = join2(3000, 3000, seed=7)
     bad = plan.inputs[1].columns[0].pages.copy()

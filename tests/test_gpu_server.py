@@ -133,3 +133,32 @@ def test_admission_passes_over_a_plan_that_does_not_fit():
         srv.close()
     assert st["skipped_ahead"] >= 1, st
     assert st["peak_admitted_bytes"] <= st["memory_budget"]
+
+
+@pytest.mark.parametrize("cache_mb", [0, 64, 1024])
+def test_reserved_host_cache(gpu_ctx, cache_mb):
+    """Host results carved from a page-locked cache reserved at creation:
+    results held at once, freed out of order and re-used by later plans of
+    other sizes, each equal to the plan run alone. A cache too small for
+    the results held at once (64 MB) falls back to allocating blocks; a
+    large one (1 GB) serves them all without another allocation."""
+    plans = mixed_plans(30, seed=9)
+    alone = [run_product(p, gpu_ctx)[0] for p in plans]
+    srv = Server(slots=4, max_batch=8, host_cache_bytes=cache_mb << 20)
+    try:
+        st0 = srv.stats(reset=True)
+        assert st0["pinned_allocs"] == (1 if cache_mb else 0)  # the reservation itself
+        for rnd in range(2):
+            tickets = [srv.submit(p) for p in plans]
+            results = [srv.wait(t)[0] for t in tickets]
+            got = [oa.PagedResult.from_result(r) for r in results]
+            for r in results[1::2] + results[0::2]:  # freed out of order
+                r.free()
+            for i, (g, a) in enumerate(zip(got, alone)):
+                assert_same(g, a, f"round {rnd} plan {i} cache {cache_mb} MB")
+        st = srv.stats()
+    finally:
+        srv.close()
+    assert st["completed"] == 2 * len(plans) and st["failed"] == 0
+    if cache_mb >= 1024:
+        assert st["pinned_allocs"] == 0
