@@ -394,7 +394,7 @@ Relation Executor::exec_join(uint64_t node_idx, int depth, bool is_root, cj_resu
          * join on to the hash table. */
         auto build_open = [&]() -> bool {
             if (bk.type != CJ_INT32 || B.rows > kOpenMaxRows) return false;
-            open_n = std::max<uint64_t>(2 * B.rows, 1024);
+            open_n = (std::max<uint64_t>(2 * B.rows, 1024) + 3) & ~3ull; /* groups of 4 slots */
             open_slots = ctx.alloc(open_n * 8);
             ck(cudaMemsetAsync(d_params + kOpenDup, 0, 8, ctx.stream), "memset");
             KScope k(*this, "open_build");

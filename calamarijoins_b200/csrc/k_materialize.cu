@@ -46,19 +46,6 @@ __global__ void k_gather_u32(const uint32_t *__restrict__ src, const uint32_t *_
         out[i] = __ldg(src + __ldcs(idx + i));
 }
 
-/* Warp-0 exclusive scan of the per-warp counts in s_warp; total lands in
- * s_warp[nwarps]. Caller brackets with __syncthreads(). */
-CJ_DEV void scan_warp_counts(uint32_t *s_warp) {
-    const int nwarps = kMatThreads / 32;
-    if ((threadIdx.x >> 5) == 0) {
-        uint32_t lane = lane_id();
-        uint32_t w = lane < (uint32_t)nwarps ? s_warp[lane] : 0u;
-        uint32_t wi = warp_inclusive_scan(w);
-        if (lane < (uint32_t)nwarps) s_warp[lane] = wi - w;
-        if (lane == 31) s_warp[nwarps] = wi;
-    }
-}
-
 constexpr int kMatMinBlocks = 8; /* page writers: 8 x 256 threads per SM */
 
 struct PageSmem {

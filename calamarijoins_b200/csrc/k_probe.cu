@@ -251,14 +251,19 @@ template <int kItemsT> struct ArrayMatcherT {
 using ArrayMatcher = ArrayMatcherT<4>;
 
 /* Open-addressing table of unique INT32 keys (launch_open_build): walk the
- * slots from the key's hash until the key or an empty slot. */
+ * slots from the key's hash until the key or an empty slot. The walk reads
+ * the aligned group of four slots (one 32-byte sector) around its position
+ * with two independent 16-byte loads and examines the group's slots from
+ * there on, so most rows are answered by one round trip instead of one per
+ * slot (the slot count is a multiple of 4: a group never runs past the
+ * end). */
 struct OpenMatcher {
     static constexpr bool kAtMostOne = true; /* unique keys */
     static constexpr bool kHeavy = false;
     static constexpr int kItems = 4;
     static constexpr int kMinBlocks = kProbeMinBlocks;
     const unsigned long long *slots;
-    uint32_t nslots; /* < 2^32 (launch_probe_tiles_open checks) */
+    uint32_t nslots; /* < 2^32 and a multiple of 4 (launch_probe_tiles_open checks) */
     const unsigned long long *dup;
     struct Shared {
         uint32_t unused;
@@ -268,15 +273,25 @@ struct OpenMatcher {
     CJ_DEV void init(Shared &) const {}
     CJ_DEV uint32_t count(const Shared &, int64_t key, uint32_t &first) const {
         if (key != (int64_t)(int32_t)key) return 0; /* no INT32 build key equals it */
+        const uint32_t k32 = (uint32_t)(int32_t)key;
         uint32_t h = open_slot(key, nslots);
-        for (uint32_t step = 0; step < nslots; ++step) {
-            const unsigned long long v = __ldg(slots + h);
-            if (v == ~0ull) return 0;
-            if ((int32_t)(uint32_t)(v >> 32) == (int32_t)key) {
-                first = (uint32_t)v;
-                return 1;
+        for (uint32_t step = 0; step < nslots;) {
+            const uint32_t g0 = h & ~3u;
+            const ulonglong2 *grp = reinterpret_cast<const ulonglong2 *>(slots + g0);
+            const ulonglong2 a = __ldg(grp), b = __ldg(grp + 1);
+#pragma unroll
+            for (uint32_t q = 0; q < 4; ++q) {
+                if (q < (h & 3u)) continue;
+                const unsigned long long v = q == 0 ? a.x : q == 1 ? a.y : q == 2 ? b.x : b.y;
+                if (v == ~0ull) return 0;
+                if ((uint32_t)(v >> 32) == k32) {
+                    first = (uint32_t)v;
+                    return 1;
+                }
+                ++step;
             }
-            if (++h == nslots) h = 0;
+            h = g0 + 4;
+            if (h >= nslots) h = 0;
         }
         return 0;
     }
@@ -632,7 +647,7 @@ cudaError_t launch_probe_tiles_array(const Launch &L, const ColView &pkey, uint3
 cudaError_t launch_probe_tiles_open(const Launch &L, const ColView &pkey, uint32_t n_probe,
                                     const unsigned long long *slots, uint64_t nslots,
                                     const unsigned long long *dup, const MatchOut &out, void *sched_mem) {
-    if (nslots > 0xFFFFFFFFull) return cudaErrorInvalidValue;
+    if (nslots > 0xFFFFFFFFull || nslots % 4 || reinterpret_cast<uintptr_t>(slots) % 16) return cudaErrorInvalidValue;
     OpenMatcher m{slots, (uint32_t)nslots, dup};
     return run_tiles(L, pkey, n_probe, m, out, sched_mem);
 }
