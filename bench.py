@@ -823,23 +823,31 @@ def run_serve(args):
                 "rejected": st["rejected"], "peak_admitted_gb": st["peak_admitted_bytes"] / 1e9,
                 "batches": st["batches"], "mean_batch": st["mean_batch"], "skipped_ahead": st["skipped_ahead"],
                 "batch_fallbacks": st["batch_fallbacks"], "pinned_allocs": st["pinned_allocs"],
-                "pinned_alloc_mb": st["pinned_alloc_bytes"] / 1e6}
+                "pinned_alloc_mb": st["pinned_alloc_bytes"] / 1e6, "pool_high_gb": st["pool_high_bytes"] / 1e9}
+
+    # device time of one execution: the sum of its phases' event intervals
+    # on the kernel stream (an upper bound of the GPU's busy time for it)
+    DEVICE_PHASES = ("decode_us", "build_us", "probe_us", "nested_loop_us", "intermediate_us", "materialize_us")
 
     def plain(ctx, arrivals, order, flags):
         lat = []
+        dev_us = []
         t0 = time.perf_counter()
         last = t0
         for at, k in zip(arrivals, order):
             d = at - (time.perf_counter() - t0)
             if d > 0:
                 time.sleep(d)
-            r, _ = cj.execute_raw(pool[k], ctx, flags, descs[k])
+            r, st_p = cj.execute_raw(pool[k], ctx, flags, descs[k])
             r.free()
             last = time.perf_counter()
             lat.append((last - t0) - at)
+            dev_us.append(sum(st_p.exec[n] for n in DEVICE_PHASES))
         wall = last - (t0 + arrivals[0])
+        dev_ms = statistics.mean(dev_us) / 1e3
         return {"plans_per_s": len(lat) / wall, "p50_ms": pct(lat, 0.5) * 1e3, "p99_ms": pct(lat, 0.99) * 1e3,
-                "mean_ms": statistics.mean(lat) * 1e3, "max_ms": max(lat) * 1e3}
+                "mean_ms": statistics.mean(lat) * 1e3, "max_ms": max(lat) * 1e3,
+                "device_ms_per_plan": dev_ms, "device_bound_plans_per_s": 1e3 / dev_ms if dev_ms else None}
 
     from calamarijoins_b200 import _lib
     modes = {"host": 0, "device": _lib.CJ_EXEC_RESULT_ON_DEVICE}
@@ -848,7 +856,7 @@ def run_serve(args):
     try:
         for mode, flags in modes.items():
             srv = cj.Server(device=0, slots=4, memory_budget=150 << 30, flags=flags,
-                            host_cache_bytes=(8 << 30) if mode == "host" else 0)
+                            host_cache_bytes=(8 << 30) if mode == "host" else 0, device_reserve_bytes=100 << 30)
             try:
                 log(f"{mode} results: warm-up")
                 for _ in range(2):  # every worker sees plans of every size: pinned and pool blocks exist
@@ -900,13 +908,15 @@ def run_serve(args):
                                     "base tables resident in HBM, results to host memory; Poisson arrivals, each "
                                     "plan drawn from the pool; served: "
                                     "4 worker streams, 150 GB admission budget, continuous batching, 8 GB "
-                                    "page-locked result cache reserved at creation; plain: "
+                                    "page-locked result cache and 100 GB of device pool reserved at creation; plain: "
                                     "cj_execute one plan at a time in arrival order"), "scale": args.scale,
                        "probe_rows": {"min": min(probe_rows), "max": max(probe_rows)}},
             "rates": per_rate,
             "plain_best_plans_per_s": plain_best,
             "served_over_plain_at_saturation": best["served"]["plans_per_s"] / plain_best,
             "result_mb_per_plan": mean_mb,
+            "device_ms_per_plan": statistics.mean(x["plain"]["device_ms_per_plan"] for x in per_rate),
+            "device_bound_plans_per_s": 1e3 / statistics.mean(x["plain"]["device_ms_per_plan"] for x in per_rate),
             "result_download_gbs_at_best": mean_mb * best["served"]["plans_per_s"] / 1e3,
             "device_results": {"rates": per_mode["device"], **summary(per_mode["device"]),
                                "note": "the same trace with results left in HBM (CJ_EXEC_RESULT_ON_DEVICE) in "

@@ -106,7 +106,7 @@ class BatchStatsC(C.Structure):
 class ServerConfigC(C.Structure):
     _fields_ = [("device", C.c_int32), ("slots", C.c_uint32), ("memory_budget", C.c_uint64),
                 ("exec_flags", C.c_uint32), ("max_batch", C.c_uint32), ("age_limit_us", C.c_uint64),
-                ("host_cache_bytes", C.c_uint64)]
+                ("host_cache_bytes", C.c_uint64), ("device_reserve_bytes", C.c_uint64)]
 
 
 class ServerStatsC(C.Structure):
@@ -115,7 +115,8 @@ class ServerStatsC(C.Structure):
         "peak_admitted_bytes", "memory_budget")]
         + [(n, C.c_double) for n in ("p50_us", "p99_us", "mean_us", "max_us", "wall_s", "plans_per_s")]
         + [("batches", C.c_uint64), ("skipped_ahead", C.c_uint64), ("mean_batch", C.c_double),
-           ("batch_fallbacks", C.c_uint64), ("pinned_allocs", C.c_uint64), ("pinned_alloc_bytes", C.c_uint64)])
+           ("batch_fallbacks", C.c_uint64), ("pinned_allocs", C.c_uint64), ("pinned_alloc_bytes", C.c_uint64),
+           ("pool_high_bytes", C.c_uint64)])
 
 
 # every function of include/cj_b200.h: name -> (restype, argtypes)

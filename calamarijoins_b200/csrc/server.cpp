@@ -322,6 +322,21 @@ int cj_server_create(const cj_server_config *cfg, cj_server **out) {
         s->pinned = std::make_shared<cj::PinnedPool>(); /* one cache of result blocks for all workers */
         if (cfg->host_cache_bytes) s->pinned->reserve(cfg->host_cache_bytes);
         for (uint32_t w = 0; w < slots; ++w) s->workers.emplace_back(cj::create_context(dev, s->pool, s->pinned));
+        if (cfg->device_reserve_bytes) {
+            /* one block of the requested size, freed at once: the pool keeps
+             * the memory (release threshold = keep) and later allocations are
+             * carved from it */
+            const cudaStream_t st = s->workers[0]->stream;
+            void *p = nullptr;
+            cudaError_t e = cudaMallocFromPoolAsync(&p, cfg->device_reserve_bytes, s->pool, st);
+            if (e != cudaSuccess) {
+                cudaGetLastError();
+                cj::fail(CJ_ERR_OUT_OF_MEMORY,
+                         "device reserve of " + std::to_string(cfg->device_reserve_bytes) + " bytes failed");
+            }
+            cj::check_cuda(cudaFreeAsync(p, st), "cudaFreeAsync");
+            cj::check_cuda(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+        }
     } catch (const cj::Error &e) {
         for (auto &w : s->workers) w.reset();
         if (s->pool) cudaMemPoolDestroy(s->pool);
@@ -425,9 +440,14 @@ int cj_server_get_stats(cj_server *s, cj_server_stats *out, int reset) {
     const cj::PinnedPool &pp = *s->pinned;
     st.pinned_allocs = pp.host_allocs.load() - s->pinned_allocs0;
     st.pinned_alloc_bytes = pp.host_alloc_bytes.load() - s->pinned_bytes0;
+    uint64_t high = 0; /* the attribute is a 64-bit unsigned value */
+    if (cudaMemPoolGetAttribute(s->pool, cudaMemPoolAttrReservedMemHigh, &high) != cudaSuccess) cudaGetLastError();
+    st.pool_high_bytes = high;
     *out = st;
     if (reset) {
         s->pinned_allocs0 = pp.host_allocs.load();
+        uint64_t zero = 0; /* restarts the pool's high-water mark */
+        if (cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReservedMemHigh, &zero) != cudaSuccess) cudaGetLastError();
         s->pinned_bytes0 = pp.host_alloc_bytes.load();
         s->latencies.clear();
         s->completed = s->failed = s->rejected = s->cancelled = s->submitted = 0;

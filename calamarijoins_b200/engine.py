@@ -388,12 +388,14 @@ class Server:
     worker that frees up takes up to `max_batch` queued plans that fit and
     runs them as one grouped execution (continuous batching). Host results
     are carved from `host_cache_bytes` of page-locked memory reserved at
-    creation, when given."""
+    creation, when given; `device_reserve_bytes` pre-grows the server's
+    device memory pool."""
 
     def __init__(self, device: int = -1, slots: int = 4, memory_budget: int = 0, flags: int = 0,
-                 max_batch: int = 0, age_limit_us: int = 0, host_cache_bytes: int = 0):
+                 max_batch: int = 0, age_limit_us: int = 0, host_cache_bytes: int = 0,
+                 device_reserve_bytes: int = 0):
         cfg = _lib.ServerConfigC(int(device), int(slots), int(memory_budget), int(flags), int(max_batch),
-                                 int(age_limit_us), int(host_cache_bytes))
+                                 int(age_limit_us), int(host_cache_bytes), int(device_reserve_bytes))
         h = C.c_void_p()
         check(lib().cj_server_create(C.byref(cfg), C.byref(h)))
         self.handle = h.value

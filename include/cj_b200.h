@@ -541,6 +541,11 @@ typedef struct cj_server_config {
                                 (any mix of sizes, no allocation while it has
                                 room); 0 = none: blocks are allocated as
                                 needed and cached by size for reuse          */
+    uint64_t device_reserve_bytes; /* device memory the server's pool takes at
+                                creation and keeps, so that the first large
+                                batches do not wait for the pool to grow
+                                (mapping new memory is slow); 0 = the pool
+                                grows on demand                              */
 } cj_server_config;
 
 typedef struct cj_server_stats {
@@ -562,6 +567,9 @@ typedef struct cj_server_stats {
                                                allocated for results (the
                                                rest came from the cache)    */
     uint64_t pinned_alloc_bytes;
+    uint64_t pool_high_bytes;               /* most device memory the server's
+                                               pool has held (since creation
+                                               or the last reset)          */
 } cj_server_stats;
 
 int cj_server_create(const cj_server_config *config, cj_server **out);

@@ -162,3 +162,22 @@ def test_reserved_host_cache(gpu_ctx, cache_mb):
     assert st["completed"] == 2 * len(plans) and st["failed"] == 0
     if cache_mb >= 1024:
         assert st["pinned_allocs"] == 0
+
+
+def test_device_reserve(gpu_ctx):
+    """A server whose pool takes 2 GB at creation holds at least that much
+    from the start and runs plans as usual; the results equal the plans run
+    alone."""
+    plans = mixed_plans(8, seed=12)
+    alone = [run_product(p, gpu_ctx)[0] for p in plans]
+    srv = Server(slots=2, device_reserve_bytes=2 << 30)
+    try:
+        assert srv.stats()["pool_high_bytes"] >= 2 << 30
+        tickets = [srv.submit(p) for p in plans]
+        for i, (t, a) in enumerate(zip(tickets, alone)):
+            r, _ = srv.wait(t)
+            got = oa.PagedResult.from_result(r)
+            r.free()
+            assert_same(got, a, f"plan {i}")
+    finally:
+        srv.close()
