@@ -855,7 +855,8 @@ def run_serve(args):
     result_bytes = []
     try:
         for mode, flags in modes.items():
-            srv = cj.Server(device=0, slots=4, memory_budget=150 << 30, flags=flags,
+            srv = cj.Server(device=0, slots=args.c5_slots, memory_budget=150 << 30, flags=flags,
+                            max_batch=args.c5_max_batch,
                             host_cache_bytes=(8 << 30) if mode == "host" else 0, device_reserve_bytes=100 << 30)
             try:
                 log(f"{mode} results: warm-up")
@@ -907,7 +908,8 @@ def run_serve(args):
                                     "10 % VARCHAR outputs, probes log-uniform 1e4-1e7 rows, dimensions 10-1e6 rows, "
                                     "base tables resident in HBM, results to host memory; Poisson arrivals, each "
                                     "plan drawn from the pool; served: "
-                                    "4 worker streams, 150 GB admission budget, continuous batching, 8 GB "
+                                    f"{args.c5_slots} worker streams, 150 GB admission budget, continuous batching "
+                                    f"(at most {args.c5_max_batch} plans per grouped execution), 8 GB "
                                     "page-locked result cache and 100 GB of device pool reserved at creation; plain: "
                                     "cj_execute one plan at a time in arrival order"), "scale": args.scale,
                        "probe_rows": {"min": min(probe_rows), "max": max(probe_rows)}},
@@ -939,6 +941,8 @@ def main(argv=None):
     ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (kernel defaults)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-worker", type=int, default=0, help=argparse.SUPPRESS)
+    ap.add_argument("--c5-slots", type=int, default=4, help="c5: the server's worker streams")
+    ap.add_argument("--c5-max-batch", type=int, default=32, help="c5: plans per grouped execution, at most")
     ap.add_argument("--workload", choices=["c2", "c1", "c2s", "c2h", "c3", "c4", "c5"], default="c2",
                     help="c2 (default): the headline line; the others: see the module docstring")
     args = ap.parse_args(argv)
