@@ -48,7 +48,13 @@ namespace {
 #endif
 constexpr int kProbeThreads = 256;
 constexpr int kProbeItems = CJ_PROBE_ITEMS; /* rows per thread (hash, nested loop)      */
-constexpr uint32_t kTileRows = kProbeThreads * kProbeItems; /* grouped kernel's tile */
+/* The grouped kernel's tile: four rows per thread. A usable direct-mapped
+ * table probes it at once (ArrayMatcherT<4>, one light chain per row); hash
+ * tables and nested loops probe it as two halves of kProbeItems rows per
+ * thread, as their own kernels do. */
+constexpr int kGroupedItems = 4;
+constexpr uint32_t kTileRows = kProbeThreads * kGroupedItems;
+static_assert(kGroupedItems == 2 * kProbeItems, "a grouped tile is two hash / nested-loop tiles");
 constexpr int kProbeMinBlocks = CJ_PROBE_MIN_BLOCKS; /* 8 x 256 threads = 64 warps/SM */
 
 struct TileSched {
@@ -500,9 +506,10 @@ __global__ void __launch_bounds__(kProbeThreads, CJ_GROUPED_MIN_BLOCKS)
     k_probe_grouped(const ProbeTask *__restrict__ tasks, uint32_t ntasks, uint32_t total_tiles,
                     unsigned int *ticket, const uint16_t *__restrict__ g_bloom) {
     __shared__ GroupedShared sh;
-    __shared__ ProbeSmemT<kProbeItems> ps;
+    __shared__ ProbeSmemT<kProbeItems> ps;   /* ticket, task, and the halves' row state */
+    __shared__ ProbeSmemT<kGroupedItems> pw; /* row state of a whole-tile direct probe   */
     static_assert(HashMatcher<int32_t>::kItems == kProbeItems && LoopMatcher::kItems == kProbeItems,
-                  "the grouped kernel's tiles have kTileRows rows");
+                  "hash and nested-loop tasks probe half tiles");
     __shared__ uint32_t loaded_task;
     if (threadIdx.x == 0) loaded_task = 0xffffffffu;
     load_bloom(sh.h.bloom, g_bloom);
@@ -528,9 +535,9 @@ __global__ void __launch_bounds__(kProbeThreads, CJ_GROUPED_MIN_BLOCKS)
         if (T.kind == 2 && T.params[3] == 0ull) {
             /* a direct-mapped table the build found usable (unique keys
              * over a dense range); otherwise the task's hash table below */
-            const ArrayMatcherT<kProbeItems> m = ArrayMatcherT<kProbeItems>{T.slots, T.params}.resolved();
-            ArrayMatcherT<kProbeItems>::Shared none;
-            probe_tile(T.pkey, T.n_probe, m, none, T.out, tile, ps);
+            const ArrayMatcherT<kGroupedItems> m = ArrayMatcherT<kGroupedItems>{T.slots, T.params}.resolved();
+            ArrayMatcherT<kGroupedItems>::Shared none;
+            probe_tile(T.pkey, T.n_probe, m, none, T.out, tile, pw);
         } else if (T.kind == 1) {
             LoopMatcher m{T.nl_keys, T.nl_rids, T.nl_count};
             if (loaded_task != ps.task) {
@@ -541,7 +548,8 @@ __global__ void __launch_bounds__(kProbeThreads, CJ_GROUPED_MIN_BLOCKS)
                 bloom_live = false;
                 __syncthreads();
             }
-            probe_tile(T.pkey, T.n_probe, m, sh.l, T.out, tile, ps);
+            probe_tile(T.pkey, T.n_probe, m, sh.l, T.out, 2 * tile, ps);
+            probe_tile(T.pkey, T.n_probe, m, sh.l, T.out, 2 * tile + 1, ps);
         } else {
             if (!bloom_live) {
                 __syncthreads();
@@ -553,12 +561,14 @@ __global__ void __launch_bounds__(kProbeThreads, CJ_GROUPED_MIN_BLOCKS)
             if (T.build_key_type == CJ_INT32) {
                 HashMatcher<int32_t> m{{T.dir, reinterpret_cast<const Tuple<int32_t> *>(T.tuples), T.log2_slots},
                                        g_bloom};
-                probe_tile(T.pkey, T.n_probe, m, sh.h, T.out, tile, ps);
+                probe_tile(T.pkey, T.n_probe, m, sh.h, T.out, 2 * tile, ps);
+                probe_tile(T.pkey, T.n_probe, m, sh.h, T.out, 2 * tile + 1, ps);
             } else {
                 HashMatcher<int64_t> m{{T.dir, reinterpret_cast<const Tuple<int64_t> *>(T.tuples), T.log2_slots},
                                        g_bloom};
-                probe_tile(T.pkey, T.n_probe, m, *reinterpret_cast<const HashMatcher<int64_t>::Shared *>(&sh.h),
-                           T.out, tile, ps);
+                const auto &hs = *reinterpret_cast<const HashMatcher<int64_t>::Shared *>(&sh.h);
+                probe_tile(T.pkey, T.n_probe, m, hs, T.out, 2 * tile, ps);
+                probe_tile(T.pkey, T.n_probe, m, hs, T.out, 2 * tile + 1, ps);
             }
         }
     }
