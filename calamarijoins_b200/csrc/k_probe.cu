@@ -39,9 +39,10 @@ namespace {
 #ifndef CJ_HASH_MIN_BLOCKS
 #define CJ_HASH_MIN_BLOCKS 8
 #endif
-/* The grouped kernel carries every matcher's code: at 5 CTAs per SM (48
- * registers) it spills nothing and ran C4 2 % faster than at 8 (32
- * registers, 260 bytes of spills). The hash matchers alone spill a little at
+/* The grouped kernel carries every matcher's code and the shared memory of
+ * both tile shapes (35 KB): at 5 CTAs per SM (48 registers, 80 bytes of
+ * spills) it ran C4 faster than at 4 (64 registers, no spills) and at 6 (40
+ * registers, 252 bytes of spills). The hash matchers alone spill a little at
  * 8 CTAs but ran 11 % slower at 6 without spills: occupancy wins there. */
 #ifndef CJ_GROUPED_MIN_BLOCKS
 #define CJ_GROUPED_MIN_BLOCKS 5
